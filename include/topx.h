@@ -1,0 +1,179 @@
+/*
+ * topx.h -- C ABI of the B200-native TOP3D_XL engine (libtopx.so).
+ *
+ * The MATLAB reference (TOP3D_XL.m) has no foreign-function interface; this
+ * header is the boundary a MATLAB/Octave MEX gateway (or ctypes, or any C
+ * caller) binds.  Each entry point names the reference function it replaces
+ * ("TX:<line>" = line in TOP3D_XL.m).
+ *
+ * Conventions
+ *  - Every call returns a topx_status; TOPX_OK is 0.  No C++ exception crosses
+ *    this boundary; topx_last_error() gives the message of the last failure.
+ *  - The caller owns every host buffer.  Arrays follow the reference's layouts:
+ *    voxel volumes are column-major (nely, nelx, nelz) like MATLAB logical
+ *    arrays; DOF vectors are interleaved (3k-2, 3k-1, 3k in MATLAB numbering,
+ *    i.e. 3k+c 0-based) over the compact node numbering of meshHierarchy_(1);
+ *    element vectors follow the compact element numbering (eleMapBack order).
+ *  - Integer index arrays returned by topx_get_index_array are 1-based, as in
+ *    the reference.
+ *  - A context is not thread-safe: use one host thread per context.  Device
+ *    memory is allocated at the first GPU call and freed by topx_destroy.
+ *  - There is no CPU fallback: GPU calls return TOPX_ERR_CUDA when no usable
+ *    sm_100 device is present.
+ */
+#ifndef TOPX_H_
+#define TOPX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int topx_status;
+enum {
+  TOPX_OK = 0,
+  TOPX_STOP = 1,          /* topx_step: the loop condition ended the run (TX:111 / TX:311) */
+  TOPX_ERR_ARG = -1,      /* bad argument (the reference's error('Wrong Input!') etc.) */
+  TOPX_ERR_STATE = -2,    /* call out of order (no model loaded, no run begun) */
+  TOPX_ERR_CUDA = -3,     /* CUDA runtime error or no usable device */
+  TOPX_ERR_MODEL = -4,    /* model/BC error (format, no loads, no fixations, unsupported BCs) */
+  TOPX_ERR_NUMERIC = -5,  /* solver failure (MMA dual solve did not finish, non-finite values) */
+  TOPX_ERR_INTERNAL = -6
+};
+
+enum { TOPX_GLOBAL = 0, TOPX_LOCAL = 1 };        /* consType (TX:12-18) */
+enum { TOPX_FP64 = 0, TOPX_MIXED = 1 };          /* arithmetic of the solver */
+
+typedef struct topx_ctx topx_ctx;
+
+/* InitialSettings (TX:21-38) plus engine options */
+typedef struct topx_params {
+  double modulus;          /* E0, 1.0 */
+  double poissonRatio;     /* 0.3 */
+  double modulusMin;       /* Emin, 1e-6 */
+  double SIMPpenalty;      /* 3 */
+  double cellSize;         /* 1 */
+  double tol;              /* PCG relative tolerance, 1e-3 */
+  int maxIT;               /* PCG iteration cap, 800 */
+  double weightFactorJacobi; /* 0.6 */
+  int64_t coarsestResolutionControl; /* 50000 */
+  int precision;           /* TOPX_FP64 or TOPX_MIXED */
+  int device;              /* CUDA device ordinal */
+} topx_params;
+
+/* sizes of the loaded model */
+typedef struct topx_info {
+  int numLevels;
+  int nelx, nely, nelz;             /* input resolution */
+  int64_t numElements, numNodes, numDOFs;  /* level 1 */
+  int resX[8], resY[8], resZ[8];    /* padded resolution per level */
+  int64_t levelElements[8], levelNodes[8];
+  int numLoadCases;
+  int64_t numFixedDOFs;
+  int64_t numPassive;
+} topx_info;
+
+/* one optimisation iteration (history row of TX:186-191 / TX:393-399) */
+typedef struct topx_iter {
+  int loop;
+  double c;        /* cDesign: objective (compliance) */
+  double vol;      /* V: mean density before the update */
+  double sharp;    /* sharpness after the update */
+  double cons;     /* fval: constraint value */
+  double change;   /* max density change */
+  int its[8];      /* PCG iterations per load case (iters_Target.dat) */
+  int filter_its;  /* PDE-filter PCG iterations summed over the filters of this iteration */
+  double t_assemble, t_cg, t_opt, t_filter, t_total;  /* seconds */
+} topx_iter;
+
+/* which index array topx_get_index_array returns */
+enum {
+  TOPX_ARR_ENODMAT = 0,            /* numElements x 8, row-major [e][j] (meshHierarchy_(l).eNodMat) */
+  TOPX_ARR_ELEMAPBACK = 1,         /* numElements */
+  TOPX_ARR_NODMAPBACK = 2,         /* numNodes (grid ids of the level's own grid) */
+  TOPX_ARR_NODESONBOUNDARY = 3,
+  TOPX_ARR_ELEMENTSONBOUNDARY = 4, /* level 1 only */
+  TOPX_ARR_ELEMENTUPWARDMAP = 5,   /* numElements x span^3 (levels >= 2) */
+  TOPX_ARR_TRANSFERMAT = 6,        /* numElements x (span+1)^3 (levels >= 2), [e][k] */
+  TOPX_ARR_SOLIDNODEMAP = 7,       /* solidNodeMapCoarser2Finer (levels >= 2) */
+  TOPX_ARR_FIXEDDOFS = 8,          /* numDOFs 0/1 (level 1) */
+  TOPX_ARR_MAPUNIQUEKES = 9,       /* numElements (level 1) */
+  TOPX_ARR_ISTHISELE2NDLEVEL = 10  /* level-2 elements holding fixed DOFs (level 2) */
+};
+
+/* ---- lifecycle ------------------------------------------------------------ */
+topx_status topx_default_params(topx_params* p);
+topx_status topx_create(topx_ctx** ctx, const topx_params* p);
+topx_status topx_destroy(topx_ctx* ctx);
+const char* topx_last_error(const topx_ctx* ctx);
+const char* topx_version(void);
+
+/* ---- model (host only; no GPU needed) ------------------------------------- */
+/* CreateVoxelFEAmodel, logical input with built-in cuboid BCs (TX:529-560) +
+ * FEA_ApplyBoundaryCondition (TX:1294) + FEA_SetupVoxelBased (TX:1238) */
+topx_status topx_load_voxels(topx_ctx* ctx, const uint8_t* vox, int nely, int nelx, int nelz);
+/* CreateVoxelFEAmodel, .TopVoxel v1.0 input (TX:448-528) */
+topx_status topx_load_topvoxel(topx_ctx* ctx, const char* path);
+topx_status topx_get_info(const topx_ctx* ctx, topx_info* out);
+/* element stiffness matrix (TX:1254-1292), 24x24 row-major */
+topx_status topx_get_ke(const topx_ctx* ctx, double* out576);
+/* integer arrays of meshHierarchy_(level) / BC set-up for bit-exact comparison */
+topx_status topx_get_index_array(const topx_ctx* ctx, int level, int which, int32_t* out, size_t n, size_t* n_needed);
+/* transferMatCoeffi of a level >= 2 */
+topx_status topx_get_transfer_coeffi(const topx_ctx* ctx, int level, double* out, size_t n, size_t* n_needed);
+/* load vector F_(:,lc), interleaved DOFs (TX:1316-1322) */
+topx_status topx_get_load(const topx_ctx* ctx, int lc, double* out, size_t n);
+
+/* ---- solver building blocks (GPU; host buffers) --------------------------- */
+/* element moduli E (numElements) for the calls below; SIMP is applied by the caller */
+topx_status topx_set_moduli(topx_ctx* ctx, const double* E, size_t n);
+/* Solving_KbyU_MatrixFree, level 1 (TX:641-725): y = K(E) u, FP64 */
+topx_status topx_ku(topx_ctx* ctx, const double* u, double* y, size_t ndof);
+/* Solving_AssembleFEAstencil (TX:919-1066) for the current moduli */
+topx_status topx_assemble(topx_ctx* ctx);
+/* Solving_Vcycle (TX:747-781): z = M r in the context's precision */
+topx_status topx_vcycle(topx_ctx* ctx, const double* r, double* z, size_t ndof);
+/* Jacobi diagonal meshHierarchy_(level).diagK (level < numLevels), interleaved */
+topx_status topx_get_diag(topx_ctx* ctx, int level, double* out, size_t n);
+/* Solving_PCG with K*u and the V-cycle (TX:600-639), warm start from u; its = iterations */
+topx_status topx_pcg(topx_ctx* ctx, int lc, double* u, size_t ndof, int* its);
+/* TopOpti_ConductPDEFiltering_matrixFree (TX:870-902) with radius rmin */
+topx_status topx_filter(topx_ctx* ctx, double rmin, const double* src, double* out, size_t ne, int* its);
+/* TopOpti_ComputeUnitCompliance (TX:579-598) of displacement fields U (numDOFs x numLoadCases, column-major) */
+topx_status topx_unit_compliance(topx_ctx* ctx, const double* U, double* ce, size_t ne);
+
+/* ---- optimisation (TOP3D_XL_TO TX:40-223, TOP3D_XL_PIO TX:225-440) -------- */
+/* set-up + compliance of the fully solid domain (iteration 0) */
+topx_status topx_begin(topx_ctx* ctx, int consType, double V0, int nLoop, double rMin, double rHat,
+                       double* cSolid);
+/* one iteration of the while loop; TOPX_STOP when the loop condition fails */
+topx_status topx_step(topx_ctx* ctx, topx_iter* out);
+/* full run: begin + steps; hist may be NULL, else an array of at least nLoop rows */
+topx_status topx_run(topx_ctx* ctx, int consType, double V0, int nLoop, double rMin, double rHat,
+                     topx_iter* hist, int* loops, double* cSolid);
+/* densityLayout_ = xPhys (numElements) */
+topx_status topx_get_density(topx_ctx* ctx, double* out, size_t ne);
+topx_status topx_set_density(topx_ctx* ctx, const double* xPhys, size_t ne);
+/* displacement U(:,lc), interleaved DOFs */
+topx_status topx_get_displacement(topx_ctx* ctx, int lc, double* out, size_t ndof);
+
+/* ---- measurement (no reference counterpart) --------------------------------- */
+typedef struct topx_profile {
+  double ku_ms;             /* summed device time of the level-1 K*u launches inside PCG solves */
+  int64_t ku_launches;      /* launches that ran a PCG iteration */
+  int64_t pcg_iterations;   /* PCG iterations since profiling was switched on */
+} topx_profile;
+/* CUDA-event timer on the engine's stream */
+topx_status topx_timer_start(topx_ctx* ctx);
+topx_status topx_timer_stop(topx_ctx* ctx, double* ms);
+/* per-launch timing of the K*u kernel (events around each launch); on != 0 resets the counters */
+topx_status topx_set_profiling(topx_ctx* ctx, int on);
+topx_status topx_get_profile(topx_ctx* ctx, topx_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOPX_H_ */

@@ -1,0 +1,157 @@
+"""C ABI of libtopx.so on CPU: every symbol of include/topx.h is exported, the
+host-side model (discretisation, hierarchy, BCs) is bit-exact with the oracle's
+1-based reference numbering, and errors come back as status codes."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import top3dxl_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_symbols():
+    txt = open(os.path.join(ROOT, "include", "topx.h")).read()
+    return sorted(set(re.findall(r"\b(?:topx_status|const char\*)\s+(topx_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_header_symbol():
+    from top3d_xl_b200 import _lib
+    lib = _lib.load()
+    syms = _header_symbols()
+    assert len(syms) >= 30
+    for s in syms:
+        assert hasattr(lib, s), s
+        assert s in _lib.SIGNATURES, s
+
+
+def _compare(vox):
+    from top3d_xl_b200 import Context
+    m = O.build_model(vox)
+    ctx = Context()
+    info = ctx.load_voxels(vox)
+    assert info.numLevels == m.numLevels
+    for l in range(1, m.numLevels + 1):
+        lv = m.levels[l - 1]
+        checks = [("ENODMAT", lv.eNodMat.ravel()), ("ELEMAPBACK", lv.eleMapBack), ("NODMAPBACK", lv.nodMapBack),
+                  ("NODESONBOUNDARY", lv.nodesOnBoundary)]
+        if l == 1:
+            checks += [("ELEMENTSONBOUNDARY", lv.elementsOnBoundary), ("FIXEDDOFS", m.fixedDOFs.astype(np.int32)),
+                       ("MAPUNIQUEKES", m.mapUniqueKes)]
+        else:
+            checks += [("ELEMENTUPWARDMAP", lv.elementUpwardMap.ravel()), ("TRANSFERMAT", lv.transferMat.T.ravel()),
+                       ("SOLIDNODEMAP", lv.solidNodeMapCoarser2Finer)]
+            assert np.array_equal(ctx.transfer_coeffi(l), lv.transferMatCoeffi)
+        if l == 2:
+            checks.append(("ISTHISELE2NDLEVEL", m.isThisEle2ndLevel))
+        for name, ref in checks:
+            got = ctx.index_array(l, name)
+            assert got.dtype == np.int32 and np.array_equal(got, ref.astype(np.int32)), (l, name)
+    assert np.max(np.abs(ctx.ke() - m.levels[0].Ke)) < 1e-15
+    assert np.array_equal(ctx.load_vector(0), m.F[:, 0])
+    ctx.close()
+
+
+def test_indexing_bit_exact_config1():
+    _compare(np.ones((25, 50, 25), bool))
+
+
+def test_indexing_bit_exact_odd_cuboid():
+    _compare(np.ones((13, 29, 11), bool))
+
+
+def test_indexing_bit_exact_irregular():
+    rng = np.random.default_rng(4)
+    vox = rng.random((18, 37, 15)) < 0.7
+    vox[:, 0, :] = True
+    vox[:, -1, :] = True
+    _compare(vox)
+
+
+def _write_topvoxel(path, vox, fixed, loads, passive=(), density=False):
+    ny, nx, nz = vox.shape
+    solid = np.flatnonzero(vox.ravel(order="F")) + 1
+    with open(path, "w") as fh:
+        fh.write("# TOP3D_XL voxel model\nVersion: 1.0\nResolution: %d %d %d\n" % (nx, ny, nz))
+        fh.write("Density included: %d\nSolid voxels: %d\n" % (1 if density else 0, solid.size))
+        for s in solid:
+            fh.write("%d 1.0\n" % s if density else "%d\n" % s)
+        fh.write("Passive elements: %d\n" % len(passive))
+        for p in passive:
+            fh.write("%d\n" % p)
+        fh.write("Fixations: %d\n" % len(fixed))
+        for n, a, b, c in fixed:
+            fh.write("%d %d %d %d\n" % (n, a, b, c))
+        fh.write("Loads: %d\n" % len(loads[0]))
+        for n, a, b, c in loads[0]:
+            fh.write("%d %.17g %.17g %.17g\n" % (n, a, b, c))
+        fh.write("Additional Loads: %d\n" % (len(loads) - 1))
+        for k, ld in enumerate(loads[1:], start=2):
+            fh.write("Loads: %d %d\n" % (len(ld), k))
+            for n, a, b, c in ld:
+                fh.write("%d %.17g %.17g %.17g\n" % (n, a, b, c))
+
+
+def test_topvoxel_reader_matches_oracle(tmp_path):
+    from top3d_xl_b200 import Context
+    rng = np.random.default_rng(9)
+    ny, nx, nz = 10, 21, 9
+    vox = np.ones((ny, nx, nz), bool)
+    vox[rng.random(vox.shape) < 0.15] = False
+    vox[:, :2, :] = True
+    nny, nnx = ny + 1, nx + 1
+    fixed = [(iy + 1 + nny * nnx * iz, 1, 1, 1) for iz in range(nz + 1) for iy in range(nny)]
+    loads = [[(1 + iy + nny * nx + nny * nnx * nz, 0.0, 0.0, -1.0 / 3) for iy in range(3)]]
+    vox[:, -1, -1] = True
+    path = str(tmp_path / "m.TopVoxel")
+    _write_topvoxel(path, vox, fixed, loads, passive=[5, 17], density=True)
+    m = O.Model()
+    m.load_topvoxel(path)
+    m.apply_boundary_condition()
+    m.setup()
+    ctx = Context()
+    info = ctx.load_topvoxel(path)
+    assert info.numPassive == len(m.passiveElements)
+    assert np.array_equal(ctx.index_array(1, "ENODMAT"), m.levels[0].eNodMat.ravel())
+    assert np.array_equal(ctx.index_array(1, "FIXEDDOFS"), m.fixedDOFs.astype(np.int32))
+    assert np.array_equal(ctx.load_vector(0), m.F[:, 0])
+    ctx.close()
+
+
+def test_errors_are_status_codes():
+    from top3d_xl_b200 import Context, TopxError
+    ctx = Context()
+    with pytest.raises(TopxError) as e:
+        ctx.load_voxels(np.ones((2, 5, 5), bool))
+    assert "TOPX_ERR_ARG" in str(e.value)
+    with pytest.raises(TopxError) as e:
+        ctx.index_array(1, "ENODMAT")
+    assert "TOPX_ERR_STATE" in str(e.value)
+    with pytest.raises(TopxError):
+        ctx.load_topvoxel("/nonexistent.TopVoxel")
+    ctx.close()
+
+
+def test_local_requires_rhat():
+    from top3d_xl_b200 import TOP3D_XL
+    with pytest.raises(ValueError, match="Wrong Input!"):
+        TOP3D_XL(np.ones((4, 8, 4), bool), "LOCAL", 0.5, 3, 1.5, out_dir="/tmp/_topx_unused")
+
+
+def _have_gpu():
+    from tests.conftest import _have_gpu as h
+    return h()
+
+
+@pytest.mark.skipif(_have_gpu(), reason="checks the no-GPU error path")
+def test_gpu_call_without_device_fails_loudly():
+    from top3d_xl_b200 import Context, TopxError
+    ctx = Context()
+    ctx.load_voxels(np.ones((4, 8, 4), bool))
+    with pytest.raises(TopxError) as e:
+        ctx.assemble()
+    assert "TOPX_ERR_CUDA" in str(e.value)
+    ctx.close()

@@ -1,0 +1,132 @@
+"""GPU-vs-oracle parity of the solver building blocks, called through the C ABI.
+
+Sizes are chosen so the FP64 oracle finishes in seconds.  Tolerances: the
+native path computes the same FP64 arithmetic in a different summation order
+(node-centric gathers instead of accumarray scatters, slab LDL^T instead of a
+permuted sparse Cholesky), so single operators agree to ~1e-13 relative and
+iterative solves to ~1e-9.
+"""
+import numpy as np
+import pytest
+
+from oracle import top3dxl_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+@pytest.fixture(scope="module", params=["cuboid", "irregular"])
+def setup(request):
+    from top3d_xl_b200 import Context
+    if request.param == "cuboid":
+        vox = np.ones((12, 24, 12), bool)
+    else:
+        rng = np.random.default_rng(5)
+        vox = rng.random((13, 27, 11)) < 0.75
+        vox[:, 0, :] = True
+        vox[:, -1, :] = True
+    m = O.build_model(vox)
+    ctx = Context("fp64")
+    ctx.load_voxels(vox)
+    rng = np.random.default_rng(1)
+    x = rng.uniform(0.05, 1.0, m.levels[0].numElements)
+    S = m.S
+    E = S.modulusMin + x ** S.SIMPpenalty * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    ctx.set_moduli(E)
+    ctx.assemble()
+    yield dict(m=m, ctx=ctx, sol=sol, E=E, x=x, vox=vox)
+    ctx.close()
+
+
+def test_ku(setup):
+    m, ctx, sol = setup["m"], setup["ctx"], setup["sol"]
+    u = np.random.default_rng(2).standard_normal(m.levels[0].numDOFs)
+    y = ctx.ku(u)
+    assert _rel(y, sol.ku(u)) < 1e-13
+
+
+def test_diagonals(setup):
+    m, ctx = setup["m"], setup["ctx"]
+    for l in range(1, m.numLevels):
+        assert _rel(ctx.diag(l), m.levels[l - 1].diagK) < 1e-13, l
+
+
+def test_vcycle(setup):
+    m, ctx, sol = setup["m"], setup["ctx"], setup["sol"]
+    r = np.random.default_rng(3).standard_normal(m.levels[0].numDOFs)
+    assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-11
+
+
+def test_pcg(setup):
+    # the tol-1e-3 PCG amplifies rounding ~1e8 (tests/test_oracle.py), so the
+    # solution agrees to ~1e-8 while the compliance f'u agrees to ~1e-13
+    m, ctx, sol = setup["m"], setup["ctx"], setup["sol"]
+    u, its = ctx.pcg()
+    uo, itso, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], m.S.tol, m.S.maxIT)
+    f = m.F[:, 0]
+    assert its == itso
+    assert _rel(u, uo) < 1e-6
+    assert abs(f @ u - f @ uo) / abs(f @ uo) < 1e-11
+
+
+def test_compliance(setup):
+    m, ctx, sol = setup["m"], setup["ctx"], setup["sol"]
+    U = np.random.default_rng(4).standard_normal((m.levels[0].numDOFs, 1))
+    assert _rel(ctx.unit_compliance(U), O.unit_compliance(m, U)) < 1e-13
+
+
+@pytest.mark.parametrize("rmin", [np.sqrt(3), 6.0])
+def test_filter(setup, rmin):
+    m, ctx = setup["m"], setup["ctx"]
+    src = np.random.default_rng(6).uniform(0, 1, m.levels[0].numElements)
+    out, its = ctx.filter(rmin, src)
+    flt = O.PDEFilter(m, rmin, m.S)
+    ref = flt(src)
+    assert its == flt.last_its
+    assert _rel(out, ref) < 1e-10
+
+
+@pytest.fixture(scope="module")
+def mixed_setup():
+    from top3d_xl_b200 import Context
+    vox = np.ones((12, 24, 12), bool)
+    m = O.build_model(vox)
+    ctx = Context("mixed")
+    ctx.load_voxels(vox)
+    x = np.random.default_rng(1).uniform(0.05, 1.0, m.levels[0].numElements)
+    S = m.S
+    E = S.modulusMin + x ** S.SIMPpenalty * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    ctx.set_moduli(E)
+    ctx.assemble()
+    yield dict(m=m, ctx=ctx, sol=sol)
+    ctx.close()
+
+
+def test_mixed_vcycle_is_fp32_accurate(mixed_setup):
+    m, ctx, sol = mixed_setup["m"], mixed_setup["ctx"], mixed_setup["sol"]
+    r = np.random.default_rng(3).standard_normal(m.levels[0].numDOFs)
+    assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-5
+
+
+def test_mixed_pcg_keeps_fp64_compliance(mixed_setup):
+    # FP32 noise confined to the preconditioner keeps CG's Galerkin property
+    m, ctx, sol = mixed_setup["m"], mixed_setup["ctx"], mixed_setup["sol"]
+    u, its = ctx.pcg()
+    uo, itso, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], m.S.tol, m.S.maxIT)
+    f = m.F[:, 0]
+    assert abs(its - itso) <= 1
+    assert abs(f @ u - f @ uo) / abs(f @ uo) < 1e-9
+    assert np.linalg.norm(f - ctx.ku(u)) / np.linalg.norm(f) < m.S.tol
+
+
+def test_filter_preserves_constants(setup):
+    m, ctx = setup["m"], setup["ctx"]
+    out, _ = ctx.filter(np.sqrt(3), np.ones(m.levels[0].numElements))
+    assert np.max(np.abs(out - 1.0)) < 1e-3

@@ -1,0 +1,69 @@
+"""End-to-end FP64 parity of the optimisation loop against the golden oracle
+histories (tests/golden/make_golden.py), through the C ABI.
+
+Bar: identical PCG iteration counts; per-iteration compliance within 1e-9
+relative while the reference algorithm's own rounding sensitivity allows it
+(the golden files hold `env_c`, the spread of the oracle against itself with
+1e-15 relative noise in its coarse solve), and within 10x that envelope after;
+final density within max(1e-6, 10*env_x) in the max norm.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _run(vox, cons, V0, nLoop, rMin, rHat, steps, precision="fp64"):
+    from top3d_xl_b200 import Context
+    with Context(precision) as ctx:
+        ctx.load_voxels(vox)
+        cs = ctx.begin(cons, V0, nLoop, rMin, rHat)
+        hist = []
+        for _ in range(steps):
+            r = ctx.step()
+            if r is None:
+                break
+            hist.append(r)
+        return cs, hist, ctx.density()
+
+
+def _check(g, cs, hist, x):
+    assert abs(cs - g["cSolid"]) / g["cSolid"] < 1e-11
+    c = np.array([h["c"] for h in hist])
+    its = np.array([k for h in hist for k in h["its"]])
+    assert len(c) == len(g["c"])
+    assert np.array_equal(its, g["its"]), (its, g["its"])
+    rel = np.abs(c - g["c"]) / np.abs(g["c"])
+    env = g["env_c"]
+    bar = np.where(env < 1e-10, 1e-9, np.maximum(1e-9, 10 * env))
+    assert np.all(rel < bar), (rel, bar)
+    assert np.max(np.abs(x - g["xPhys"])) < max(1e-6, 10 * float(g["env_x"]))
+
+
+def test_config1_global_10_iterations():
+    g = np.load(os.path.join(GOLD, "config1_global_10.npz"))
+    cs, hist, x = _run(np.ones((25, 50, 25), bool), "GLOBAL", 0.12, 50, np.sqrt(3), 0.0, 10)
+    _check(g, cs, hist, x)
+
+
+def test_irregular_global_6_iterations():
+    g = np.load(os.path.join(GOLD, "irregular_global_6.npz"))
+    cs, hist, x = _run(g["vox"], "GLOBAL", 0.3, 50, np.sqrt(3), 0.0, 6)
+    _check(g, cs, hist, x)
+
+
+def test_small_local_6_iterations():
+    g = np.load(os.path.join(GOLD, "small_local_6.npz"))
+    cs, hist, x = _run(np.ones((12, 24, 12), bool), "LOCAL", 0.5, 300, np.sqrt(3), 6.0, 6)
+    _check(g, cs, hist, x)
+
+
+def test_mixed_precision_error_vs_fp64():
+    g = np.load(os.path.join(GOLD, "config1_global_10.npz"))
+    cs, hist, x = _run(np.ones((25, 50, 25), bool), "GLOBAL", 0.12, 50, np.sqrt(3), 0.0, 10, "mixed")
+    c = np.array([h["c"] for h in hist])
+    rel = np.abs(c - g["c"]) / np.abs(g["c"])
+    assert rel.max() < 1e-5, rel

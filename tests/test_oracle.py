@@ -1,0 +1,181 @@
+"""Pins of the FP64 oracle (CPU).  The reference ships no tests or golden
+vectors and MATLAB/Octave cannot run here, so the restatement is pinned by
+properties of the reference's algorithm and by entries of its closed-form Ke."""
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import top3dxl_oracle as O
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_ke_closed_form_entries():
+    # first row of TOP3D_XL.m:1287-1288: KE = 1/((1+nu)(2nu-1)) * (A11 + nu*B11 ...), C from TX:1259
+    nu = 0.3
+    Ke = O.element_stiffness(nu, 1.0)
+    C = [2 / 9, 1 / 18, 1 / 24, 1 / 36, 1 / 48, 5 / 72, 1 / 3, 1 / 6, 1 / 12]
+    f = 1 / ((1 + nu) * (2 * nu - 1))
+    a11 = [-C[0], -C[2], -C[2], C[1], C[2], C[2]]
+    b11 = [C[6], 0, 0, 0, -C[7], -C[7]]
+    expect = [f * (a + nu * b) for a, b in zip(a11, b11)]
+    assert np.allclose(Ke[0, :6], expect, rtol=0, atol=1e-15)
+
+
+def test_ke_symmetric_with_six_rigid_modes():
+    Ke = O.element_stiffness(0.3, 1.0)
+    assert np.allclose(Ke, Ke.T, atol=1e-16)
+    w = np.linalg.eigvalsh(Ke)
+    assert np.sum(np.abs(w) < 1e-12) == 6
+    assert np.all(w > -1e-12)
+
+
+def test_ke_scales_with_cell_size():
+    assert np.allclose(O.element_stiffness(0.3, 2.0), 2 * O.element_stiffness(0.3, 1.0), atol=1e-15)
+
+
+def test_discretisation_sizes_match_reference_rules():
+    # config 1 of the reference (25x50x25): padded 56x32x32, levels 3, coarsest 600 DOFs
+    lvl, nl = O.discretize(np.ones((25, 50, 25), bool), O.Settings())
+    assert (lvl.resX, lvl.resY, lvl.resZ) == (56, 32, 32)
+    assert nl == 4
+    m = O.build_model(np.ones((25, 50, 25), bool))
+    assert m.numLevels == 3
+    assert m.levels[0].numElements == 31250 and m.levels[0].numNodes == 34476
+    assert (m.levels[1].resX, m.levels[1].resY, m.levels[1].resZ) == (14, 8, 8)
+    assert m.levels[1].numElements == 637 and m.levels[2].numElements == 112
+    assert m.levels[2].numDOFs == 600
+    assert m.fixingCond.shape[0] == 676 and m.loadingCond[0].shape[0] == 130
+
+
+def _small(vox=None, seed=1):
+    vox = np.ones((8, 16, 8), bool) if vox is None else vox
+    m = O.build_model(vox)
+    rng = np.random.default_rng(seed)
+    S = m.S
+    x = rng.uniform(0.05, 1, m.levels[0].numElements)
+    E = S.modulusMin + x ** 3 * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    return m, sol, E
+
+
+def _assembled_K(m, sol):
+    l1 = m.levels[0]
+    Kel = sol.element_mats_level1()
+    en = l1.eNodMat - 1
+    edof = np.empty((l1.numElements, 24), dtype=np.int64)
+    for a in range(8):
+        for c in range(3):
+            edof[:, 3 * a + c] = 3 * en[:, a] + c
+    rows = np.repeat(edof, 24, axis=1).ravel()
+    cols = np.tile(edof, (1, 24)).ravel()
+    return sp.csr_matrix((Kel.reshape(l1.numElements, -1).ravel(), (rows, cols)), shape=(l1.numDOFs,) * 2)
+
+
+def test_matrix_free_ku_equals_assembled_K():
+    m, sol, E = _small()
+    K = _assembled_K(m, sol)
+    u = np.random.default_rng(2).standard_normal(m.levels[0].numDOFs)
+    assert np.allclose(sol.ku(u), K @ u, rtol=1e-13, atol=1e-13)
+    # fixed DOFs get an identity row (sum of 1/nAdj)
+    fx = np.flatnonzero(m.fixedDOFs)
+    assert np.allclose(K[fx][:, fx].diagonal(), 1.0, atol=1e-15)
+
+
+def _prolong_matrix(sol, ii):
+    lv = sol.m.levels[ii - 1]
+    n = lv.numDOFs
+    cols = [sol.prolong(np.eye(1, n, k).ravel(), ii) for k in range(n)]
+    return np.array(cols).T
+
+
+def test_restriction_is_transpose_of_prolongation():
+    m, sol, E = _small()
+    for ii in range(2, m.numLevels + 1):
+        P = _prolong_matrix(sol, ii)
+        r = np.random.default_rng(ii).standard_normal(P.shape[0])
+        assert np.allclose(sol.restrict(r, ii), P.T @ r, atol=1e-12)
+
+
+def test_galerkin_coarse_operators_equal_PtKP():
+    m, sol, E = _small()
+    K1 = _assembled_K(m, sol).toarray()
+    P2 = _prolong_matrix(sol, 2)
+    K2 = P2.T @ K1 @ P2
+    # level-2 diagonal from the Galerkin element operators
+    assert np.allclose(m.levels[1].diagK, np.diag(K2), rtol=1e-12)
+    P3 = _prolong_matrix(sol, 3)
+    K3 = P3.T @ K2 @ P3
+    assert np.allclose(sol.K_coarsest.toarray(), K3, rtol=1e-10, atol=1e-12)
+
+
+def test_vcycle_is_symmetric():
+    m, sol, E = _small()
+    rng = np.random.default_rng(3)
+    a, b = rng.standard_normal((2, m.levels[0].numDOFs))
+    assert abs(a @ sol.vcycle(b) - b @ sol.vcycle(a)) < 1e-10 * abs(a @ sol.vcycle(b))
+
+
+def test_filter_preserves_constants_and_is_symmetric():
+    m, sol, E = _small()
+    flt = O.PDEFilter(m, math.sqrt(3), m.S)
+    out = flt(np.ones(m.levels[0].numElements))
+    assert np.max(np.abs(out - 1)) < 1e-3
+
+
+def test_oc_satisfies_volume_constraint():
+    h = O.run_global(np.ones((8, 16, 8), bool), 0.3, 3, math.sqrt(3))
+    assert abs(np.mean(h["xPhys"]) - 0.3) < 1e-5
+
+
+def test_mma_kkt_on_small_problem():
+    # min sum((x-a)^2) s.t. mean(x) <= 0.3 via one MMA step from a feasible point moves toward the optimum
+    n = 50
+    rng = np.random.default_rng(0)
+    a = rng.uniform(0, 1, n)
+    x = np.full(n, 0.3)
+    xold1 = xold2 = x.copy()
+    low = upp = np.zeros(n)
+    f0 = np.sum((x - a) ** 2)
+    for it in range(1, 6):
+        df = 2 * (x - a)
+        g = np.array([np.mean(x) - 0.3])
+        dg = np.full((1, n), 1.0 / n)
+        x, xold1, xold2, low, upp = O.mma_seq(1, n, it, x, np.maximum(0, x - 0.1), np.minimum(1, x + 0.1),
+                                              xold1, xold2, df, g, dg, low, upp)
+    assert np.sum((x - a) ** 2) < f0
+    assert np.mean(x) <= 0.3 + 1e-3
+
+
+def test_pcg_rounding_sensitivity_of_the_reference_algorithm():
+    """A 1e-16 relative perturbation of the coarse solve moves the tol-1e-3 PCG
+    solution by ~1e-8: the reference algorithm amplifies rounding ~1e8, which
+    bounds how closely any re-implementation can track it."""
+    m, sol, E = _small(np.ones((12, 24, 12), bool))
+    S = m.S
+    u0, it0, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], S.tol, S.maxIT)
+    cs = sol.coarse_solve
+    rng = np.random.default_rng(7)
+    sol.coarse_solve = lambda r: cs(r) * (1 + 1e-16 * rng.standard_normal(r.shape))
+    u1, it1, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], S.tol, S.maxIT)
+    sol.coarse_solve = cs
+    d = np.linalg.norm(u1 - u0) / np.linalg.norm(u0)
+    assert it0 == it1 and 1e-12 < d < 1e-6
+
+
+def test_golden_fixtures_reproduce():
+    g = np.load(os.path.join(GOLD, "config1_global_10.npz"))
+    h = O.run_global(np.ones((25, 50, 25), bool), 0.12, 50, math.sqrt(3), max_loops=2)
+    assert np.allclose(h["c"], g["c"][:2], rtol=1e-12)
+    assert list(h["its"]) == list(g["its"][:2])
+
+
+def test_history_file_formats(tmp_path):
+    h = dict(its=[3, 4], c=[1.5, 2.25], sharp=[0.5, 0.25])
+    O.write_history_files(str(tmp_path), h)
+    assert open(tmp_path / "c_Target.dat").read() == "%30.16e\n%30.16e\n" % (1.5, 2.25)
+    assert open(tmp_path / "iters_Target.dat").read() == "3\n4\n"

@@ -1,0 +1,104 @@
+"""ctypes binding of libtopx.so (include/topx.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+libtopx.so is missing or cannot be loaded, importing the engine raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtopx.so")
+
+TOPX_OK, TOPX_STOP = 0, 1
+ERRORS = {-1: "TOPX_ERR_ARG", -2: "TOPX_ERR_STATE", -3: "TOPX_ERR_CUDA", -4: "TOPX_ERR_MODEL",
+          -5: "TOPX_ERR_NUMERIC", -6: "TOPX_ERR_INTERNAL"}
+
+ARR = dict(ENODMAT=0, ELEMAPBACK=1, NODMAPBACK=2, NODESONBOUNDARY=3, ELEMENTSONBOUNDARY=4,
+           ELEMENTUPWARDMAP=5, TRANSFERMAT=6, SOLIDNODEMAP=7, FIXEDDOFS=8, MAPUNIQUEKES=9,
+           ISTHISELE2NDLEVEL=10)
+
+
+class Params(C.Structure):
+    _fields_ = [("modulus", C.c_double), ("poissonRatio", C.c_double), ("modulusMin", C.c_double),
+                ("SIMPpenalty", C.c_double), ("cellSize", C.c_double), ("tol", C.c_double),
+                ("maxIT", C.c_int), ("weightFactorJacobi", C.c_double),
+                ("coarsestResolutionControl", C.c_int64), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [("numLevels", C.c_int), ("nelx", C.c_int), ("nely", C.c_int), ("nelz", C.c_int),
+                ("numElements", C.c_int64), ("numNodes", C.c_int64), ("numDOFs", C.c_int64),
+                ("resX", C.c_int * 8), ("resY", C.c_int * 8), ("resZ", C.c_int * 8),
+                ("levelElements", C.c_int64 * 8), ("levelNodes", C.c_int64 * 8),
+                ("numLoadCases", C.c_int), ("numFixedDOFs", C.c_int64), ("numPassive", C.c_int64)]
+
+
+class Iter(C.Structure):
+    _fields_ = [("loop", C.c_int), ("c", C.c_double), ("vol", C.c_double), ("sharp", C.c_double),
+                ("cons", C.c_double), ("change", C.c_double), ("its", C.c_int * 8), ("filter_its", C.c_int),
+                ("t_assemble", C.c_double), ("t_cg", C.c_double), ("t_opt", C.c_double),
+                ("t_filter", C.c_double), ("t_total", C.c_double)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("ku_ms", C.c_double), ("ku_launches", C.c_int64), ("pcg_iterations", C.c_int64)]
+
+
+# exported symbols and their argument types (checked by tests/test_abi.py)
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I32 = C.POINTER(C.c_int32)
+_SZ = C.c_size_t
+SIGNATURES = {
+    "topx_default_params": [C.POINTER(Params)],
+    "topx_create": [C.POINTER(_P), C.POINTER(Params)],
+    "topx_destroy": [_P],
+    "topx_last_error": [_P],
+    "topx_version": [],
+    "topx_load_voxels": [_P, C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_int],
+    "topx_load_topvoxel": [_P, C.c_char_p],
+    "topx_get_info": [_P, C.POINTER(Info)],
+    "topx_get_ke": [_P, _D],
+    "topx_get_index_array": [_P, C.c_int, C.c_int, _I32, _SZ, C.POINTER(_SZ)],
+    "topx_get_transfer_coeffi": [_P, C.c_int, _D, _SZ, C.POINTER(_SZ)],
+    "topx_get_load": [_P, C.c_int, _D, _SZ],
+    "topx_set_moduli": [_P, _D, _SZ],
+    "topx_ku": [_P, _D, _D, _SZ],
+    "topx_assemble": [_P],
+    "topx_vcycle": [_P, _D, _D, _SZ],
+    "topx_get_diag": [_P, C.c_int, _D, _SZ],
+    "topx_pcg": [_P, C.c_int, _D, _SZ, C.POINTER(C.c_int)],
+    "topx_filter": [_P, C.c_double, _D, _D, _SZ, C.POINTER(C.c_int)],
+    "topx_unit_compliance": [_P, _D, _D, _SZ],
+    "topx_begin": [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, _D],
+    "topx_step": [_P, C.POINTER(Iter)],
+    "topx_run": [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.POINTER(Iter),
+                 C.POINTER(C.c_int), _D],
+    "topx_get_density": [_P, _D, _SZ],
+    "topx_set_density": [_P, _D, _SZ],
+    "topx_get_displacement": [_P, C.c_int, _D, _SZ],
+    "topx_timer_start": [_P],
+    "topx_timer_stop": [_P, _D],
+    "topx_set_profiling": [_P, C.c_int],
+    "topx_get_profile": [_P, C.POINTER(Profile)],
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libtopx.so and declare its prototypes; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libtopx.so not built at {path}; run `python -m top3d_xl_b200.build`")
+    lib = C.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version") else C.c_int
+    _lib = lib
+    return lib

@@ -1,0 +1,755 @@
+// Device engine of the TOP3D_XL B200 path (see topx_engine.hpp).
+#include "topx_engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+namespace topx {
+
+static int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+Engine::Engine(Model& model, int precision, int device) : M(model), prec(precision) {
+  TOPX_CUDA_OK(cudaSetDevice(device));
+  // blocking stream: ordered with the synchronous cudaMemset/cudaMemcpy calls of the set-up code
+  TOPX_CUDA_OK(cudaStreamCreate(&st));
+  nl = M.numLevels;
+  if (nl < 3 || int(M.levels.size()) != nl) throw std::runtime_error("model hierarchy not built");
+  for (int l = 0; l < nl; ++l) {
+    const Level& L = M.levels[l];
+    Grid g;
+    g.ny = L.resY;
+    g.nx = L.resX;
+    g.nz = L.resZ;
+    g.stride = round_up(g.nnodes(), 32);
+    G.push_back(g);
+  }
+  const Level& l1 = M.levels[0];
+  Ne = l1.numElements;
+  Nn = l1.numNodes;
+  // ---- presence masks per level -------------------------------------------
+  present.resize(nl);
+  epresent.resize(nl);
+  for (int l = 0; l < nl; ++l) {
+    const Level& L = M.levels[l];
+    std::vector<uint8_t> pn(size_t(G[l].nnodes()), 0), pe(size_t(G[l].nelems()), 0);
+    for (auto k : L.nodMapBack) pn[k - 1] = 1;
+    for (auto k : L.eleMapBack) pe[k - 1] = 1;
+    present[l].upload(pn.data(), pn.size());
+    epresent[l].upload(pe.data(), pe.size());
+    if (l == 0) solid1.upload(pe.data(), pe.size());
+  }
+  std::vector<int32_t> emb(Ne), nmb(Nn);
+  for (int64_t e = 0; e < Ne; ++e) emb[e] = l1.eleMapBack[e] - 1;
+  for (int64_t k = 0; k < Nn; ++k) nmb[k] = l1.nodMapBack[k] - 1;
+  eleMapBack0.upload(emb.data(), emb.size());
+  nodMapBack0.upload(nmb.data(), nmb.size());
+  // ---- boundary conditions: global form of the per-element BC matrices -------
+  // (TOP3D_XL.m:1338-1437).  Check that the element matrices reduce to
+  // y = m.*K(m.*u) + (1-m).*cfix.*u before relying on it.
+  std::vector<uint8_t> fb(size_t(G[0].nnodes()), 0);
+  std::vector<double> cf(size_t(G[0].nnodes()), 0.0);
+  for (int64_t k = 0; k < Nn; ++k) {
+    uint8_t b = 0;
+    for (int c = 0; c < 3; ++c)
+      if (M.fixedDOFs[size_t(k) * 3 + c]) b |= uint8_t(1u << c);
+    fb[nmb[k]] = b;
+  }
+  std::vector<double> cacc(size_t(Nn) * 3, 0.0);
+  for (int a = 0; a < 8; ++a)
+    for (int64_t e = 0; e < Ne; ++e) {
+      const int32_t sl = M.mapUniqueKes[e];
+      const int32_t node = l1.eNodMat[size_t(e) * 8 + a];
+      const uint8_t nb = fb[nmb[node - 1]];
+      if (sl == 0) {
+        if (nb) throw std::runtime_error("unsupported boundary conditions: element without BC matrix at a fixed DOF");
+        continue;
+      }
+      for (int c = 0; c < 3; ++c) {
+        const bool zm = (M.keFreeZeroMask[sl - 1] >> (3 * a + c)) & 1u;
+        if (zm != bool((nb >> c) & 1))
+          throw std::runtime_error("unsupported boundary conditions: element BC matrix differs from the fixed-DOF mask");
+        if (zm) cacc[size_t(node - 1) * 3 + c] += M.keFixedDiag[sl - 1][3 * a + c];
+      }
+    }
+  for (int64_t k = 0; k < Nn; ++k) {
+    double v = 0.0;
+    for (int c = 0; c < 3; ++c)
+      if (M.fixedDOFs[size_t(k) * 3 + c]) {
+        if (v != 0.0 && cacc[size_t(k) * 3 + c] != v)
+          throw std::runtime_error("unsupported boundary conditions: per-component fixed diagonal differs");
+        v = cacc[size_t(k) * 3 + c];
+      }
+    cf[nmb[k]] = v;
+  }
+  fixbits.upload(fb.data(), fb.size());
+  // ---- load vectors -----------------------------------------------------------
+  const int nL = int(M.loads.size());
+  F.resize(nL);
+  U.resize(nL);
+  for (int lc = 0; lc < nL; ++lc) {
+    std::vector<double> f(size_t(G[0].stride) * 3, 0.0);
+    for (size_t i = 0; i < M.loads[lc].node.size(); ++i) {
+      const int64_t n = nmb[M.loads[lc].node[i] - 1];
+      for (int c = 0; c < 3; ++c) f[n + c * G[0].stride] = M.loads[lc].f[i][c];
+    }
+    F[lc].upload(f.data(), f.size());
+    U[lc].alloc(f.size());
+  }
+  // ---- element matrices ---------------------------------------------------------
+  upload_ke(M.Ke.data());
+  {
+    std::vector<double> T2 = galerkin_templates(M.Ke, M.levels[1].span);
+    const std::vector<double> P4 = child_prolongators(M.levels[1].span);
+    const int nc = M.levels[1].span * M.levels[1].span * M.levels[1].span;
+    // BC-modified templates of level-2 children with fixed DOFs, de-duplicated by (slot, mask)
+    std::map<std::pair<int, uint32_t>, int> modid;
+    const Level& l2 = M.levels[1];
+    std::vector<int32_t> fe, ts;
+    std::vector<double> ff;
+    auto tmpl = [&](const double* Pc, const double* K, double* out) {
+      double KP[576];
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) {
+          double s = 0;
+          for (int q = 0; q < 24; ++q) s += K[i * 24 + q] * Pc[q * 24 + j];
+          KP[i * 24 + j] = s;
+        }
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) {
+          double s = 0;
+          for (int q = 0; q < 24; ++q) s += Pc[q * 24 + i] * KP[q * 24 + j];
+          out[i * 24 + j] = s;
+        }
+    };
+    for (int64_t j = 0; j < l2.numElements; ++j) {
+      const int32_t idx = M.isThisEle2ndLevel[j];
+      if (idx == 0) continue;
+      fe.push_back(l2.eleMapBack[j] - 1);
+      std::vector<int32_t> sel(nc);
+      for (int c = 0; c < nc; ++c) sel[c] = c;
+      std::vector<double> Fj(576, 0.0);
+      for (int c : M.sonElesWithFixedDOFs[idx - 1]) {
+        const int32_t e = l2.elementUpwardMap[size_t(j) * nc + c];
+        const int32_t sl = M.mapUniqueKes[e - 1];
+        const uint32_t mask = M.keFreeZeroMask[sl - 1];
+        auto key = std::make_pair(c, mask);
+        auto it = modid.find(key);
+        if (it == modid.end()) {
+          double Kf[576], Tm[576];
+          for (int r = 0; r < 24; ++r)
+            for (int q = 0; q < 24; ++q)
+              Kf[r * 24 + q] = ((mask >> r) & 1u) || ((mask >> q) & 1u) ? 0.0 : M.Ke[r * 24 + q];
+          tmpl(&P4[size_t(c) * 576], Kf, Tm);
+          const int id = nc + int(modid.size());
+          T2.insert(T2.end(), Tm, Tm + 576);
+          it = modid.emplace(key, id).first;
+        }
+        sel[c] = it->second;
+        double Kx[576] = {0}, Tx[576];
+        for (int r = 0; r < 24; ++r) Kx[r * 25] = M.keFixedDiag[sl - 1][r];
+        tmpl(&P4[size_t(c) * 576], Kx, Tx);
+        for (int k = 0; k < 576; ++k) Fj[k] += Tx[k];
+      }
+      ts.insert(ts.end(), sel.begin(), sel.end());
+      ff.insert(ff.end(), Fj.begin(), Fj.end());
+    }
+    nflag = int(fe.size());
+    Tall.upload(T2.data(), T2.size());
+    if (nflag) {
+      fl_elem.upload(fe.data(), fe.size());
+      fl_tsel.upload(ts.data(), ts.size());
+      fl_F.upload(ff.data(), ff.size());
+    }
+    const std::vector<double> P2 = child_prolongators(2);
+    P8.upload(P2.data(), P2.size());
+  }
+  Ks.resize(nl);
+  for (int l = 1; l < nl; ++l) Ks[l].alloc(size_t(G[l].nelems()) * 576);
+  // ---- coarsest slab structure -------------------------------------------------
+  {
+    const Grid& g = G[nl - 1];
+    const int dims[3] = {g.nny(), g.nnx(), g.nnz()};
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+      if (dims[a] > dims[ax]) ax = a;
+    si.axis = ax;
+    si.ns = dims[ax];
+    if (ax == 0) {
+      si.nu = dims[1];
+      si.nv = dims[2];
+    } else if (ax == 1) {
+      si.nu = dims[0];
+      si.nv = dims[2];
+    } else {
+      si.nu = dims[0];
+      si.nv = dims[1];
+    }
+    si.m = 3 * si.nu * si.nv;
+    if (si.m > 4096) throw std::runtime_error("coarsest level too large for the slab solver");
+    const size_t mm = size_t(si.m) * si.m;
+    slabA.alloc(mm * si.ns);
+    slabSinv.alloc(mm * si.ns);
+    slabBup.alloc(size_t(si.nu) * si.nv * 81 * std::max(1, si.ns - 1));
+    slabT.alloc(mm);
+    gjP.alloc(32 * 32);
+    gjR.alloc(size_t(32) * si.m);
+    gjC.alloc(size_t(si.m) * 32);
+    slabW.alloc(size_t(si.m) * si.ns);
+    slabV.alloc(size_t(si.m) * si.ns * 2);
+  }
+  // ---- workspaces ------------------------------------------------------------
+  {
+    const size_t S1 = size_t(G[0].stride) * 3;
+    for (DevBuf<double>* b : {&kw.r, &kw.z, &kw.p, &kw.q}) b->alloc(S1);
+    E64.alloc(size_t(G[0].nelems()));
+    cfix64.upload(cf.data(), cf.size());
+    if (prec == PREC_FP64) {
+      alloc_vwork(v64);
+      alloc_fwork(f64);
+    } else {
+      alloc_vwork(v32);
+      alloc_fwork(f32);
+    }
+  }
+  // ---- reductions and scalars ---------------------------------------------------
+  red1.alloc(size_t(kMaxRedBlocks) * kMaxRedSlots);
+  red2.alloc(size_t(kMaxRedBlocks) * kMaxRedSlots);
+  tickets.alloc(8);
+  rs1 = RedScratch{red1.p, tickets.p};
+  rs2 = RedScratch{red2.p, tickets.p + 1};
+  scE.alloc(1);
+  scF.alloc(1);
+  objS.alloc(1);
+  ocS.alloc(1);
+  mmaS.alloc(1);
+  dscal.alloc(16);
+  TOPX_CUDA_OK(cudaMallocHost(&h_sc, sizeof(PcgScalars)));
+  // ---- optimiser state -------------------------------------------------------
+  for (DevBuf<double>* b : {&x, &xPhys, &dc, &ce, &tmpA, &tmpB, &xTilde, &xhat, &dfdx, &dxv, &volMax})
+    b->alloc(size_t(Ne));
+  int64_t npas = 0;
+  for (auto e : M.passiveElements) npas += (e >= 1 && e <= Ne) ? 1 : 0;
+  nActive_ = Ne - npas;
+  if (!M.passiveElements.empty()) {
+    std::vector<uint8_t> pm(size_t(Ne), 0);
+    for (auto e : M.passiveElements) pm[e - 1] = 1;
+    passive.upload(pm.data(), pm.size());
+  }
+  for (int i = 0; i < 8; ++i) {
+    cudaEvent_t e;
+    TOPX_CUDA_OK(cudaEventCreate(&e));
+    ev.push_back(e);
+  }
+  for (int i = 0; i < 2; ++i) TOPX_CUDA_OK(cudaEventCreate(&tev[i]));
+  for (int i = 0; i < 16; ++i) {
+    cudaEvent_t e;
+    TOPX_CUDA_OK(cudaEventCreate(&e));
+    pev.push_back(e);
+  }
+  std::ostringstream os;
+  os << "levels=" << nl;
+  for (int l = 0; l < nl; ++l) os << " L" << (l + 1) << "=" << G[l].nx << "x" << G[l].ny << "x" << G[l].nz;
+  os << " slab(axis=" << si.axis << ",ns=" << si.ns << ",m=" << si.m << ") flagged=" << nflag;
+  info_ = os.str();
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+}
+
+Engine::~Engine() {
+  for (auto e : ev) cudaEventDestroy(e);
+  for (auto e : pev) cudaEventDestroy(e);
+  for (auto e : tev)
+    if (e) cudaEventDestroy(e);
+  if (h_sc) cudaFreeHost(h_sc);
+  if (st) cudaStreamDestroy(st);
+}
+
+template <typename TC>
+void Engine::alloc_vwork(VWork<TC>& v) {
+  v.d1.alloc(size_t(G[0].stride) * 3);
+  v.rl.resize(nl);
+  v.xl.resize(nl);
+  v.dl.resize(nl);
+  size_t tmax = 0;
+  for (int l = 1; l < nl; ++l) {
+    const size_t Sl = size_t(G[l].stride) * 3;
+    v.rl[l].alloc(Sl);
+    v.xl[l].alloc(Sl);
+    if (l < nl - 1) v.dl[l].alloc(Sl);
+    const Grid& gf = G[l - 1];
+    const Grid& gc = G[l];
+    tmax = std::max(tmax, size_t(gc.nny()) * gf.nnx() * gf.nnz());
+  }
+  v.tmp1.alloc(tmax * 3);
+  v.tmp2.alloc(tmax * 3);
+}
+
+template <typename TF>
+void Engine::alloc_fwork(FWork<TF>& f) {
+  const size_t N1 = size_t(G[0].nnodes());
+  for (DevBuf<TF>* b : {&f.fr, &f.fz, &f.fp, &f.fq, &f.fy, &f.fb}) b->alloc(N1);
+  f.fsrc.alloc(size_t(G[0].nelems()));
+  f.fdp[0].alloc(N1);
+  f.fdp[1].alloc(N1);
+}
+
+void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
+  TOPX_CUDA_OK(cudaMemcpyAsync(h_sc, d, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  h = *h_sc;
+}
+
+// ---------------------------------------------------------------------------
+// design state
+// ---------------------------------------------------------------------------
+void Engine::set_xphys(const double* h) {
+  TOPX_CUDA_OK(cudaMemcpy(xPhys.p, h, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+}
+void Engine::get_xphys(double* h) const {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h, xPhys.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+}
+void Engine::get_U(int lc, double* h) const {
+  DevBuf<double> tmp;
+  tmp.alloc(size_t(Nn) * 3);
+  launch_grid_to_compact_nodes<double>(st, U[lc].p, tmp.p, G[0], nodMapBack0.p, Nn);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h, tmp.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+}
+void Engine::set_U(int lc, const double* h) {
+  DevBuf<double> tmp;
+  tmp.upload(h, size_t(Nn) * 3);
+  TOPX_CUDA_OK(cudaMemsetAsync(U[lc].p, 0, U[lc].bytes(), st));
+  launch_compact_to_grid_nodes<double>(st, tmp.p, U[lc].p, G[0], nodMapBack0.p, Nn);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+}
+
+void Engine::update_moduli(const double* d_xPhys, bool solid) {
+  if (solid)
+    launch_fill_scatter(st, eleMapBack0.p, Ne, M.S.modulus, E64.p, nullptr);
+  else
+    launch_simp_scatter(st, d_xPhys, eleMapBack0.p, Ne, M.S.modulusMin, M.S.modulus, M.S.SIMPpenalty, E64.p,
+                        nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Solving_AssembleFEAstencil (TOP3D_XL.m:919-1066)
+// ---------------------------------------------------------------------------
+void Engine::assemble() {
+  if (prec == PREC_FP64)
+    launch_diag_l1<double>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v64.d1.p);
+  else
+    launch_diag_l1<double, float>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v32.d1.p);
+  launch_galerkin_l2(st, G[1], E64.p, Tall.p, Ks[1].p);
+  launch_galerkin_l2_flagged(st, G[1], E64.p, nflag, fl_elem.p, fl_tsel.p, fl_F.p, Tall.p, Ks[1].p);
+  for (int l = 2; l < nl; ++l) launch_galerkin_span2(st, G[l], Ks[l - 1].p, epresent[l].p, P8.p, Ks[l].p);
+  for (int l = 1; l < nl - 1; ++l) {
+    if (prec == PREC_FP64)
+      launch_diag_coarse<double>(st, G[l], Ks[l].p, present[l].p, v64.dl[l].p);
+    else
+      launch_diag_coarse<float>(st, G[l], Ks[l].p, present[l].p, v32.dl[l].p);
+  }
+  factor_coarsest();
+}
+
+void Engine::factor_coarsest() {
+  launch_slab_assemble(st, G[nl - 1], si, Ks[nl - 1].p, present[nl - 1].p, slabA.p, slabBup.p);
+  const size_t mm = size_t(si.m) * si.m;
+  const size_t bs = size_t(si.nu) * si.nv * 81;
+  for (int s = 0; s < si.ns; ++s) {
+    double* Sinv = slabSinv.p + s * mm;
+    launch_slab_schur(st, si, s, s ? slabSinv.p + (s - 1) * mm : nullptr, s ? slabBup.p + (s - 1) * bs : nullptr,
+                      slabA.p + s * mm, slabT.p, Sinv);
+    launch_spd_inverse(st, si.m, Sinv, gjP.p, gjR.p, gjC.p);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 'Adapted' V-cycle (TOP3D_XL.m:747-781)
+// ---------------------------------------------------------------------------
+template <typename TC>
+void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
+  launch_restrict<double, TC>(st, M.levels[1].span, kw.r.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
+  for (int l = 2; l < nl; ++l)
+    launch_restrict<TC, TC>(st, M.levels[l].span, v.rl[l - 1].p, G[l - 1], v.tmp1.p, v.tmp2.p, v.rl[l].p, G[l]);
+  launch_slab_solve<TC>(st, G[nl - 1], si, slabSinv.p, slabBup.p, v.rl[nl - 1].p, slabW.p, slabV.p,
+                        v.xl[nl - 1].p, sc);
+  const double om = M.S.weightFactorJacobi;
+  for (int l = nl - 2; l >= 1; --l)
+    launch_prolong_smooth<TC, TC, TC>(st, M.levels[l + 1].span, v.xl[l + 1].p, G[l + 1], v.rl[l].p, v.dl[l].p,
+                                      present[l].p, v.xl[l].p, G[l], om, false, false, sc, rs1);
+  launch_prolong_smooth<TC, double, TC>(st, M.levels[1].span, v.xl[1].p, G[1], kw.r.p, v.d1.p, present[0].p,
+                                        kw.z.p, G[0], om, true, init, sc, rs1);
+}
+
+void Engine::vcycle(bool init, PcgScalars* sc) {
+  if (prec == PREC_FP64)
+    vcycle_t<double>(v64, init, sc);
+  else
+    vcycle_t<float>(v32, init, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Solving_PCG (TOP3D_XL.m:600-639) on device-resident scalars
+// ---------------------------------------------------------------------------
+int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
+  const Grid& g = G[0];
+  PcgScalars* sc = scE.p;
+  if (warm)
+    launch_ku<double>(st, KU_PLAIN, g, y, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+  else
+    TOPX_CUDA_OK(cudaMemsetAsync(kw.q.p, 0, kw.q.bytes(), st));
+  launch_residual_init<double>(st, g, b, kw.q.p, kw.r.p, sc, rs1, tol, maxIT);
+  vcycle(true, sc);
+  const int CH = 8;
+  PcgScalars h{};
+  int launched = 0;
+  while (launched < maxIT) {
+    const int first = launched;
+    for (int c = 0; c < CH && launched < maxIT; ++c, ++launched) {
+      if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c], st));
+      launch_ku<double>(st, KU_P_UPDATE, g, kw.p.p, kw.z.p, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+      if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
+      launch_pcg_update<double, double>(st, g, y, kw.z.p, kw.p.p, kw.r.p, kw.q.p, sc, rs1);
+      vcycle(false, sc);
+    }
+    read_scalars(h, sc);
+    if (prof_) {
+      // count the launches that ran an iteration (later ones return at once)
+      for (int c = 0; first + c < launched && first + c < h.its; ++c) {
+        float ms = 0.f;
+        TOPX_CUDA_OK(cudaEventElapsedTime(&ms, pev[2 * c], pev[2 * c + 1]));
+        prof_ku_ms += ms;
+        prof_ku_launches += 1;
+      }
+    }
+    if (h.done) break;
+  }
+  read_scalars(h, sc);
+  if (prof_) prof_pcg_its += h.its;
+  return h.its;
+}
+
+int Engine::solve(int lc) { return pcg(F[lc].p, U[lc].p, true, M.S.tol, M.S.maxIT); }
+
+void Engine::compliance(double* d_ce) {
+  for (size_t lc = 0; lc < U.size(); ++lc)
+    launch_unit_compliance(st, G[0], U[lc].p, eleMapBack0.p, Ne, M.objWeighting[lc], lc > 0, d_ce);
+}
+
+// ---------------------------------------------------------------------------
+// PDE filter (TOP3D_XL.m:816-917)
+// ---------------------------------------------------------------------------
+void Engine::setup_filter(int slot, double rmin) {
+  const std::array<double, 64> KF = pde_filter_kernel(rmin, M.S.cellSize * 1.0);
+  upload_filter_kernel(KF.data(), slot);
+  filterR[slot] = rmin;
+  if (prec == PREC_FP64)
+    launch_filter_diag<double>(st, G[0], solid1.p, slot, f64.fdp[slot].p);
+  else
+    launch_filter_diag<float>(st, G[0], solid1.p, slot, f32.fdp[slot].p);
+}
+
+template <typename T>
+int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) {
+  const Grid& g = G[0];
+  PcgScalars* sc = scF.p;
+  launch_scatter_elems_t<T>(st, d_src, eleMapBack0.p, Ne, w.fsrc.p);
+  launch_filter_e2n<T>(st, g, w.fsrc.p, w.fb.p);
+  launch_filter_residual_init<T>(st, g, w.fb.p, w.fdp[slot].p, w.fr.p, w.fz.p, w.fy.p, sc, rs1, M.S.tol / 10,
+                                 M.S.maxIT);
+  const int CH = 8;
+  PcgScalars h{};
+  int launched = 0;
+  while (launched < M.S.maxIT) {
+    for (int c = 0; c < CH && launched < M.S.maxIT; ++c, ++launched) {
+      launch_filter_ku<T>(st, KU_P_UPDATE, g, slot, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
+      launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1);
+    }
+    read_scalars(h, sc);
+    if (h.done) break;
+  }
+  launch_filter_n2e<T>(st, g, w.fy.p, eleMapBack0.p, Ne, d_out);
+  return h.its;
+}
+
+int Engine::filter(int slot, const double* d_src, double* d_out) {
+  if (prec == PREC_FP64) return filter_t<double>(f64, slot, d_src, d_out);
+  return filter_t<float>(f32, slot, d_src, d_out);
+}
+
+// ---------------------------------------------------------------------------
+// test entry points
+// ---------------------------------------------------------------------------
+void Engine::apply_K(const double* h_u, double* h_y) {
+  DevBuf<double> cu, du, dy;
+  cu.upload(h_u, size_t(Nn) * 3);
+  du.alloc(size_t(G[0].stride) * 3);
+  dy.alloc(size_t(G[0].stride) * 3);
+  launch_compact_to_grid_nodes<double>(st, cu.p, du.p, G[0], nodMapBack0.p, Nn);
+  launch_ku<double>(st, KU_PLAIN, G[0], du.p, nullptr, nullptr, dy.p, E64.p, fixbits.p, cfix64.p, nullptr, rs1);
+  launch_grid_to_compact_nodes<double>(st, dy.p, cu.p, G[0], nodMapBack0.p, Nn);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h_y, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+}
+
+void Engine::apply_vcycle(const double* h_r, double* h_z) {
+  DevBuf<double> cu;
+  cu.upload(h_r, size_t(Nn) * 3);
+  PcgScalars z{};
+  z.done = 0;
+  TOPX_CUDA_OK(cudaMemcpy(scE.p, &z, sizeof(z), cudaMemcpyHostToDevice));
+  TOPX_CUDA_OK(cudaMemsetAsync(kw.r.p, 0, kw.r.bytes(), st));
+  launch_compact_to_grid_nodes<double>(st, cu.p, kw.r.p, G[0], nodMapBack0.p, Nn);
+  vcycle(true, scE.p);
+  launch_grid_to_compact_nodes<double>(st, kw.z.p, cu.p, G[0], nodMapBack0.p, Nn);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h_z, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+}
+
+void Engine::timer_start() { TOPX_CUDA_OK(cudaEventRecord(tev[0], st)); }
+double Engine::timer_stop_ms() {
+  TOPX_CUDA_OK(cudaEventRecord(tev[1], st));
+  TOPX_CUDA_OK(cudaEventSynchronize(tev[1]));
+  float ms = 0.f;
+  TOPX_CUDA_OK(cudaEventElapsedTime(&ms, tev[0], tev[1]));
+  return double(ms);
+}
+void Engine::set_profiling(bool on) {
+  prof_ = on;
+  prof_ku_ms = 0.0;
+  prof_ku_launches = 0;
+  prof_pcg_its = 0;
+}
+
+void Engine::set_moduli_host(const double* h_E) {
+  TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_E, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  launch_scatter_elems_t<double>(st, tmpA.p, eleMapBack0.p, Ne, E64.p);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+}
+
+int Engine::pcg_host(int lc, double* h_u) {
+  set_U(lc, h_u);
+  const int its = solve(lc);
+  get_U(lc, h_u);
+  return its;
+}
+
+int Engine::filter_host(double rmin, const double* h_src, double* h_out) {
+  setup_filter(0, rmin);
+  TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_src, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  const int its = filter(0, tmpA.p, tmpB.p);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h_out, tmpB.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+  return its;
+}
+
+void Engine::compliance_host(const double* h_U, double* h_ce) {
+  for (size_t lc = 0; lc < U.size(); ++lc) set_U(int(lc), h_U + lc * size_t(Nn) * 3);
+  compliance(ce.p);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  TOPX_CUDA_OK(cudaMemcpy(h_ce, ce.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+}
+
+void Engine::get_diag(int level, double* h_d) const {
+  // compact interleaved diagonal of `level` (1-based, < numLevels)
+  const Level& L = M.levels[level - 1];
+  const Grid& g = G[level - 1];
+  std::vector<double> dense(size_t(g.stride) * 3);
+  if (prec == PREC_FP64) {
+    const double* src = level == 1 ? v64.d1.p : v64.dl[level - 1].p;
+    TOPX_CUDA_OK(cudaStreamSynchronize(st));
+    TOPX_CUDA_OK(cudaMemcpy(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> f(dense.size());
+    const float* src = level == 1 ? v32.d1.p : v32.dl[level - 1].p;
+    TOPX_CUDA_OK(cudaStreamSynchronize(st));
+    TOPX_CUDA_OK(cudaMemcpy(f.data(), src, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < f.size(); ++i) dense[i] = f[i];
+  }
+  for (int64_t k = 0; k < L.numNodes; ++k)
+    for (int c = 0; c < 3; ++c) h_d[3 * k + c] = dense[(L.nodMapBack[k] - 1) + c * g.stride];
+}
+
+// ---------------------------------------------------------------------------
+// optimisation loop
+// ---------------------------------------------------------------------------
+void Engine::begin(int consType, double V0, int nLoop, double rMin, double rHat) {
+  consType_ = consType;
+  V0_ = V0;
+  nLoop_ = nLoop;
+  rMin_ = rMin;
+  rHat_ = rHat;
+  loop_ = 0;
+  loopbeta_ = 0;
+  change_ = 1.0;
+  sharp_ = 1.0;
+  betaPIO_ = 1.0;
+  setup_filter(0, rMin);
+  if (consType == 1) setup_filter(1, rHat);
+  std::vector<double> h(size_t(Ne), V0);
+  for (DevBuf<double>* b : {&x, &xPhys, &xTilde, &volMax}) TOPX_CUDA_OK(cudaMemcpy(b->p, h.data(), sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  for (auto& u : U) TOPX_CUDA_OK(cudaMemsetAsync(u.p, 0, u.bytes(), st));
+  // compliance of the fully solid domain (TOP3D_XL.m:94-104)
+  update_moduli(nullptr, true);
+  assemble();
+  for (size_t lc = 0; lc < U.size(); ++lc) solve(int(lc));
+  compliance(ce.p);
+  launch_sum(st, Ne, ce.p, nullptr, dscal.p, rs1);
+  double s = 0;
+  TOPX_CUDA_OK(cudaMemcpyAsync(&s, dscal.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  cSolid_ = M.S.modulus * s;
+}
+
+static double ev_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return double(ms) * 1e-3;
+}
+
+bool Engine::step(IterRecord& rec) {
+  if (!(loop_ < nLoop_ && change_ > 0.0001 && sharp_ > 0.01)) return false;
+  const auto t_host0 = std::chrono::steady_clock::now();
+  ++loop_;
+  rec = IterRecord{};
+  rec.loop = loop_;
+  const double Emin = M.S.modulusMin, E0 = M.S.modulus, pen = M.S.SIMPpenalty;
+  TOPX_CUDA_OK(cudaEventRecord(ev[0], st));
+  update_moduli(xPhys.p, false);
+  assemble();
+  TOPX_CUDA_OK(cudaEventRecord(ev[1], st));
+  for (size_t lc = 0; lc < U.size(); ++lc) rec.its.push_back(solve(int(lc)));
+  TOPX_CUDA_OK(cudaEventRecord(ev[2], st));
+  compliance(ce.p);
+  launch_objective(st, Ne, ce.p, xPhys.p, cSolid_, Emin, E0, pen, dc.p, objS.p, rs1);
+  ObjState os{};
+  TOPX_CUDA_OK(cudaMemcpyAsync(&os, objS.p, sizeof(os), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaEventRecord(ev[3], st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  rec.c = os.cObj * cSolid_;
+  rec.vol = os.xsum / double(Ne);
+  if (consType_ == 0) {
+    // sensitivity filter ft = 1 (TOP3D_XL.m:135-137)
+    launch_ewise(st, EW_MUL, Ne, x.p, dc.p, tmpA.p, 0.0);
+    rec.filter_its = filter(0, tmpA.p, tmpB.p);
+    launch_ewise(st, EW_DIV_MAXX, Ne, tmpB.p, x.p, dc.p, 1e-3);
+    TOPX_CUDA_OK(cudaEventRecord(ev[4], st));
+    // OC bisection (TOP3D_XL.m:145-156)
+    OcState oc{};
+    oc.l1 = 0.0;
+    oc.l2 = 1e9;
+    oc.fval = os.xsum / double(Ne) - V0_;
+    TOPX_CUDA_OK(cudaMemcpyAsync(ocS.p, &oc, sizeof(oc), cudaMemcpyHostToDevice, st));
+    const uint8_t* pas = passive.p;
+    for (int chunk = 0; chunk < 8; ++chunk) {
+      for (int k = 0; k < 32; ++k) launch_oc_step(st, Ne, x.p, dc.p, pas, ocS.p, rs1, 0.2);
+      TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
+      TOPX_CUDA_OK(cudaStreamSynchronize(st));
+      if (oc.converged) break;
+    }
+    launch_oc_final(st, Ne, x.p, dc.p, pas, xPhys.p, ocS.p, rs1, rs2, 0.2);
+    TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
+    TOPX_CUDA_OK(cudaEventRecord(ev[5], st));
+    TOPX_CUDA_OK(cudaStreamSynchronize(st));
+    rec.cons = oc.fval;
+    rec.change = oc.change;
+    rec.sharp = 4 * oc.sharpsum / double(Ne);
+    rec.t_assemble = ev_ms(ev[0], ev[1]);
+    rec.t_cg = ev_ms(ev[1], ev[2]);
+    rec.t_filter = ev_ms(ev[3], ev[4]);
+    rec.t_opt = ev_ms(ev[2], ev[3]) + ev_ms(ev[4], ev[5]);
+  } else {
+    step_local(rec, os);
+  }
+  change_ = rec.change;
+  sharp_ = rec.sharp;
+  rec.t_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_host0).count();
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// LOCAL: porous infill with local-volume p-norm constraint and MMA
+// (TOP3D_XL.m:311-401)
+// ---------------------------------------------------------------------------
+void Engine::step_local(IterRecord& rec, const ObjState& os) {
+  (void)os;
+  const double etaPIO = 0.5;
+  const int pPIO = 16;
+  const double pMaxPIO = 128;
+  ++loopbeta_;
+  if (!xold1.p) {
+    for (DevBuf<double>* b : {&xold1, &xold2, &low, &upp, &alpha, &beta, &p0, &q0, &pij, &qij, &xmma})
+      b->alloc(size_t(Ne));
+  }
+  TOPX_CUDA_OK(cudaEventRecord(ev[3], st));
+  // local volume fraction and its sensitivity (TOP3D_XL.m:333-335)
+  int fits = filter(1, xPhys.p, xhat.p);
+  launch_pnorm_terms(st, Ne, xhat.p, V0_, pPIO, dscal.p, rs1);
+  double pnsum = 0;
+  TOPX_CUDA_OK(cudaMemcpyAsync(&pnsum, dscal.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  const double pn = pnsum / double(Ne);
+  launch_local_sens(st, Ne, xhat.p, xTilde.p, dc.p, V0_, pPIO, pn, betaPIO_, etaPIO, dfdx.p, dxv.p, tmpA.p);
+  // filtered sensitivities (TOP3D_XL.m:338-350)
+  fits += filter(0, tmpA.p, dc.p);
+  fits += filter(1, dfdx.p, tmpB.p);
+  launch_ewise(st, EW_MUL, Ne, tmpB.p, dxv.p, tmpA.p, 0.0);
+  fits += filter(0, tmpA.p, dfdx.p);
+  TOPX_CUDA_OK(cudaEventRecord(ev[4], st));
+  // MMA update (TOP3D_XL.m:352-369)
+  const double fval = std::pow(pnsum / double(Ne), 1.0 / pPIO) - 1;
+  if (loop_ == 1) {
+    TOPX_CUDA_OK(cudaMemcpyAsync(xold1.p, x.p, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, st));
+    TOPX_CUDA_OK(cudaMemcpyAsync(xold2.p, x.p, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, st));
+    TOPX_CUDA_OK(cudaMemsetAsync(low.p, 0, low.bytes(), st));
+    TOPX_CUDA_OK(cudaMemsetAsync(upp.p, 0, upp.bytes(), st));
+  }
+  const uint8_t* pas = passive.p;
+  launch_mma_gensub(st, Ne, loop_, 0.1, x.p, pas, xold1.p, xold2.p, low.p, upp.p, dc.p, dfdx.p, fval, nActive_,
+                    alpha.p, beta.p, p0.p, q0.p, pij.p, qij.p, mmaS.p, rs1);
+  MmaState ms{};
+  for (int chunk = 0; chunk < 64; ++chunk) {
+    for (int k = 0; k < 16; ++k) {
+      launch_mma_newton(st, Ne, pas, low.p, upp.p, alpha.p, beta.p, p0.p, q0.p, pij.p, qij.p, mmaS.p, rs1);
+      launch_mma_residual(st, Ne, pas, low.p, upp.p, alpha.p, beta.p, p0.p, q0.p, pij.p, qij.p, xmma.p, mmaS.p, rs1);
+    }
+    TOPX_CUDA_OK(cudaMemcpyAsync(&ms, mmaS.p, sizeof(ms), cudaMemcpyDeviceToHost, st));
+    TOPX_CUDA_OK(cudaStreamSynchronize(st));
+    if (ms.finished) break;
+  }
+  if (!ms.finished) throw std::runtime_error("MMA dual solve did not finish");
+  launch_mma_finish(st, Ne, pas, xmma.p, xold1.p, x.p, mmaS.p, rs2);
+  TOPX_CUDA_OK(cudaEventRecord(ev[5], st));
+  // density filter + Heaviside projection with beta continuation (TOP3D_XL.m:372-382)
+  fits += filter(0, x.p, xTilde.p);
+  if (loopbeta_ >= 40) {
+    betaPIO_ = std::min(2 * betaPIO_, pMaxPIO);
+    loopbeta_ = 0;
+  }
+  launch_heaviside(st, Ne, xTilde.p, pas, betaPIO_, etaPIO, xPhys.p, dscal.p + 1, rs1);
+  double sh = 0;
+  TOPX_CUDA_OK(cudaMemcpyAsync(&sh, dscal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaMemcpyAsync(&ms, mmaS.p, sizeof(ms), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaEventRecord(ev[6], st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  rec.filter_its = fits;
+  rec.cons = fval;
+  rec.change = ms.change;
+  rec.sharp = 4 * sh / double(Ne);
+  rec.t_assemble = ev_ms(ev[0], ev[1]);
+  rec.t_cg = ev_ms(ev[1], ev[2]);
+  rec.t_opt = ev_ms(ev[2], ev[3]) + ev_ms(ev[4], ev[5]);
+  rec.t_filter = ev_ms(ev[3], ev[4]) + ev_ms(ev[5], ev[6]);
+}
+
+template void Engine::alloc_vwork<double>(VWork<double>&);
+template void Engine::alloc_vwork<float>(VWork<float>&);
+template void Engine::alloc_fwork<double>(FWork<double>&);
+template void Engine::alloc_fwork<float>(FWork<float>&);
+
+}  // namespace topx

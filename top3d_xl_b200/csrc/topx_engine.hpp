@@ -1,0 +1,208 @@
+// Device engine of the TOP3D_XL B200 path: owns all HBM-resident state of one
+// design job (moduli, displacements, multigrid hierarchy, coarse factor, filter
+// and optimiser state) and runs the optimisation loop of TOP3D_XL.m
+// (GLOBAL: TOP3D_XL.m:40-183, LOCAL: TOP3D_XL.m:225-401) on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "topx_kernels.cuh"
+#include "topx_mesh.hpp"
+#include "topx_opt.cuh"
+
+namespace topx {
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count, bool zero = true) {
+    release();
+    n = count;
+    if (count) {
+      TOPX_CUDA_OK(cudaMalloc(&p, sizeof(T) * count));
+      if (zero) TOPX_CUDA_OK(cudaMemset(p, 0, sizeof(T) * count));
+    }
+  }
+  void upload(const T* h, size_t count) {
+    alloc(count, false);
+    if (count) TOPX_CUDA_OK(cudaMemcpy(p, h, sizeof(T) * count, cudaMemcpyHostToDevice));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return sizeof(T) * n; }
+};
+
+enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+struct IterRecord {
+  int loop = 0;
+  double c = 0, vol = 0, sharp = 0, cons = 0, change = 0;
+  std::vector<int> its;  // per load case
+  double t_assemble = 0, t_cg = 0, t_opt = 0, t_filter = 0, t_lvf = 0, t_total = 0;
+  int filter_its = 0;
+};
+
+// Level-1 Krylov vectors of the PCG (always FP64: operator, residual, dots).
+struct KrylovWork {
+  DevBuf<double> r, z, p, q;
+};
+
+// Multigrid preconditioner workspace in its storage precision TC (double for
+// the plain FP64 path, float for the mixed path): Jacobi diagonals and the
+// residual/correction fields of every level.
+template <typename TC>
+struct VWork {
+  DevBuf<TC> d1;
+  std::vector<DevBuf<TC>> rl, xl, dl;  // per level (index = level-1; level 1 uses the Krylov vectors)
+  DevBuf<TC> tmp1, tmp2;                // separable restriction passes
+};
+
+// PDE-filter workspace (scalar node fields) in precision TF.
+template <typename TF>
+struct FWork {
+  DevBuf<TF> fr, fz, fp, fq, fy, fb, fsrc;
+  std::array<DevBuf<TF>, 2> fdp;
+};
+
+class Engine {
+ public:
+  Engine(Model& model, int precision, int device);
+  ~Engine();
+
+  // ---- design state -----------------------------------------------------
+  void set_xphys(const double* h_xPhys);  // host, compact order
+  void get_xphys(double* h_xPhys) const;
+  void get_U(int lc, double* h_U) const;  // interleaved compact DOFs
+  void set_U(int lc, const double* h_U);
+
+  // ---- building blocks (device-resident) -----------------------------------
+  void update_moduli(const double* d_xPhys, bool solid);  // SIMP -> E (dense)
+  void assemble();                                        // diagonals, Galerkin, coarse factor
+  int solve(int lc);                                      // PCG for load case lc (warm start U)
+  void compliance(double* d_ce);                          // load-weighted unit compliance
+  int filter(int slot, const double* d_src, double* d_out);
+  void setup_filter(int slot, double rmin);
+
+  // host-buffer entry points of the C ABI
+  void set_moduli_host(const double* h_E);
+  int pcg_host(int lc, double* h_u);
+  int filter_host(double rmin, const double* h_src, double* h_out);
+  void compliance_host(const double* h_U, double* h_ce);
+  // for tests: y = K u (FP64), z = M r (V-cycle in the engine precision)
+  void apply_K(const double* h_u, double* h_y);
+  void apply_vcycle(const double* h_r, double* h_z);
+  void get_diag(int level, double* h_d) const;
+
+  // ---- optimisation drivers ------------------------------------------------
+  void begin(int consType, double V0, int nLoop, double rMin, double rHat);
+  bool step(IterRecord& rec);  // false when the loop condition ends the run
+  double cSolid() const { return cSolid_; }
+  int loop() const { return loop_; }
+  const std::string& info() const { return info_; }
+
+  // ---- measurement ----------------------------------------------------------
+  // device timer on the engine stream; per-launch timing of the level-1 K*u
+  // kernel inside PCG solves (events around each launch, read after each chunk)
+  void timer_start();
+  double timer_stop_ms();
+  void set_profiling(bool on);
+  double prof_ku_ms = 0.0;
+  int64_t prof_ku_launches = 0;
+  int64_t prof_pcg_its = 0;
+
+  Model& M;
+  int prec;
+  cudaStream_t st = nullptr;
+  int nl = 0;
+  std::vector<Grid> G;  // per level
+  int64_t Ne = 0, Nn = 0;
+
+ private:
+  template <typename TC>
+  void alloc_vwork(VWork<TC>& v);
+  template <typename TF>
+  void alloc_fwork(FWork<TF>& f);
+  template <typename TC>
+  void vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc);
+  void vcycle(bool init, PcgScalars* sc);
+  int pcg(const double* b, double* y, bool warm, double tol, int maxIT);
+  template <typename TF>
+  int filter_t(FWork<TF>& f, int slot, const double* d_src, double* d_out);
+  void step_local(IterRecord& rec, const ObjState& os);
+  void factor_coarsest();
+  void read_scalars(PcgScalars& h, const PcgScalars* d) const;
+
+  // level-1 static data
+  DevBuf<uint8_t> fixbits, solid1;
+  std::vector<DevBuf<uint8_t>> present, epresent;  // per level
+  DevBuf<int32_t> eleMapBack0, nodMapBack0;
+  DevBuf<double> E64, cfix64;        // dense moduli (elements) and fixed-DOF diagonal (nodes)
+  std::vector<DevBuf<double>> F, U;  // per load case, dense SoA FP64
+  // coarse operators
+  std::vector<DevBuf<double>> Ks;  // per level (index = level-1), dense elements x 576
+  DevBuf<double> Tall, P8;
+  DevBuf<int32_t> fl_elem, fl_tsel;
+  DevBuf<double> fl_F;
+  int nflag = 0;
+  SlabInfo si;
+  DevBuf<double> slabA, slabBup, slabSinv, slabT, gjP, gjR, gjC, slabW, slabV;
+  // workspaces
+  KrylovWork kw;
+  VWork<double> v64;
+  VWork<float> v32;
+  FWork<double> f64;
+  FWork<float> f32;
+  // scalars & reductions
+  DevBuf<double> red1, red2;
+  DevBuf<unsigned> tickets;
+  RedScratch rs1{}, rs2{};
+  DevBuf<PcgScalars> scE, scF;
+  DevBuf<ObjState> objS;
+  DevBuf<OcState> ocS;
+  DevBuf<MmaState> mmaS;
+  DevBuf<double> dscal;
+  PcgScalars* h_sc = nullptr;  // pinned
+  // optimiser state (compact, FP64)
+  DevBuf<double> x, xPhys, dc, ce, tmpA, tmpB, xTilde, xhat, dfdx, dxv, volMax;
+  DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;
+  DevBuf<uint8_t> passive;
+  std::array<double, 2> filterR{{0, 0}};
+  // run state
+  int consType_ = 0, nLoop_ = 0, loop_ = 0, loopbeta_ = 0;
+  int64_t nActive_ = 0;
+  double V0_ = 0, rMin_ = 0, rHat_ = 0, cSolid_ = 0, change_ = 1, sharp_ = 1, betaPIO_ = 1;
+  std::string info_;
+  std::vector<cudaEvent_t> ev;
+  bool prof_ = false;
+  std::vector<cudaEvent_t> pev;  // pairs around K*u launches of one chunk
+  cudaEvent_t tev[2] = {nullptr, nullptr};
+};
+
+}  // namespace topx

@@ -1,0 +1,579 @@
+// Level-1 elasticity kernels of the TOP3D_XL B200 path: matrix-free K*u,
+// Jacobi diagonal, PCG vector algebra, trilinear multigrid transfers, SIMP,
+// unit compliance.  FP64 (plain path) and FP32 (mixed path) instantiations.
+#include <type_traits>
+
+#include "topx_kernels.cuh"
+
+namespace topx {
+
+__constant__ double c_Ke64[576];
+__constant__ float c_Ke32[576];
+
+template <typename T>
+__device__ __forceinline__ T ke(int i);
+template <>
+__device__ __forceinline__ double ke<double>(int i) {
+  return c_Ke64[i];
+}
+template <>
+__device__ __forceinline__ float ke<float>(int i) {
+  return c_Ke32[i];
+}
+
+void upload_ke(const double* Ke576) {
+  float f[576];
+  for (int i = 0; i < 576; ++i) f[i] = float(Ke576[i]);
+  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Ke64, Ke576, sizeof(double) * 576));
+  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Ke32, f, sizeof(float) * 576));
+}
+
+static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return unsigned(b);
+}
+
+// ---------------------------------------------------------------------------
+// K*u, level 1 (Solving_KbyU_MatrixFree, TOP3D_XL.m:684-725).
+//
+// Node-centric gather: one thread per grid node owns its 3 DOFs.  A CTA
+// stages a (32+2)x(4+2)x(2+2) halo tile of u (masked by the free-DOF mask) and
+// the 33x5x3 element moduli in shared memory, then sums, for each of the 8
+// surrounding hexes, the node's 3 rows of E_e*Ke times the hex's 24 DOFs.  No
+// atomics: the result is deterministic.  The reference's per-element BC
+// matrices (uniqueKesFree_/uniqueKesFixed_) reduce exactly to
+//     y = m .* K_E (m .* u) + (1-m) .* cfix .* u
+// with m the free-DOF mask and cfix(node) = sum over its hexes of 1/nAdj.
+// The PCG mode forms the direction p = z (+ beta*p) on the fly (the update
+// kernel stores it) and reduces p'q.
+// ---------------------------------------------------------------------------
+constexpr int KTY = 32, KTX = 4, KTZ = 2;
+constexpr int KNT = KTY * KTX * KTZ;
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(KNT) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
+                                                T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
+                                                const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
+                                                PcgScalars* sc, RedScratch rs) {
+  if (MODE != KU_PLAIN && sc->done) return;
+  __shared__ T su[3][KTZ + 2][KTX + 2][KTY + 2];
+  __shared__ T sp[3][KTZ][KTX][KTY];
+  __shared__ T se[KTZ + 1][KTX + 1][KTY + 1];
+  const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
+  const int64_t S = g.stride;
+  const int y0 = blockIdx.x * KTY, x0 = blockIdx.y * KTX, z0 = blockIdx.z * KTZ;
+  const int tid = threadIdx.x + KTY * (threadIdx.y + KTX * threadIdx.z);
+  const bool first = (MODE != KU_PLAIN) && sc->first;
+  const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
+  constexpr int NSU = (KTZ + 2) * (KTX + 2) * (KTY + 2);
+  for (int i = tid; i < NSU; i += KNT) {
+    const int sy = i % (KTY + 2), r = i / (KTY + 2), sx = r % (KTX + 2), sz = r / (KTX + 2);
+    const int gy = y0 - 1 + sy, gx = x0 - 1 + sx, gz = z0 - 1 + sz;
+    T v0 = T(0), v1 = T(0), v2 = T(0);
+    if (gy >= 0 && gy < nny && gx >= 0 && gx < nnx && gz >= 0 && gz < nnz) {
+      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
+      if (MODE == KU_PLAIN) {
+        v0 = in[n];
+        v1 = in[n + S];
+        v2 = in[n + 2 * S];
+      } else if (first) {
+        v0 = zin[n];
+        v1 = zin[n + S];
+        v2 = zin[n + 2 * S];
+      } else {
+        v0 = zin[n] + beta * in[n];
+        v1 = zin[n + S] + beta * in[n + S];
+        v2 = zin[n + 2 * S] + beta * in[n + 2 * S];
+      }
+      const bool interior = sy >= 1 && sy <= KTY && sx >= 1 && sx <= KTX && sz >= 1 && sz <= KTZ;
+      if (interior) {
+        sp[0][sz - 1][sx - 1][sy - 1] = v0;
+        sp[1][sz - 1][sx - 1][sy - 1] = v1;
+        sp[2][sz - 1][sx - 1][sy - 1] = v2;
+      }
+      const uint8_t fb = fixbits[n];
+      if (fb & 1) v0 = T(0);
+      if (fb & 2) v1 = T(0);
+      if (fb & 4) v2 = T(0);
+    }
+    su[0][sz][sx][sy] = v0;
+    su[1][sz][sx][sy] = v1;
+    su[2][sz][sx][sy] = v2;
+  }
+  constexpr int NSE = (KTZ + 1) * (KTX + 1) * (KTY + 1);
+  for (int i = tid; i < NSE; i += KNT) {
+    const int sy = i % (KTY + 1), r = i / (KTY + 1), sx = r % (KTX + 1), sz = r / (KTX + 1);
+    const int ey = y0 - 1 + sy, ex = x0 - 1 + sx, ez = z0 - 1 + sz;
+    T v = T(0);
+    if (ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz)
+      v = E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)];
+    se[sz][sx][sy] = v;
+  }
+  __syncthreads();
+  const int ty = threadIdx.x, tx = threadIdx.y, tz = threadIdx.z;
+  const int gy = y0 + ty, gx = x0 + tx, gz = z0 + tz;
+  double dot = 0.0;
+  if (gy < nny && gx < nnx && gz < nnz) {
+    T acc[8][3];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const T u0 = su[0][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
+          const T u1 = su[1][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
+          const T u2 = su[2][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
+            const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
+            if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
+            const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              T s = acc[e][i];
+              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
+              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
+              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
+              acc[e][i] = s;
+            }
+          }
+        }
+    // combine the 8 hexes in the reference's local-node order
+    T y[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
+      const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
+      const T Ee = se[tz + 1 + oz][tx + 1 + ox][ty + 1 + oy];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
+    }
+    const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
+    const uint8_t fb = fixbits[n];
+    const T p0 = sp[0][tz][tx][ty], p1 = sp[1][tz][tx][ty], p2 = sp[2][tz][tx][ty];
+    if (fb) {
+      const T cf = cfix[n];
+      if (fb & 1) y[0] = cf * p0;
+      if (fb & 2) y[1] = cf * p1;
+      if (fb & 4) y[2] = cf * p2;
+    }
+    out[n] = y[0];
+    out[n + S] = y[1];
+    out[n + 2 * S] = y[2];
+    if (MODE != KU_PLAIN) dot = double(p0) * double(y[0]) + double(p1) * double(y[1]) + double(p2) * double(y[2]);
+  }
+  if (MODE != KU_PLAIN) {
+    double v[1] = {dot}, tot[1];
+    if (reduce_publish<1>(v, rs, tot) && tid == 0) sc->pq = tot[0];
+  }
+}
+
+template <typename T>
+void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
+  dim3 blk(KTY, KTX, KTZ);
+  dim3 grd((g.nny() + KTY - 1) / KTY, (g.nnx() + KTX - 1) / KTX, (g.nnz() + KTZ - 1) / KTZ);
+  if (mode == KU_PLAIN)
+    k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs);
+  else
+    k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Finest-level Jacobi diagonal (TOP3D_XL.m:1020-1050): sum over the node's
+// hexes, in local-node order, of E_e * diag(Ke); fixed DOFs take cfix; absent
+// nodes get 1 so that r./d stays 0 there.
+// ---------------------------------------------------------------------------
+template <typename TE, typename T>
+__global__ void k_diag_l1(Grid g, const TE* __restrict__ E, const uint8_t* __restrict__ fixbits,
+                          const TE* __restrict__ cfix, const uint8_t* __restrict__ present, T* __restrict__ d) {
+  const int64_t N = g.nnodes();
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    double v[3] = {1.0, 1.0, 1.0};
+    if (present[n]) {
+      const int gy = int(n % nny), gx = int((n / nny) % nnx), gz = int(n / (int64_t(nny) * nnx));
+      double s[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < 8; ++a) {
+        const int ey = gy - hex_ly(a), ex = gx - hex_lx(a), ez = gz - hex_lz(a);
+        if (ey < 0 || ey >= g.ny || ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+        const double Ee = double(E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)]);
+        for (int c = 0; c < 3; ++c) s[c] += double(ke<double>((3 * a + c) * 25)) * Ee;
+      }
+      const uint8_t fb = fixbits[n];
+      for (int c = 0; c < 3; ++c) v[c] = (fb >> c) & 1 ? double(cfix[n]) : s[c];
+    }
+    for (int c = 0; c < 3; ++c) d[n + c * g.stride] = T(v[c]);
+  }
+}
+
+template <typename TE, typename T>
+void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
+                    const uint8_t* present, T* d) {
+  k_diag_l1<TE, T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, E, fixbits, cfix, present, d);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector algebra (TOP3D_XL.m:613-622)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_residual_init(Grid g, const T* __restrict__ b, const T* __restrict__ Ay, T* __restrict__ r,
+                                PcgScalars* sc, RedScratch rs, double tol, int maxIT) {
+  const int64_t N = g.nnodes(), S = g.stride;
+  double bb = 0.0;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T bv = b[n + c * S];
+      r[n + c * S] = bv - Ay[n + c * S];
+      bb += double(bv) * double(bv);
+    }
+  }
+  double v[1] = {bb}, tot[1];
+  if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) {
+    sc->normB = sqrt(tot[0]);
+    sc->tol = tol;
+    sc->maxIT = maxIT;
+    sc->its = 0;
+    sc->done = 0;
+    sc->first = 1;
+    sc->beta = 0.0;
+  }
+}
+
+template <typename T>
+void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r, PcgScalars* sc, RedScratch rs,
+                          double tol, int maxIT) {
+  k_residual_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, Ay, r, sc, rs, tol, maxIT);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+template <typename T, typename TY>
+__global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z, T* __restrict__ p,
+                             T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs) {
+  if (sc->done) return;
+  const bool first = sc->first;
+  const T beta = T(sc->beta);
+  const double lam = sc->x1 / sc->pq;
+  const T lamT = T(lam);
+  const int64_t N = g.nnodes(), S = g.stride;
+  double rr = 0.0;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = n + c * S;
+      const T pv = first ? z[k] : z[k] + beta * p[k];
+      p[k] = pv;
+      y[k] = y[k] + TY(lam) * TY(pv);
+      const T rv = r[k] - lamT * q[k];
+      r[k] = rv;
+      rr += double(rv) * double(rv);
+    }
+  }
+  double v[1] = {rr}, tot[1];
+  if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) {
+    sc->rr = tot[0];
+    sc->resnorm = sqrt(tot[0]) / sc->normB;
+    sc->its += 1;
+    sc->first = 0;
+    if (sc->resnorm < sc->tol)
+      sc->done = 1;
+    else if (sc->its >= sc->maxIT)
+      sc->done = 2;
+  }
+}
+
+template <typename T, typename TY>
+void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
+                       RedScratch rs) {
+  k_pcg_update<T, TY><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Trilinear restriction R = P^T (Solving_RestrictResidual, TOP3D_XL.m:783-798)
+// as three separable passes (y, x, z).  Weights (S-|d|)/S are exact in binary,
+// equal to the reference's multiGridOperatorRI entries.
+// ---------------------------------------------------------------------------
+template <typename TI, typename T, int S, int AXIS>
+__global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny, int inx, int inz,
+                                T* __restrict__ out, int64_t ostr, int ony, int onx, int onz) {
+  const int64_t N = int64_t(ony) * onx * onz;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    const int oy = int(n % ony), ox = int((n / ony) % onx), oz = int(n / (int64_t(ony) * onx));
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int d = -(S - 1); d <= S - 1; ++d) {
+      int iy = oy, ix = ox, iz = oz;
+      int lim;
+      if (AXIS == 0) {
+        iy = S * oy + d;
+        lim = iny;
+      } else if (AXIS == 1) {
+        ix = S * ox + d;
+        lim = inx;
+      } else {
+        iz = S * oz + d;
+        lim = inz;
+      }
+      const int ia = AXIS == 0 ? iy : (AXIS == 1 ? ix : iz);
+      if (ia < 0 || ia >= lim) continue;
+      const T w = T(S - (d < 0 ? -d : d)) / T(S);
+      const int64_t k = iy + int64_t(iny) * (ix + int64_t(inx) * iz);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[c] = fma(w, T(in[k + c * istr]), acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[n + c * ostr] = acc[c];
+  }
+}
+
+template <typename TI, typename T>
+void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc) {
+  const int fy = gf.nny(), fx = gf.nnx(), fz = gf.nnz();
+  const int cy = gc.nny(), cx = gc.nnx(), cz = gc.nnz();
+  const int64_t s1 = int64_t(cy) * fx * fz, s2 = int64_t(cy) * cx * fz;
+  if (span == 4) {
+    k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz);
+    k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz);
+    k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
+                                                                             cx, cz);
+  } else {
+    k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz);
+    k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz);
+    k_restrict_axis<T, T, 2, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
+                                                                             cx, cz);
+  }
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Prolongation + Jacobi up-smoothing of the 'Adapted' V-cycle
+// (TOP3D_XL.m:757-778, Solving_InterpolationDeviation 800-814):
+//   x = omega*(r./d) + P*xc + (omega*r)./d   on present fine nodes.
+// The level-1 instance also reduces z'r and updates beta/x1 (TOP3D_XL.m:626-630).
+// ---------------------------------------------------------------------------
+template <typename TX, typename T, typename TD, int S, bool DOT>
+__global__ void k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __restrict__ r, const TD* __restrict__ d,
+                                 const uint8_t* __restrict__ present, T* __restrict__ x, Grid gf, T omega,
+                                 PcgScalars* sc, RedScratch rs, int init) {
+  if (DOT && sc->done) return;
+  const int64_t N = gf.nnodes();
+  const int fny = gf.nny(), fnx = gf.nnx();
+  const int cny = gc.nny(), cnx = gc.nnx();
+  double zr = 0.0;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    T v[3] = {T(0), T(0), T(0)};
+    if (present[n]) {
+      const int fy = int(n % fny), fx = int((n / fny) % fnx), fz = int(n / (int64_t(fny) * fnx));
+      const int Y = fy / S, X = fx / S, Z = fz / S;
+      const int ty = fy - S * Y, tx = fx - S * X, tz = fz - S * Z;
+      T pc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        // corner a of the coarse hex, summed in the reference's local-node order
+        const int oy = hex_ly(a), ox = hex_lx(a), oz = hex_lz(a);
+        if ((oy && ty == 0) || (ox && tx == 0) || (oz && tz == 0)) continue;
+        const T wy = oy ? T(ty) / T(S) : T(S - ty) / T(S);
+        const T wx = ox ? T(tx) / T(S) : T(S - tx) / T(S);
+        const T wz = oz ? T(tz) / T(S) : T(S - tz) / T(S);
+        const T w = wy * wx * wz;
+        const int64_t k = (Y + oy) + int64_t(cny) * ((X + ox) + int64_t(cnx) * (Z + oz));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pc[c] = fma(w, T(xc[k + c * gc.stride]), pc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T rv = r[n + c * gf.stride], dv = T(d[n + c * gf.stride]);
+        T t = omega * (rv / dv);
+        t = t + pc[c];
+        t = t + (omega * rv) / dv;
+        v[c] = t;
+        if (DOT) zr += double(t) * double(rv);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[n + c * gf.stride] = v[c];
+  }
+  if (DOT) {
+    double vv[1] = {zr}, tot[1];
+    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0) {
+      if (init) {
+        sc->x1 = tot[0];
+      } else {
+        sc->beta = tot[0] / sc->x1;
+        sc->x1 = tot[0];
+      }
+    }
+  }
+}
+
+template <typename TX, typename T, typename TD>
+void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
+                           const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
+                           PcgScalars* sc, RedScratch rs) {
+  const unsigned nb = grid1d(gf.nnodes(), 256);
+  const T w = T(omega);
+  if (span == 4) {
+    if (dot)
+      k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+    else
+      k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+  } else {
+    if (dot)
+      k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+    else
+      k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+  }
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// conversions between the reference's compact numbering and the dense grid
+// ---------------------------------------------------------------------------
+template <typename TA, typename TB>
+__global__ void k_convert(const TA* __restrict__ a, TB* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    b[i] = TB(a[i]);
+}
+template <typename TA, typename TB>
+void launch_convert(cudaStream_t st, const TA* a, TB* b, int64_t n) {
+  k_convert<TA, TB><<<grid1d(n, 256), 256, 0, st>>>(a, b, n);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// interleaved compact DOF vector (3k+c) -> SoA dense grid field
+template <typename T>
+__global__ void k_c2g_nodes(const double* __restrict__ src, T* __restrict__ dst, Grid g,
+                            const int32_t* __restrict__ nmb0, int64_t nn) {
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nn; k += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t n = nmb0[k];
+    for (int c = 0; c < 3; ++c) dst[n + c * g.stride] = T(src[3 * k + c]);
+  }
+}
+template <typename T>
+void launch_compact_to_grid_nodes(cudaStream_t st, const double* src, T* dst, Grid g, const int32_t* nodMapBack0,
+                                  int64_t numNodes) {
+  k_c2g_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+template <typename T>
+__global__ void k_g2c_nodes(const T* __restrict__ src, double* __restrict__ dst, Grid g,
+                            const int32_t* __restrict__ nmb0, int64_t nn) {
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nn; k += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t n = nmb0[k];
+    for (int c = 0; c < 3; ++c) dst[3 * k + c] = double(src[n + c * g.stride]);
+  }
+}
+template <typename T>
+void launch_grid_to_compact_nodes(cudaStream_t st, const T* src, double* dst, Grid g, const int32_t* nodMapBack0,
+                                  int64_t numNodes) {
+  k_g2c_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// SIMP moduli E = Emin + xPhys^p (E0 - Emin), compact -> dense (TOP3D_XL.m:107,116)
+__global__ void k_simp_scatter(const double* __restrict__ x, const int32_t* __restrict__ emb0, int64_t Ne,
+                               double Emin, double E0, double penal, double* __restrict__ Ed,
+                               float* __restrict__ Ef) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
+    const double v = Emin + pow(x[e], penal) * (E0 - Emin);
+    const int64_t k = emb0[e];
+    Ed[k] = v;
+    if (Ef) Ef[k] = float(v);
+  }
+}
+void launch_simp_scatter(cudaStream_t st, const double* xPhys, const int32_t* eleMapBack0, int64_t Ne, double Emin,
+                         double E0, double penal, double* Ed, float* Ef) {
+  k_simp_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(xPhys, eleMapBack0, Ne, Emin, E0, penal, Ed, Ef);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// TopOpti_ComputeUnitCompliance (TOP3D_XL.m:579-598): ce_e = u_e^T Ke u_e with the
+// unmodified Ke, one thread per element (compact order), FP64.
+__global__ void k_unit_compliance(Grid g, const double* __restrict__ U, const int32_t* __restrict__ emb0,
+                                  int64_t Ne, double w, int acc, double* __restrict__ ce) {
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t id = emb0[e];
+    const int ey = int(id % g.ny), ex = int((id / g.ny) % g.nx), ez = int(id / (int64_t(g.ny) * g.nx));
+    double u[24];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int64_t n = (ey + hex_ly(a)) + int64_t(nny) * ((ex + hex_lx(a)) + int64_t(nnx) * (ez + hex_lz(a)));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[3 * a + c] = U[n + c * g.stride];
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 24; ++j) {
+      double v = 0.0;
+#pragma unroll
+      for (int i = 0; i < 24; ++i) v = fma(u[i], c_Ke64[i * 24 + j], v);
+      s = fma(v, u[j], s);
+    }
+    ce[e] = acc ? ce[e] + w * s : w * s;
+  }
+}
+void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int32_t* eleMapBack0, int64_t Ne,
+                            double weight, bool accumulate, double* ce) {
+  k_unit_compliance<<<grid1d(Ne, 128), 128, 0, st>>>(g, U, eleMapBack0, Ne, weight, accumulate ? 1 : 0, ce);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// explicit instantiations
+#define TOPX_INST(T)                                                                                             \
+  template void launch_ku<T>(cudaStream_t, KuMode, Grid, const T*, const T*, T*, T*, const T*, const uint8_t*,   \
+                             const T*, PcgScalars*, RedScratch);                                                 \
+  template void launch_diag_l1<T, T>(cudaStream_t, Grid, const T*, const uint8_t*, const T*, const uint8_t*, T*); \
+  template void launch_residual_init<T>(cudaStream_t, Grid, const T*, const T*, T*, PcgScalars*, RedScratch,     \
+                                        double, int);                                                            \
+  template void launch_restrict<T, T>(cudaStream_t, int, const T*, Grid, T*, T*, T*, Grid);                      \
+  template void launch_prolong_smooth<T, T, T>(cudaStream_t, int, const T*, Grid, const T*, const T*,            \
+                                               const uint8_t*, T*, Grid, double, bool, bool, PcgScalars*,        \
+                                               RedScratch);                                                      \
+  template void launch_compact_to_grid_nodes<T>(cudaStream_t, const double*, T*, Grid, const int32_t*, int64_t); \
+  template void launch_grid_to_compact_nodes<T>(cudaStream_t, const T*, double*, Grid, const int32_t*, int64_t);
+TOPX_INST(double)
+TOPX_INST(float)
+template void launch_pcg_update<double, double>(cudaStream_t, Grid, double*, const double*, double*, double*,
+                                                const double*, PcgScalars*, RedScratch);
+template void launch_pcg_update<float, float>(cudaStream_t, Grid, float*, const float*, float*, float*, const float*,
+                                              PcgScalars*, RedScratch);
+template void launch_diag_l1<double, float>(cudaStream_t, Grid, const double*, const uint8_t*, const double*,
+                                           const uint8_t*, float*);
+template void launch_restrict<double, float>(cudaStream_t, int, const double*, Grid, float*, float*, float*, Grid);
+template void launch_prolong_smooth<float, double, float>(cudaStream_t, int, const float*, Grid, const double*,
+                                                          const float*, const uint8_t*, double*, Grid, double, bool,
+                                                          bool, PcgScalars*, RedScratch);
+template void launch_convert<double, float>(cudaStream_t, const double*, float*, int64_t);
+template void launch_convert<float, double>(cudaStream_t, const float*, double*, int64_t);
+template void launch_convert<double, double>(cudaStream_t, const double*, double*, int64_t);
+
+}  // namespace topx
+
+namespace topx {
+
+// E = val on every solid element (compact -> dense); the solid-domain solve of
+// TOP3D_XL.m:94-104 uses repmat(modulus_) rather than SIMP(1).
+__global__ void k_fill_scatter(const int32_t* __restrict__ emb0, int64_t Ne, double val, double* __restrict__ Ed,
+                               float* __restrict__ Ef) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
+    Ed[emb0[e]] = val;
+    if (Ef) Ef[emb0[e]] = float(val);
+  }
+}
+void launch_fill_scatter(cudaStream_t st, const int32_t* eleMapBack0, int64_t Ne, double val, double* Ed, float* Ef) {
+  k_fill_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(eleMapBack0, Ne, val, Ed, Ef);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+}  // namespace topx

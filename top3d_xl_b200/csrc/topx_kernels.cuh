@@ -1,0 +1,104 @@
+// Launch wrappers of the TOP3D_XL sm_100a kernels (all asynchronous on `st`).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "topx_device.cuh"
+
+namespace topx {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t e, const char* expr, const char* file, int line)
+      : std::runtime_error(std::string(cudaGetErrorString(e)) + " at " + file + ":" + std::to_string(line) +
+                           " (" + expr + ")"),
+        code(e) {}
+};
+
+// Dense padded grid of one multigrid level: ny, nx, nz elements; node fields
+// are SoA with plane stride `stride` (>= (ny+1)(nx+1)(nz+1)).
+struct Grid {
+  int ny = 0, nx = 0, nz = 0;
+  int64_t stride = 0;
+  __host__ __device__ int nny() const { return ny + 1; }
+  __host__ __device__ int nnx() const { return nx + 1; }
+  __host__ __device__ int nnz() const { return nz + 1; }
+  __host__ __device__ int64_t nnodes() const { return int64_t(ny + 1) * (nx + 1) * (nz + 1); }
+  __host__ __device__ int64_t nelems() const { return int64_t(ny) * nx * nz; }
+};
+
+// KU_PLAIN: out = K in.  KU_P_UPDATE: p = z (first PCG step) or z + beta*p_in,
+// out = K p, p'q reduced into sc->pq.
+enum KuMode { KU_PLAIN = 0, KU_P_UPDATE = 2 };
+
+// element matrices in constant memory
+void upload_ke(const double* Ke576);
+void upload_filter_kernel(const double* KF64, int slot);
+
+// --- level-1 elasticity --------------------------------------------------
+template <typename T>
+void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs);
+template <typename TE, typename T = TE>
+void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
+                    const uint8_t* present, T* d);
+// p = z (+ beta p); y += lambda p; r -= lambda q; ||r|| stop test into sc
+template <typename T, typename TY>
+void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
+                       RedScratch rs);
+template <typename T>
+void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r, PcgScalars* sc, RedScratch rs,
+                          double tol, int maxIT);
+// --- transfers -----------------------------------------------------------
+template <typename TI, typename T>
+void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc);
+// x = omega*(r/d) + P(xc) + (omega*r)/d on present fine nodes; with dot: z.r
+// into sc (init: x1 = z.r; else beta = z.r/x1, x1 = z.r)
+template <typename TX, typename T, typename TD>
+void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
+                           const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
+                           PcgScalars* sc, RedScratch rs);
+// --- conversions -----------------------------------------------------------
+template <typename TA, typename TB>
+void launch_convert(cudaStream_t st, const TA* a, TB* b, int64_t n);
+template <typename T>
+void launch_compact_to_grid_nodes(cudaStream_t st, const double* src, T* dst, Grid g, const int32_t* nodMapBack0,
+                                  int64_t numNodes);
+template <typename T>
+void launch_grid_to_compact_nodes(cudaStream_t st, const T* src, double* dst, Grid g, const int32_t* nodMapBack0,
+                                  int64_t numNodes);
+void launch_simp_scatter(cudaStream_t st, const double* xPhys, const int32_t* eleMapBack0, int64_t Ne, double Emin,
+                         double E0, double penal, double* Ed, float* Ef);
+void launch_fill_scatter(cudaStream_t st, const int32_t* eleMapBack0, int64_t Ne, double val, double* Ed, float* Ef);
+// ce_e = u_e^T Ke u_e (load-case weighted, accumulated into ce when accumulate)
+void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int32_t* eleMapBack0, int64_t Ne,
+                            double weight, bool accumulate, double* ce);
+
+// --- coarse levels -----------------------------------------------------------
+void launch_galerkin_l2(cudaStream_t st, Grid gc, const double* Efine, const double* Tm, double* Ks);
+void launch_galerkin_l2_flagged(cudaStream_t st, Grid gc, const double* Efine, int nflag, const int32_t* fl_elem,
+                                const int32_t* fl_tsel, const double* fl_F, const double* Tall, double* Ks);
+void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* P8,
+                           double* Ks);
+template <typename T>
+void launch_diag_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* present, T* d);
+
+// Slab block-LDL^T of the coarsest level (node grid split into slabs along `axis`)
+struct SlabInfo {
+  int axis = 0;        // 0:y 1:x 2:z
+  int ns = 0;          // number of slabs
+  int nu = 0, nv = 0;  // in-slab node dims (u varies fastest)
+  int m = 0;           // DOFs per slab = 3*nu*nv
+};
+void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks, const uint8_t* present, double* A,
+                          double* Bup);
+void launch_slab_schur(cudaStream_t st, SlabInfo si, int s, const double* Sinv_prev, const double* Bup_prev,
+                       const double* A_s, double* T, double* S_out);
+void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C);
+template <typename T>
+void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const double* Sinv, const double* Bup, const T* b,
+                       double* w, double* v, T* x, const PcgScalars* sc);
+
+}  // namespace topx
