@@ -104,8 +104,10 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def run_native(wl, precision, steps, warmup, device, profile=False, keep=False):
-    """Run `warmup` then `steps` timed OC iterations; device time via CUDA events on the engine stream."""
+def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False):
+    """Run `warmup` then `steps` timed OC iterations (device time via CUDA events on the
+    engine stream); then, if asked, `profile_steps` more iterations with per-section
+    event timing (direct launches instead of CUDA graphs, outside the timed region)."""
     from top3d_xl_b200 import Context
     ctx = Context(precision, device=device)
     vox = np.ones(wl["shape"], bool)
@@ -114,15 +116,21 @@ def run_native(wl, precision, steps, warmup, device, profile=False, keep=False):
     hist = []
     for _ in range(warmup):
         hist.append(ctx.step())
-    if profile:
-        ctx.set_profiling(True)
     ctx.timer_start()
     t0 = time.perf_counter()
     for _ in range(steps):
         hist.append(ctx.step())
     ms = ctx.timer_stop()
     wall = time.perf_counter() - t0
-    prof = ctx.profile() if profile else None
+    prof = None
+    if profile_steps:
+        ctx.set_profiling(True)
+        for _ in range(profile_steps):
+            if ctx.step() is None:
+                break
+        prof = ctx.profile()
+        prof["steps"] = profile_steps
+        ctx.set_profiling(False)
     out = dict(ms=ms, wall=wall, hist=hist, prof=prof, ne=ctx.numElements, ndof=ctx.numDOFs,
                nnodes=int(ctx.info.numNodes))
     if keep:
@@ -217,6 +225,8 @@ def main(argv=None):
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--workload", default="cuboid128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="run one precision arm only (profiling); prints its timing and exits")
     a = ap.parse_args(argv)
     wl = WORKLOADS[a.workload]
     ws, rank, local, dist, torch = dist_setup()
@@ -247,10 +257,18 @@ def main(argv=None):
         return 0
 
     device = local
+    if a.only:
+        r = run_native(wl, a.only, a.steps, a.warmup, device, profile_steps=1)
+        print(json.dumps({"only": a.only, "ms_per_step": r["ms"] / max(1, a.steps),
+                          "pcg_its": [k for h in r["hist"] for k in h["its"]],
+                          "ku_ms_per_launch": r["prof"]["ku_ms"] / max(1, r["prof"]["ku_launches"]),
+                          "sections_ms_per_profiled_step": {k: v[0] for k, v in r["prof"]["sections"].items()}}),
+              flush=True)
+        return 0
     if dist:
         dist.barrier()
     with Clocks(device) as clk:
-        mixed = run_native(wl, "mixed", a.steps, a.warmup, device, profile=True)
+        mixed = run_native(wl, "mixed", a.steps, a.warmup, device, profile_steps=2)
     ms_local = mixed["ms"]
     if dist:
         t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
@@ -280,6 +298,10 @@ def main(argv=None):
     its64 = [k for h in fp64["hist"][a.warmup:] for k in h["its"]]
     fits = [h["filter_its"] for h in mixed["hist"][a.warmup:]]
     e2e = run_e2e(wl, "mixed", max(3, a.steps // 2), 2, device)
+
+    def phases(run):
+        hs = run["hist"][a.warmup:]
+        return {k: 1000.0 * float(np.mean([h[k] for h in hs])) for k in ("t_assemble", "t_cg", "t_filter", "t_opt")}
     line = {"metric": METRIC, "value": value, "unit": "OC iterations/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 outer residual, dots, coarse solve, compliance/OC sums)",
@@ -289,6 +311,9 @@ def main(argv=None):
             "mixed_vs_fp64": {"speedup": (a.steps / (ms_local / 1000.0)) / (a.steps / (fp64["ms"] / 1000.0)),
                               "max_rel_compliance_err": relerr, "iterations_compared": n},
             "pcg_its_per_step": float(np.mean(its_mixed)), "filter_its_per_step": float(np.mean(fits)),
+            "phases_ms": {"mixed": phases(mixed), "fp64": phases(fp64)},
+            "sections_ms_per_step": {k: round(v[0] / prof["steps"], 3) for k, v in prof["sections"].items()},
+            "section_groups_per_step": {k: round(v[1] / prof["steps"], 1) for k, v in prof["sections"].items()},
             "gpu_launches": None,
             "roofline": {"kernel": "k_ku_l1<float> (level-1 K*u, PCG mode)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -160,11 +160,15 @@ topx_status topx_set_density(topx_ctx* ctx, const double* xPhys, size_t ne);
 topx_status topx_get_displacement(topx_ctx* ctx, int lc, double* out, size_t ndof);
 
 /* ---- measurement (no reference counterpart) --------------------------------- */
+#define TOPX_PROFILE_SECTIONS 14
 typedef struct topx_profile {
   double ku_ms;             /* summed device time of the level-1 K*u launches inside PCG solves */
   int64_t ku_launches;      /* launches that ran a PCG iteration */
   int64_t pcg_iterations;   /* PCG iterations since profiling was switched on */
+  double section_ms[TOPX_PROFILE_SECTIONS];     /* device time per section (see topx_profile_section_name) */
+  int64_t section_count[TOPX_PROFILE_SECTIONS]; /* timed launch groups per section */
 } topx_profile;
+const char* topx_profile_section_name(int section);
 /* CUDA-event timer on the engine's stream */
 topx_status topx_timer_start(topx_ctx* ctx);
 topx_status topx_timer_stop(topx_ctx* ctx, double* ms);

@@ -42,8 +42,12 @@ class Iter(C.Structure):
                 ("t_filter", C.c_double), ("t_total", C.c_double)]
 
 
+NSECTIONS = 14
+
+
 class Profile(C.Structure):
-    _fields_ = [("ku_ms", C.c_double), ("ku_launches", C.c_int64), ("pcg_iterations", C.c_int64)]
+    _fields_ = [("ku_ms", C.c_double), ("ku_launches", C.c_int64), ("pcg_iterations", C.c_int64),
+                ("section_ms", C.c_double * NSECTIONS), ("section_count", C.c_int64 * NSECTIONS)]
 
 
 # exported symbols and their argument types (checked by tests/test_abi.py)
@@ -83,6 +87,7 @@ SIGNATURES = {
     "topx_timer_stop": [_P, _D],
     "topx_set_profiling": [_P, C.c_int],
     "topx_get_profile": [_P, C.POINTER(Profile)],
+    "topx_profile_section_name": [C.c_int],
 }
 
 _lib = None
@@ -99,6 +104,7 @@ def load(path: str = LIB_PATH):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version") else C.c_int
+        fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version", "topx_profile_section_name") \
+            else C.c_int
     _lib = lib
     return lib

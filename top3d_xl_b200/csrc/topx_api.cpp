@@ -107,6 +107,8 @@ extern "C" {
 
 const char* topx_version(void) { return "topx 0.1 (sm_100a)"; }
 
+const char* topx_profile_section_name(int section) { return topx::Engine::section_name(section); }
+
 topx_status topx_default_params(topx_params* p) {
   if (!p) return TOPX_ERR_ARG;
   topx::Settings S;
@@ -484,6 +486,10 @@ topx_status topx_get_profile(topx_ctx* ctx, topx_profile* out) {
     out->ku_ms = ctx->engine->prof_ku_ms;
     out->ku_launches = ctx->engine->prof_ku_launches;
     out->pcg_iterations = ctx->engine->prof_pcg_its;
+    for (int i = 0; i < TOPX_PROFILE_SECTIONS && i < topx::Engine::SEC_COUNT; ++i) {
+      out->section_ms[i] = ctx->engine->sec_ms[i];
+      out->section_count[i] = ctx->engine->sec_n[i];
+    }
     return TOPX_OK;
   });
 }

@@ -3,12 +3,14 @@
 // diagonals, and the FP64 coarsest-level direct solver.
 //
 // Coarsest solver: the coarsest node grid is split into slabs (one node layer
-// each) along its longest axis, which makes K block tridiagonal:
-//     K = L D L^T,  D_s = S_s = A_s - B_{s-1}^T S_{s-1}^{-1} B_{s-1}
-// Each S_s^{-1} is formed explicitly (blocked Gauss-Jordan exchange, FP64), so
-// a coarse solve is 2*ns dense GEMVs that spread over all SMs.  This replaces
-// the reference's sparse Cholesky with fill-reducing permutation (chol(K,'lower')
-// with P, TOP3D_XL.m:1065): same exact solve, different rounding.
+// each) along its longest axis, which makes K block tridiagonal; it is
+// factorised from both ends toward the middle slab with explicit FP64 inverses
+// of the diagonal Schur complements (see launch_slab_factor), so a coarse solve
+// is ~ns dense GEMVs spread over all SMs.  This replaces the reference's sparse
+// Cholesky with fill-reducing permutation (chol(K,'lower') with P,
+// TOP3D_XL.m:1065): same exact solve, different rounding.
+#include <algorithm>
+
 #include "topx_kernels.cuh"
 
 namespace topx {
@@ -266,31 +268,74 @@ void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-// T = S_{s-1}^{-1} B_{s-1}   (m x m, B given as the stencil Bup[node a of slab s-1][9 nbrs][3][3])
-__global__ void k_schur_T(SlabInfo si, const double* __restrict__ Sinv, const double* __restrict__ Bp,
-                          double* __restrict__ T) {
+// ---------------------------------------------------------------------------
+// Twisted ("from both ends") block LDL^T of the slab-tridiagonal coarsest matrix.
+// Slabs 0..mid-1 are eliminated from the top, slabs ns-1..mid+1 from the bottom,
+// and the middle slab last, so both chains run side by side in the same
+// launches (grid dimension selects the chain) and the sequential depth halves.
+//   top:    S_s = A_s - L_{s-1} B_{s-1},        L_s = B_s^T S_s^{-1}   (s < mid)
+//   bottom: T_s = A_s - U_s B_s^T,              U_{s-1} = B_{s-1} T_s^{-1} (s > mid)
+//   middle: M   = A_mid - L_{mid-1} B_{mid-1} - U_mid B_mid^T
+// B_s couples slab s (rows) to slab s+1 (cols) and is kept as a 27-point
+// stencil Bup[node of slab s][9 neighbours][3][3].  Every diagonal inverse is
+// formed explicitly (blocked Gauss-Jordan exchange, FP64), so a solve is a
+// short chain of dense GEMVs on all SMs.
+// ---------------------------------------------------------------------------
+struct SchurOp {
+  const double* A;
+  double* S;
+  const double* Lt;  // L_{s-1} (top term), or null
+  const double* Bt;  // Bup_{s-1}
+  const double* Ub;  // U_s (bottom term), or null
+  const double* Bb;  // Bup_s
+};
+
+__global__ void k_schur(SlabInfo si, SchurOp op0, SchurOp op1) {
+  const SchurOp op = blockIdx.y == 0 ? op0 : op1;
   const int64_t m = si.m;
   const int64_t N = m * m;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
     const int64_t row = t / m, col = t % m;
-    const int b = int(col / 3), j = int(col % 3);
+    const int b = int(col / 3), jc = int(col % 3);
     const int ub = b % si.nu, vb = b / si.nu;
     double s = 0.0;
-    for (int dv = -1; dv <= 1; ++dv)
-      for (int du = -1; du <= 1; ++du) {
-        const int ua = ub - du, va = vb - dv;  // a + (du,dv) = b
-        if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
-        const int a = ua + si.nu * va;
-        const double* Bb = Bp + (int64_t(a) * 81) + ((du + 1) + 3 * (dv + 1)) * 9;
-        for (int i = 0; i < 3; ++i) s = fma(Sinv[row * m + 3 * a + i], Bb[i * 3 + j], s);
-      }
-    T[t] = s;
+    if (op.Lt) {  // (L_{s-1} B_{s-1})[row][col]: col is DOF (b, jc) of slab s, neighbours a in slab s-1
+      for (int dv = -1; dv <= 1; ++dv)
+        for (int du = -1; du <= 1; ++du) {
+          const int ua = ub - du, va = vb - dv;
+          if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
+          const int a = ua + si.nu * va;
+          const double* Bb = op.Bt + int64_t(a) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
+          for (int i = 0; i < 3; ++i) s = fma(op.Lt[row * m + 3 * a + i], Bb[i * 3 + jc], s);
+        }
+    }
+    if (op.Ub) {  // (U_s B_s^T)[row][col]: col is DOF (b, jc) of slab s, neighbours c in slab s+1
+      const double* Bc = op.Bb + int64_t(b) * 81;
+      for (int dv = -1; dv <= 1; ++dv)
+        for (int du = -1; du <= 1; ++du) {
+          const int uc = ub + du, vc = vb + dv;
+          if (uc < 0 || uc >= si.nu || vc < 0 || vc >= si.nv) continue;
+          const int c = uc + si.nu * vc;
+          const double* Bn = Bc + ((du + 1) + 3 * (dv + 1)) * 9;
+          for (int k = 0; k < 3; ++k) s = fma(op.Ub[row * m + 3 * c + k], Bn[jc * 3 + k], s);
+        }
+    }
+    op.S[t] = op.A[t] - s;
   }
 }
 
-// S = A_s - B^T T
-__global__ void k_schur_S(SlabInfo si, const double* __restrict__ Bp, const double* __restrict__ T,
-                          const double* __restrict__ As, double* __restrict__ S) {
+struct FormOp {
+  const double* Bp;    // Bup_s
+  const double* Inv;   // S_s^{-1} (kind 0) or T_{s+1}^{-1} (kind 1)
+  double* X;           // L_s (kind 0) or U_s (kind 1)
+  double* XT;          // transpose
+  int kind;
+};
+
+// kind 0: L_s = B_s^T S_s^{-1}   (rows: DOFs of slab s+1, cols: slab s)
+// kind 1: U_s = B_s T_{s+1}^{-1} (rows: DOFs of slab s,   cols: slab s+1)
+__global__ void k_form(SlabInfo si, FormOp op0, FormOp op1) {
+  const FormOp op = blockIdx.y == 0 ? op0 : op1;
   const int64_t m = si.m;
   const int64_t N = m * m;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
@@ -300,232 +345,465 @@ __global__ void k_schur_S(SlabInfo si, const double* __restrict__ Bp, const doub
     double s = 0.0;
     for (int dv = -1; dv <= 1; ++dv)
       for (int du = -1; du <= 1; ++du) {
-        const int ua = uc - du, va = vc - dv;
-        if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
-        const int a = ua + si.nu * va;
-        const double* Bb = Bp + (int64_t(a) * 81) + ((du + 1) + 3 * (dv + 1)) * 9;
-        for (int i = 0; i < 3; ++i) s = fma(Bb[i * 3 + k], T[(3 * int64_t(a) + i) * m + col], s);
+        if (op.kind == 0) {
+          const int ua = uc - du, va = vc - dv;
+          if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
+          const int a = ua + si.nu * va;
+          const double* Bb = op.Bp + int64_t(a) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
+          for (int i = 0; i < 3; ++i) s = fma(Bb[i * 3 + k], op.Inv[(3 * int64_t(a) + i) * m + col], s);
+        } else {
+          const int un = uc + du, vn = vc + dv;
+          if (un < 0 || un >= si.nu || vn < 0 || vn >= si.nv) continue;
+          const int n = un + si.nu * vn;
+          const double* Bn = op.Bp + int64_t(c) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
+          for (int q = 0; q < 3; ++q) s = fma(Bn[k * 3 + q], op.Inv[(3 * int64_t(n) + q) * m + col], s);
+        }
       }
-    S[t] = As[t] - s;
+    op.X[t] = s;
+    op.XT[col * m + row] = s;
   }
-}
-
-void launch_slab_schur(cudaStream_t st, SlabInfo si, int s, const double* Sinv_prev, const double* Bup_prev,
-                       const double* A_s, double* T, double* S_out) {
-  const int64_t N = int64_t(si.m) * si.m;
-  if (s == 0) {
-    TOPX_CUDA_OK(cudaMemcpyAsync(S_out, A_s, sizeof(double) * size_t(N), cudaMemcpyDeviceToDevice, st));
-    return;
-  }
-  k_schur_T<<<grid1d(N, 256), 256, 0, st>>>(si, Sinv_prev, Bup_prev, T);
-  k_schur_S<<<grid1d(N, 256), 256, 0, st>>>(si, Bup_prev, T, A_s, S_out);
-  TOPX_CUDA_OK(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------
-// SPD inverse in place by blocked Gauss-Jordan exchange (pivot blocks of 32).
-// One exchange step on pivot block K:  [P B; C D] -> [P^-1, -P^-1 B; C P^-1, D - C P^-1 B]
+// SPD inverse in place by blocked Gauss-Jordan exchange (pivot blocks of 64),
+// batched over up to two matrices (grid z).  One exchange step on pivot block K:
+//   [P B; C D] -> [P^-1, -P^-1 B; C P^-1, D - C P^-1 B]
 // After all blocks the matrix holds its inverse.  No pivoting is needed for SPD.
 // ---------------------------------------------------------------------------
-constexpr int GJB = 32;
+constexpr int GJB = 64;  // pivot block width (= update tile)
 
-__global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, double* __restrict__ A,
-                                                  double* __restrict__ Pinv, double* __restrict__ R,
-                                                  double* __restrict__ C) {
-  __shared__ double M[GJB][GJB + 1];
-  __shared__ double col[GJB], row[GJB];
-  const int tid = threadIdx.x;
-  for (int i = tid; i < GJB * GJB; i += 256) {
-    const int r = i / GJB, c = i % GJB;
-    M[r][c] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  for (int t = 0; t < kb; ++t) {
-    const double piv = M[t][t];
-    if (tid < GJB) {
-      col[tid] = M[tid][t];
-      row[tid] = M[t][tid];
-    }
-    __syncthreads();
-    for (int i = tid; i < GJB * GJB; i += 256) {
-      const int r = i / GJB, c = i % GJB;
-      double v;
-      if (r == t && c == t)
-        v = 1.0 / piv;
-      else if (r == t)
-        v = -row[c] / piv;
-      else if (c == t)
-        v = col[r] / piv;
-      else
-        v = M[r][c] - col[r] * row[c] / piv;
-      M[r][c] = v;
-    }
-    __syncthreads();
-  }
-  if (blockIdx.x == 0)
-    for (int i = tid; i < GJB * GJB; i += 256) Pinv[i] = M[i / GJB][i % GJB];
-  // this CTA's columns: row panel R[:, j] = -P^-1 A[K, j]; old column panel C[j, :] = A[j, K]
-  const int j = blockIdx.x * 256 + tid;
-  if (j < m && (j < k0 || j >= k0 + kb)) {
-    double a[GJB];
-#pragma unroll
-    for (int t = 0; t < GJB; ++t) a[t] = t < kb ? A[int64_t(k0 + t) * m + j] : 0.0;
-    for (int r = 0; r < kb; ++r) {
-      double s = 0.0;
-#pragma unroll
-      for (int t = 0; t < GJB; ++t) s = fma(M[r][t], a[t], s);
-      R[int64_t(r) * m + j] = -s;
-    }
-    for (int t = 0; t < kb; ++t) C[int64_t(j) * GJB + t] = A[int64_t(j) * m + k0 + t];
-  }
+struct GJSet {
+  double* A[2];
+  double* Pinv[2];
+  double* R[2];
+  double* C[2];
+};
+
+// 1/v by Newton-Raphson iteration x <- x (2 - v x) from a single-precision seed
+// (two steps: 24 -> ~48 -> full double accuracy), avoiding the long-latency
+// IEEE division on the pivot chain.
+__device__ __forceinline__ double recip_newton(double v) {
+  double x = double(1.0f / float(v));
+  x = x * (2.0 - v * x);
+  x = x * (2.0 - v * x);
+  return x;
 }
 
-__global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, double* __restrict__ A,
-                                                   const double* __restrict__ Pinv, const double* __restrict__ R,
-                                                   const double* __restrict__ C) {
-  __shared__ double sC[GJB][GJB + 1];  // rows i0..i0+31 of C (or Pinv rows), GJB cols
-  __shared__ double sR[GJB][GJB + 1];  // GJB rows of R for cols j0..j0+31
-  const int i0 = blockIdx.y * GJB, j0 = blockIdx.x * GJB;
+// pivot block P = A[K,K] -> Pinv.  One CTA of 256 threads; thread t holds row
+// t/4, columns 16*(t%4)..+15 of the block in registers; each exchange step
+// publishes the pivot row/column through double-buffered shared arrays (one
+// barrier per step).
+__global__ void __launch_bounds__(256) k_gj_pivot(int m, int k0, int kb, GJSet set) {
+  const bool z1 = blockIdx.z != 0;
+  const double* __restrict__ A = z1 ? set.A[1] : set.A[0];
+  double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
+  __shared__ double colb[2][GJB], rowb[2][GJB], rpb[2];
   const int tid = threadIdx.x;
-  const bool jK = (j0 == k0);  // column tiles are aligned to the pivot blocks
-  const bool iK = (i0 == k0);
-  for (int q = tid; q < GJB * GJB; q += 256) {
-    const int r = q / GJB, c = q % GJB;
-    const int i = i0 + r, j = j0 + c;
-    sC[r][c] = (i < m && c < kb) ? (iK ? 0.0 : C[int64_t(i) * GJB + c]) : 0.0;
-    if (jK)
-      sR[r][c] = (r < kb && c < kb) ? Pinv[r * GJB + c] : 0.0;
-    else
-      sR[r][c] = (r < kb && j < m) ? R[int64_t(r) * m + j] : 0.0;
+  const int r = tid >> 2, c0 = (tid & 3) * 16;
+  double a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int c = c0 + q;
+    a[q] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
   }
-  __syncthreads();
-  for (int q = tid; q < GJB * GJB; q += 256) {
-    const int r = q / GJB, c = q % GJB;
-    const int i = i0 + r, j = j0 + c;
-    if (i >= m || j >= m) continue;
-    double v;
-    if (iK && jK) {
-      v = Pinv[r * GJB + c];
-    } else if (iK) {
-      v = sR[r][c];
-    } else {
-      double s = 0.0;
+  for (int tb = 0; tb < GJB / 16; ++tb) {
+#pragma unroll
+    for (int qq = 0; qq < 16; ++qq) {
+      const int t = 16 * tb + qq;
+      if (t >= kb) break;
+      const int buf = t & 1;
+      if (c0 == 16 * tb) {
+        colb[buf][r] = a[qq];
+        if (r == t) rpb[buf] = recip_newton(a[qq]);
+      }
+      if (r == t) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) rowb[buf][c0 + q] = a[q];
+      }
+      __syncthreads();
+      const double rp = rpb[buf];
+      const double cr = colb[buf][r] * rp;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int c = c0 + q;
+        const double rc = rowb[buf][c];
+        double v;
+        if (r == t)
+          v = (c == t) ? rp : -rc * rp;
+        else
+          v = (c == t) ? cr : fma(-cr, rc, a[q]);
+        a[q] = v;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) Pinv[r * GJB + c0 + q] = a[q];
+}
+
+// 64x64 tile product helper: acc[4][4] += X[rows 4ty..][t] * Y[t][cols 4tx..] over 32 values of t
+__device__ __forceinline__ void tile_fma(const double (*sX)[33], const double (*sY)[68], int ty, int tx,
+                                         double (&acc)[4][4]) {
 #pragma unroll 8
-      for (int t = 0; t < GJB; ++t) s = fma(sC[r][t], sR[t][c], s);
-      v = jK ? s : A[int64_t(i) * m + j] + s;
-    }
-    A[int64_t(i) * m + j] = v;
+  for (int t = 0; t < 32; ++t) {
+    double xv[4], yv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) xv[q] = sX[4 * ty + q][t];
+    const double2 y01 = *reinterpret_cast<const double2*>(&sY[t][4 * tx]);
+    const double2 y23 = *reinterpret_cast<const double2*>(&sY[t][4 * tx + 2]);
+    yv[0] = y01.x;
+    yv[1] = y01.y;
+    yv[2] = y23.x;
+    yv[3] = y23.y;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) acc[q][w] = fma(xv[q], yv[w], acc[q][w]);
   }
 }
 
-void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C) {
+// row panel R[:, j] = -Pinv A[K, j] (j not in K): CTA (x: 64 columns, y: 16 of the kb rows),
+// and the old column panel C[j, :] = A[j, K] for 16 of the CTA's 64 rows
+__global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet set) {
+  const bool z1 = blockIdx.z != 0;
+  const double* __restrict__ A = z1 ? set.A[1] : set.A[0];
+  const double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
+  double* __restrict__ R = z1 ? set.R[1] : set.R[0];
+  double* __restrict__ C = z1 ? set.C[1] : set.C[0];
+  __shared__ double sP[16][GJB + 1];
+  __shared__ __align__(16) double sA[GJB][68];
+  const int tid = threadIdx.x;
+  const int j0 = blockIdx.x * GJB, r0 = blockIdx.y * 16;
+  for (int i = tid; i < 16 * GJB; i += 256) sP[i / GJB][i % GJB] = Pinv[(r0 + i / GJB) * GJB + i % GJB];
+  for (int i = tid; i < GJB * GJB; i += 256) {
+    const int t = i / GJB, cc = i % GJB;
+    const int j = j0 + cc;
+    sA[t][cc] = (t < kb && j < m) ? A[int64_t(k0 + t) * m + j] : 0.0;
+  }
+  __syncthreads();
+  const int rr = tid >> 4, cx = (tid & 15) * 4;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t = 0; t < kb; ++t) {
+    const double p = sP[rr][t];
+    const double2 a01 = *reinterpret_cast<const double2*>(&sA[t][cx]);
+    const double2 a23 = *reinterpret_cast<const double2*>(&sA[t][cx + 2]);
+    acc[0] = fma(p, a01.x, acc[0]);
+    acc[1] = fma(p, a01.y, acc[1]);
+    acc[2] = fma(p, a23.x, acc[2]);
+    acc[3] = fma(p, a23.y, acc[3]);
+  }
+  if (r0 + rr < kb) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int j = j0 + cx + w;
+      if (j < m && (j < k0 || j >= k0 + kb)) R[int64_t(r0 + rr) * m + j] = -acc[w];
+    }
+  }
+  for (int i = tid; i < 16 * GJB; i += 256) {
+    const int row = j0 + r0 + i / GJB, t = i % GJB;
+    if (row < m && (row < k0 || row >= k0 + kb) && t < kb) C[int64_t(row) * GJB + t] = A[int64_t(row) * m + k0 + t];
+  }
+}
+
+// rank-kb exchange update of every 64x64 tile (4x4 outputs per thread)
+__global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, GJSet set) {
+  const bool z1 = blockIdx.z != 0;
+  double* __restrict__ A = z1 ? set.A[1] : set.A[0];
+  const double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
+  const double* __restrict__ R = z1 ? set.R[1] : set.R[0];
+  const double* __restrict__ C = z1 ? set.C[1] : set.C[0];
+  __shared__ double sX[GJB][33];
+  __shared__ __align__(16) double sY[32][68];
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int i0 = blockIdx.y * GJB, j0 = blockIdx.x * GJB;
+  const bool iK = (i0 == k0), jK = (j0 == k0);
+  if (iK) {  // rows of the pivot block: new row panel / Pinv
+    for (int i = tid; i < GJB * GJB; i += 256) {
+      const int rr = i / GJB, cc = i % GJB;
+      const int ii = i0 + rr, j = j0 + cc;
+      if (rr < kb && j < m) A[int64_t(ii) * m + j] = jK ? Pinv[rr * GJB + cc] : R[int64_t(rr) * m + j];
+    }
+    return;
+  }
+  double acc[4][4] = {};
+  for (int h = 0; h < 2; ++h) {
+    for (int i = tid; i < GJB * 32; i += 256) {
+      const int rr = i / 32, t = i % 32;
+      const int ii = i0 + rr, kt = 32 * h + t;
+      sX[rr][t] = (ii < m && kt < kb) ? C[int64_t(ii) * GJB + kt] : 0.0;
+    }
+    for (int i = tid; i < 32 * GJB; i += 256) {
+      const int t = i / GJB, cc = i % GJB;
+      const int kt = 32 * h + t, j = j0 + cc;
+      double v = 0.0;
+      if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + cc] : R[int64_t(kt) * m + j];
+      sY[t][cc] = v;
+    }
+    __syncthreads();
+    tile_fma(sX, sY, ty, tx, acc);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int ii = i0 + 4 * ty + q;
+    if (ii >= m) continue;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int j = j0 + 4 * tx + w;
+      if (j >= m) continue;
+      const int64_t k = int64_t(ii) * m + j;
+      A[k] = jK ? acc[q][w] : A[k] + acc[q][w];
+    }
+  }
+}
+
+static void spd_inverse_batched(cudaStream_t st, int m, int nset, const GJSet& set) {
   const unsigned nt = (m + GJB - 1) / GJB;
   for (int k0 = 0; k0 < m; k0 += GJB) {
     const int kb = (m - k0) < GJB ? (m - k0) : GJB;
-    k_gj_panel<<<(m + 255) / 256, 256, 0, st>>>(m, k0, kb, A, Pinv, R, C);
-    k_gj_update<<<dim3(nt, nt), 256, 0, st>>>(m, k0, kb, A, Pinv, R, C);
+    k_gj_pivot<<<dim3(1, 1, nset), 256, 0, st>>>(m, k0, kb, set);
+    k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set);
+    k_gj_update<<<dim3(nt, nt, nset), 256, 0, st>>>(m, k0, kb, set);
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-// ---------------------------------------------------------------------------
-// coarse solve x = K^{-1} b with the slab LDL^T (TOP3D_XL.m:767)
-//   forward:  w_s = b_s - B_{s-1}^T v_{s-1},  v_s = S_s^{-1} w_s
-//   backward: x_s = S_s^{-1} (w_s - B_s x_{s+1})
-// One launch per slab step; each CTA forms the full right-hand side in shared
-// memory and computes a block of rows (one warp per row).
-// ---------------------------------------------------------------------------
-constexpr int SLAB_MAXM = 4096;
+void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C) {
+  GJSet set{{A, A}, {Pinv, Pinv}, {R, R}, {C, C}};
+  spd_inverse_batched(st, m, 1, set);
+}
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_slab_step(Grid g, SlabInfo si, int s, int fwd,
-                                                    const double* __restrict__ Sinv, const double* __restrict__ Bup,
-                                                    const T* __restrict__ b, double* __restrict__ w,
-                                                    double* __restrict__ v, double* __restrict__ xs, T* __restrict__ x,
-                                                    const PcgScalars* sc) {
-  if (sc && sc->done) return;
-  extern __shared__ double rhs[];
-  const int m = si.m;
-  const int nny = g.ny + 1, nnx = g.nx + 1;
-  const int tid = threadIdx.x;
-  for (int row = tid; row < m; row += 256) {
-    const int c = row / 3, k = row % 3;
-    const int uc = c % si.nu, vc = c / si.nu;
-    double val;
-    if (fwd) {
-      int gy, gx, gz;
-      slab_node(g, si, s, uc, vc, gy, gx, gz);
-      val = double(b[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride]);
-      if (s > 0) {  // - B_{s-1}^T v_{s-1}
-        const double* Bp = Bup + int64_t(s - 1) * si.nu * si.nv * 81;
-        const double* vp = v + int64_t(s - 1) * m;
-        for (int dv = -1; dv <= 1; ++dv)
-          for (int du = -1; du <= 1; ++du) {
-            const int ua = uc - du, va = vc - dv;
-            if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
-            const int a = ua + si.nu * va;
-            const double* Bb = Bp + int64_t(a) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
-            for (int i = 0; i < 3; ++i) val -= Bb[i * 3 + k] * vp[3 * a + i];
-          }
-      }
-      if (blockIdx.x == 0) w[int64_t(s) * m + row] = val;
-    } else {
-      val = w[int64_t(s) * m + row];
-      if (s < si.ns - 1) {  // - B_s x_{s+1}
-        const double* Bs = Bup + int64_t(s) * si.nu * si.nv * 81 + int64_t(c) * 81;
-        const double* xp = xs + int64_t(s + 1) * m;
-        for (int dv = -1; dv <= 1; ++dv)
-          for (int du = -1; du <= 1; ++du) {
-            const int ub = uc + du, vb = vc + dv;
-            if (ub < 0 || ub >= si.nu || vb < 0 || vb >= si.nv) continue;
-            const double* Bb = Bs + ((du + 1) + 3 * (dv + 1)) * 9;
-            const int b2 = ub + si.nu * vb;
-            for (int j = 0; j < 3; ++j) val -= Bb[k * 3 + j] * xp[3 * b2 + j];
-          }
-      }
-    }
-    rhs[row] = val;
+void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const double* Bup, double* Sinv, double* X,
+                        double* XT, double* gj_scratch) {
+  const int m = si.m, ns = si.ns, mid = ns / 2;
+  const int64_t mm = int64_t(m) * m;
+  const int64_t bs = int64_t(si.nu) * si.nv * 81;
+  const unsigned nbm = grid1d(mm, 256);
+  // per chain scratch: Pinv 64x64, R 64xm, C mx64
+  const int64_t gjs = 64 * 64 + 2 * 64 * int64_t(m);
+  GJSet set{};
+  for (int c = 0; c < 2; ++c) {
+    set.Pinv[c] = gj_scratch + c * gjs;
+    set.R[c] = set.Pinv[c] + 64 * 64;
+    set.C[c] = set.R[c] + 64 * int64_t(m);
   }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31;
-  const double* Sm = Sinv + int64_t(s) * m * m;
-  for (int row = blockIdx.x * 8 + warp; row < m; row += gridDim.x * 8) {
-    double acc = 0.0;
-    for (int j = lane; j < m; j += 32) acc = fma(Sm[int64_t(row) * m + j], rhs[j], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) {
-      if (fwd) {
-        v[int64_t(s) * m + row] = acc;
-      } else {
-        xs[int64_t(s) * m + row] = acc;
-        const int c = row / 3, k = row % 3;
-        int gy, gx, gz;
-        slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
-        x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(acc);
-      }
+  const int ntop = mid, nbot = ns - 1 - mid;
+  for (int k = 0; k < std::max(ntop, nbot); ++k) {
+    SchurOp so[2] = {};
+    FormOp fo[2] = {};
+    int nset = 0, nform = 0;
+    if (k < ntop) {  // top slab k
+      const int s = k;
+      so[nset] = SchurOp{A + s * mm, Sinv + s * mm, s ? X + (s - 1) * mm : nullptr, s ? Bup + (s - 1) * bs : nullptr,
+                         nullptr, nullptr};
+      set.A[nset] = Sinv + s * mm;
+      ++nset;
     }
+    if (k < nbot) {  // bottom slab ns-1-k
+      const int s = ns - 1 - k;
+      so[nset] = SchurOp{A + s * mm, Sinv + s * mm, nullptr, nullptr, k ? X + s * mm : nullptr, k ? Bup + s * bs : nullptr};
+      set.A[nset] = Sinv + s * mm;
+      ++nset;
+    }
+    k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]);
+    spd_inverse_batched(st, m, nset, set);
+    if (k < ntop) {  // L_k = B_k^T S_k^{-1}
+      fo[nform++] = FormOp{Bup + k * bs, Sinv + k * mm, X + k * mm, XT + k * mm, 0};
+    }
+    if (k < nbot) {  // U_{s-1} = B_{s-1} T_s^{-1}, s = ns-1-k
+      const int s = ns - 1 - k;
+      fo[nform++] = FormOp{Bup + (s - 1) * bs, Sinv + s * mm, X + (s - 1) * mm, XT + (s - 1) * mm, 1};
+    }
+    if (nform) k_form<<<dim3(nbm, nform), 256, 0, st>>>(si, fo[0], fo[1]);
+  }
+  // middle slab
+  SchurOp sm{A + mid * mm, Sinv + mid * mm, mid > 0 ? X + (mid - 1) * mm : nullptr,
+             mid > 0 ? Bup + (mid - 1) * bs : nullptr, mid < ns - 1 ? X + mid * mm : nullptr,
+             mid < ns - 1 ? Bup + mid * bs : nullptr};
+  k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm);
+  set.A[0] = Sinv + mid * mm;
+  spd_inverse_batched(st, m, 1, set);
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// coarse solve x = K^{-1} b with the twisted slab factorization (TOP3D_XL.m:767)
+//   forward:  W_0 = b_0,  W_{s+1} = b_{s+1} - L_s W_s            (s+1 < mid)
+//             W_{ns-1} = b_{ns-1},  W_s = b_s - U_s W_{s+1}      (s > mid)
+//             W_mid = b_mid - L_{mid-1} W_{mid-1} - U_mid W_{mid+1}
+//   all s:    V_s = Inv_s W_s                                     (one batched launch)
+//   backward: x_mid = V_mid,  x_s = V_s - L_s^T x_{s+1} (s < mid),  x_s = V_s - U_{s-1}^T x_{s-1} (s > mid)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_slab_gather(Grid g, SlabInfo si, const T* __restrict__ b, double* __restrict__ bs,
+                              const PcgScalars* sc) {
+  if (sc && sc->done) return;
+  const int64_t N = int64_t(si.ns) * si.m;
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
+    const int s = int(t / si.m), row = int(t % si.m);
+    const int c = row / 3, k = row % 3;
+    int gy, gx, gz;
+    slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
+    bs[t] = double(b[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride]);
   }
 }
 
 template <typename T>
-void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const double* Sinv, const double* Bup, const T* b,
-                       double* w, double* v, T* x, const PcgScalars* sc) {
-  if (si.m > SLAB_MAXM) throw std::runtime_error("coarsest slab too large");
-  const unsigned nb = unsigned((si.m + 7) / 8);
-  const size_t sh = sizeof(double) * size_t(si.m);
-  double* xs = v + int64_t(si.ns) * si.m;  // second half of the v buffer
-  for (int s = 0; s < si.ns; ++s)
-    k_slab_step<T><<<nb, 256, sh, st>>>(g, si, s, 1, Sinv, Bup, b, w, v, xs, x, sc);
-  for (int s = si.ns - 1; s >= 0; --s)
-    k_slab_step<T><<<nb, 256, sh, st>>>(g, si, s, 0, Sinv, Bup, b, w, v, xs, x, sc);
+__global__ void k_slab_scatter(Grid g, SlabInfo si, const double* __restrict__ xs, T* __restrict__ x,
+                               const PcgScalars* sc) {
+  if (sc && sc->done) return;
+  const int64_t N = int64_t(si.ns) * si.m;
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
+    const int s = int(t / si.m), row = int(t % si.m);
+    const int c = row / 3, k = row % 3;
+    int gy, gx, gz;
+    slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
+    x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(xs[t]);
+  }
+}
+
+// y = a - M1 u1 - M2 u2 (M2 optional; a optional: y = M1 u1) over `nmat` stacked m x m blocks
+// (u, a, y stacked alike).  Two rows per CTA, four warps per row, four independent
+// accumulators per lane; grid y selects one of two independent operations.
+struct GemvOp {
+  const void* M1;
+  const double* u1;
+  const void* M2;
+  const double* u2;
+  const double* a;
+  double* y;
+  int nmat;
+};
+
+template <typename TM>
+__device__ __forceinline__ double row_dot(const TM* __restrict__ Mr, const double* __restrict__ u, int j0, int j1,
+                                          int lane) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int jj = j0 + lane;
+  for (; jj + 96 < j1; jj += 128) {
+    a0 = fma(double(Mr[jj]), u[jj], a0);
+    a1 = fma(double(Mr[jj + 32]), u[jj + 32], a1);
+    a2 = fma(double(Mr[jj + 64]), u[jj + 64], a2);
+    a3 = fma(double(Mr[jj + 96]), u[jj + 96], a3);
+  }
+  for (; jj < j1; jj += 32) a0 = fma(double(Mr[jj]), u[jj], a0);
+  return (a0 + a1) + (a2 + a3);
+}
+
+template <typename TM>
+__global__ void __launch_bounds__(256) k_slab_gemv(int m, GemvOp op0, GemvOp op1, const PcgScalars* sc) {
+  if (sc && sc->done) return;
+  const GemvOp op = blockIdx.y == 0 ? op0 : op1;
+  __shared__ double part[2][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rsub = warp >> 2, q = warp & 3;
+  const int64_t rows = int64_t(m) * op.nmat;
+  const int chunk = (m + 3) / 4;
+  const int j0 = q * chunk, j1 = min(m, (q + 1) * chunk);
+  for (int64_t r0 = int64_t(blockIdx.x) * 2; r0 < rows; r0 += int64_t(gridDim.x) * 2) {
+    const int64_t r = r0 + rsub;
+    double acc = 0.0;
+    if (r < rows) {
+      const int64_t blk = r / m;
+      acc = row_dot<TM>(static_cast<const TM*>(op.M1) + r * m, op.u1 + blk * m, j0, j1, lane);
+      if (op.M2) acc += row_dot<TM>(static_cast<const TM*>(op.M2) + r * m, op.u2 + blk * m, j0, j1, lane);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) part[rsub][q] = acc;
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int64_t rr = r0 + threadIdx.x;
+      if (rr < rows) {
+        const double sum =
+            (part[threadIdx.x][0] + part[threadIdx.x][1]) + (part[threadIdx.x][2] + part[threadIdx.x][3]);
+        op.y[rr] = op.a ? op.a[rr] - sum : sum;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, typename TM>
+void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT,
+                       const T* b, double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc) {
+  const int m = si.m, ns = si.ns, mid = ns / 2;
+  const int64_t mm = int64_t(m) * m;
+  const int64_t N = int64_t(ns) * m;
+  const int ntop = mid, nbot = ns - 1 - mid;
+  const unsigned nb1 = unsigned((m + 1) / 2);
+  k_slab_gather<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, b, bs, sc);
+  // chain heads
+  if (ntop > 0) TOPX_CUDA_OK(cudaMemcpyAsync(W, bs, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+  if (nbot > 0)
+    TOPX_CUDA_OK(cudaMemcpyAsync(W + int64_t(ns - 1) * m, bs + int64_t(ns - 1) * m, sizeof(double) * m,
+                                 cudaMemcpyDeviceToDevice, st));
+  // forward chains toward the middle
+  for (int k = 0; k + 1 < std::max(ntop, nbot); ++k) {
+    GemvOp ops[2] = {};
+    int n = 0;
+    if (k + 1 < ntop)
+      ops[n++] = GemvOp{X + k * mm, W + int64_t(k) * m, nullptr, nullptr, bs + int64_t(k + 1) * m,
+                        W + int64_t(k + 1) * m, 1};
+    if (k + 1 < nbot) {
+      const int s = ns - 2 - k;  // W_s = b_s - U_s W_{s+1}
+      ops[n++] = GemvOp{X + s * mm, W + int64_t(s + 1) * m, nullptr, nullptr, bs + int64_t(s) * m,
+                        W + int64_t(s) * m, 1};
+    }
+    k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc);
+  }
+  {  // middle
+    GemvOp op{nullptr, nullptr, nullptr, nullptr, bs + int64_t(mid) * m, W + int64_t(mid) * m, 1};
+    if (ntop > 0) {
+      op.M1 = X + (mid - 1) * mm;
+      op.u1 = W + int64_t(mid - 1) * m;
+    }
+    if (nbot > 0) {
+      if (op.M1) {
+        op.M2 = X + mid * mm;
+        op.u2 = W + int64_t(mid + 1) * m;
+      } else {
+        op.M1 = X + mid * mm;
+        op.u1 = W + int64_t(mid + 1) * m;
+      }
+    }
+    if (op.M1)
+      k_slab_gemv<TM><<<dim3(nb1, 1), 256, 0, st>>>(m, op, op, sc);
+    else
+      TOPX_CUDA_OK(cudaMemcpyAsync(W + int64_t(mid) * m, bs + int64_t(mid) * m, sizeof(double) * m,
+                                   cudaMemcpyDeviceToDevice, st));
+  }
+  GemvOp ov{Inv, W, nullptr, nullptr, nullptr, V, ns};
+  k_slab_gemv<TM><<<dim3(grid1d(N / 2 + 1, 1, 148 * 32), 1), 256, 0, st>>>(m, ov, ov, sc);
+  TOPX_CUDA_OK(cudaMemcpyAsync(xs + int64_t(mid) * m, V + int64_t(mid) * m, sizeof(double) * m,
+                               cudaMemcpyDeviceToDevice, st));
+  // backward chains outward from the middle
+  for (int k = 0; k < std::max(ntop, nbot); ++k) {
+    GemvOp ops[2] = {};
+    int n = 0;
+    if (k < ntop) {
+      const int s = mid - 1 - k;  // x_s = V_s - L_s^T x_{s+1}
+      ops[n++] = GemvOp{XT + s * mm, xs + int64_t(s + 1) * m, nullptr, nullptr, V + int64_t(s) * m,
+                        xs + int64_t(s) * m, 1};
+    }
+    if (k < nbot) {
+      const int s = mid + 1 + k;  // x_s = V_s - U_{s-1}^T x_{s-1}
+      ops[n++] = GemvOp{XT + (s - 1) * mm, xs + int64_t(s - 1) * m, nullptr, nullptr, V + int64_t(s) * m,
+                        xs + int64_t(s) * m, 1};
+    }
+    k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc);
+  }
+  k_slab_scatter<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, xs, x, sc);
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
 template void launch_diag_coarse<double>(cudaStream_t, Grid, const double*, const uint8_t*, double*);
 template void launch_diag_coarse<float>(cudaStream_t, Grid, const double*, const uint8_t*, float*);
-template void launch_slab_solve<double>(cudaStream_t, Grid, SlabInfo, const double*, const double*, const double*,
-                                        double*, double*, double*, const PcgScalars*);
-template void launch_slab_solve<float>(cudaStream_t, Grid, SlabInfo, const double*, const double*, const float*,
-                                       double*, double*, float*, const PcgScalars*);
+template void launch_slab_solve<double, double>(cudaStream_t, Grid, SlabInfo, const double*, const double*,
+                                                const double*, const double*, double*, double*, double*, double*,
+                                                double*, const PcgScalars*);
+template void launch_slab_solve<float, float>(cudaStream_t, Grid, SlabInfo, const float*, const float*, const float*,
+                                              const float*, double*, double*, double*, double*, float*,
+                                              const PcgScalars*);
 
 }  // namespace topx

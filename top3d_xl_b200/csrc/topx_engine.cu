@@ -4,10 +4,12 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <sstream>
 #include <stdexcept>
+#include <type_traits>
 
 namespace topx {
 
@@ -192,15 +194,19 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
     si.m = 3 * si.nu * si.nv;
     if (si.m > 4096) throw std::runtime_error("coarsest level too large for the slab solver");
     const size_t mm = size_t(si.m) * si.m;
+    const size_t nsm1 = size_t(std::max(1, si.ns - 1));
     slabA.alloc(mm * si.ns);
     slabSinv.alloc(mm * si.ns);
-    slabBup.alloc(size_t(si.nu) * si.nv * 81 * std::max(1, si.ns - 1));
-    slabT.alloc(mm);
-    gjP.alloc(32 * 32);
-    gjR.alloc(size_t(32) * si.m);
-    gjC.alloc(size_t(si.m) * 32);
-    slabW.alloc(size_t(si.m) * si.ns);
-    slabV.alloc(size_t(si.m) * si.ns * 2);
+    slabL.alloc(mm * nsm1);
+    slabLT.alloc(mm * nsm1);
+    if (prec == PREC_MIXED) {
+      slabSinv32.alloc(mm * si.ns);
+      slabL32.alloc(mm * nsm1);
+      slabLT32.alloc(mm * nsm1);
+    }
+    slabBup.alloc(size_t(si.nu) * si.nv * 81 * nsm1);
+    gjP.alloc(2 * (64 * 64 + size_t(128) * si.m));
+    for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
   }
   // ---- workspaces ------------------------------------------------------------
   {
@@ -251,6 +257,12 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
     TOPX_CUDA_OK(cudaEventCreate(&e));
     pev.push_back(e);
   }
+  for (int i = 0; i < 4096; ++i) {
+    cudaEvent_t e;
+    TOPX_CUDA_OK(cudaEventCreate(&e));
+    sev.push_back(e);
+  }
+  sec_of.assign(sev.size() / 2, 0);
   std::ostringstream os;
   os << "levels=" << nl;
   for (int l = 0; l < nl; ++l) os << " L" << (l + 1) << "=" << G[l].nx << "x" << G[l].ny << "x" << G[l].nz;
@@ -260,7 +272,9 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
 }
 
 Engine::~Engine() {
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   for (auto e : ev) cudaEventDestroy(e);
+  for (auto e : sev) cudaEventDestroy(e);
   for (auto e : pev) cudaEventDestroy(e);
   for (auto e : tev)
     if (e) cudaEventDestroy(e);
@@ -340,31 +354,46 @@ void Engine::update_moduli(const double* d_xPhys, bool solid) {
 // Solving_AssembleFEAstencil (TOP3D_XL.m:919-1066)
 // ---------------------------------------------------------------------------
 void Engine::assemble() {
+  run_graph("assemble", [&]() { assemble_launches(); });
+  sec_harvest();
+}
+
+void Engine::assemble_launches() {
+  sec_begin(SEC_DIAG);
   if (prec == PREC_FP64)
     launch_diag_l1<double>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v64.d1.p);
   else
     launch_diag_l1<double, float>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v32.d1.p);
+  sec_end();
+  sec_begin(SEC_GALERKIN2);
   launch_galerkin_l2(st, G[1], E64.p, Tall.p, Ks[1].p);
   launch_galerkin_l2_flagged(st, G[1], E64.p, nflag, fl_elem.p, fl_tsel.p, fl_F.p, Tall.p, Ks[1].p);
+  sec_end();
+  sec_begin(SEC_GALERKIN3);
   for (int l = 2; l < nl; ++l) launch_galerkin_span2(st, G[l], Ks[l - 1].p, epresent[l].p, P8.p, Ks[l].p);
+  sec_end();
+  sec_begin(SEC_DIAG);
   for (int l = 1; l < nl - 1; ++l) {
     if (prec == PREC_FP64)
       launch_diag_coarse<double>(st, G[l], Ks[l].p, present[l].p, v64.dl[l].p);
     else
       launch_diag_coarse<float>(st, G[l], Ks[l].p, present[l].p, v32.dl[l].p);
   }
+  sec_end();
   factor_coarsest();
 }
 
 void Engine::factor_coarsest() {
+  sec_begin(SEC_SLAB_ASSEMBLE);
   launch_slab_assemble(st, G[nl - 1], si, Ks[nl - 1].p, present[nl - 1].p, slabA.p, slabBup.p);
-  const size_t mm = size_t(si.m) * si.m;
-  const size_t bs = size_t(si.nu) * si.nv * 81;
-  for (int s = 0; s < si.ns; ++s) {
-    double* Sinv = slabSinv.p + s * mm;
-    launch_slab_schur(st, si, s, s ? slabSinv.p + (s - 1) * mm : nullptr, s ? slabBup.p + (s - 1) * bs : nullptr,
-                      slabA.p + s * mm, slabT.p, Sinv);
-    launch_spd_inverse(st, si.m, Sinv, gjP.p, gjR.p, gjC.p);
+  sec_end();
+  sec_begin(SEC_INVERSE);
+  launch_slab_factor(st, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p, gjP.p);
+  sec_end();
+  if (prec == PREC_MIXED) {
+    launch_convert<double, float>(st, slabSinv.p, slabSinv32.p, int64_t(slabSinv.n));
+    launch_convert<double, float>(st, slabL.p, slabL32.p, int64_t(slabL.n));
+    launch_convert<double, float>(st, slabLT.p, slabLT32.p, int64_t(slabLT.n));
   }
 }
 
@@ -373,17 +402,28 @@ void Engine::factor_coarsest() {
 // ---------------------------------------------------------------------------
 template <typename TC>
 void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
+  sec_begin(SEC_RESTRICT);
   launch_restrict<double, TC>(st, M.levels[1].span, kw.r.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
   for (int l = 2; l < nl; ++l)
     launch_restrict<TC, TC>(st, M.levels[l].span, v.rl[l - 1].p, G[l - 1], v.tmp1.p, v.tmp2.p, v.rl[l].p, G[l]);
-  launch_slab_solve<TC>(st, G[nl - 1], si, slabSinv.p, slabBup.p, v.rl[nl - 1].p, slabW.p, slabV.p,
-                        v.xl[nl - 1].p, sc);
+  sec_end();
+  sec_begin(SEC_COARSE_SOLVE);
+  if (std::is_same<TC, double>::value)
+    launch_slab_solve<TC, TC>(st, G[nl - 1], si, (const TC*)slabSinv.p, (const TC*)slabL.p, (const TC*)slabLT.p,
+                              v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc);
+  else
+    launch_slab_solve<TC, TC>(st, G[nl - 1], si, (const TC*)slabSinv32.p, (const TC*)slabL32.p,
+                              (const TC*)slabLT32.p, v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p,
+                              v.xl[nl - 1].p, sc);
+  sec_end();
+  sec_begin(SEC_PROLONG);
   const double om = M.S.weightFactorJacobi;
   for (int l = nl - 2; l >= 1; --l)
     launch_prolong_smooth<TC, TC, TC>(st, M.levels[l + 1].span, v.xl[l + 1].p, G[l + 1], v.rl[l].p, v.dl[l].p,
                                       present[l].p, v.xl[l].p, G[l], om, false, false, sc, rs1);
   launch_prolong_smooth<TC, double, TC>(st, M.levels[1].span, v.xl[1].p, G[1], kw.r.p, v.d1.p, present[0].p,
                                         kw.z.p, G[0], om, true, init, sc, rs1);
+  sec_end();
 }
 
 void Engine::vcycle(bool init, PcgScalars* sc) {
@@ -399,22 +439,43 @@ void Engine::vcycle(bool init, PcgScalars* sc) {
 int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
   const Grid& g = G[0];
   PcgScalars* sc = scE.p;
-  if (warm)
-    launch_ku<double>(st, KU_PLAIN, g, y, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
-  else
-    TOPX_CUDA_OK(cudaMemsetAsync(kw.q.p, 0, kw.q.bytes(), st));
-  launch_residual_init<double>(st, g, b, kw.q.p, kw.r.p, sc, rs1, tol, maxIT);
-  vcycle(true, sc);
+  char key[96];
+  std::snprintf(key, sizeof(key), "pcg_init:%p:%p:%d:%.17g:%d", (const void*)b, (const void*)y, int(warm), tol, maxIT);
+  run_graph(key, [&]() {
+    if (warm)
+      launch_ku<double>(st, KU_PLAIN, g, y, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+    else
+      TOPX_CUDA_OK(cudaMemsetAsync(kw.q.p, 0, kw.q.bytes(), st));
+    launch_residual_init<double>(st, g, b, kw.q.p, kw.r.p, sc, rs1, tol, maxIT);
+    vcycle(true, sc);
+  });
   const int CH = 8;
   PcgScalars h{};
   int launched = 0;
+  std::snprintf(key, sizeof(key), "pcg_chunk:%p:%p", (const void*)b, (const void*)y);
   while (launched < maxIT) {
     const int first = launched;
+    if (!prof_ && use_graphs && launched + CH <= maxIT) {
+      run_graph(key, [&]() {
+        for (int c = 0; c < CH; ++c) {
+          launch_ku<double>(st, KU_P_UPDATE, g, kw.p.p, kw.z.p, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc,
+                            rs1);
+          launch_pcg_update<double, double>(st, g, y, kw.z.p, kw.p.p, kw.r.p, kw.q.p, sc, rs1);
+          vcycle(false, sc);
+        }
+      });
+      launched += CH;
+      read_scalars(h, sc);
+      if (h.done) break;
+      continue;
+    }
     for (int c = 0; c < CH && launched < maxIT; ++c, ++launched) {
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c], st));
       launch_ku<double>(st, KU_P_UPDATE, g, kw.p.p, kw.z.p, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
+      sec_begin(SEC_UPDATE);
       launch_pcg_update<double, double>(st, g, y, kw.z.p, kw.p.p, kw.r.p, kw.q.p, sc, rs1);
+      sec_end();
       vcycle(false, sc);
     }
     read_scalars(h, sc);
@@ -425,7 +486,10 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
         TOPX_CUDA_OK(cudaEventElapsedTime(&ms, pev[2 * c], pev[2 * c + 1]));
         prof_ku_ms += ms;
         prof_ku_launches += 1;
+        sec_ms[SEC_KU] += ms;
+        sec_n[SEC_KU] += 1;
       }
+      sec_harvest();
     }
     if (h.done) break;
   }
@@ -465,11 +529,20 @@ int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) 
   const int CH = 8;
   PcgScalars h{};
   int launched = 0;
+  const std::string key = "filter_chunk:" + std::to_string(slot);
   while (launched < M.S.maxIT) {
-    for (int c = 0; c < CH && launched < M.S.maxIT; ++c, ++launched) {
-      launch_filter_ku<T>(st, KU_P_UPDATE, g, slot, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
-      launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1);
-    }
+    const int n = std::min(CH, M.S.maxIT - launched);
+    auto body = [&]() {
+      for (int c = 0; c < n; ++c) {
+        launch_filter_ku<T>(st, KU_P_UPDATE, g, slot, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
+        launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1);
+      }
+    };
+    if (n == CH)
+      run_graph(key, body);
+    else
+      body();
+    launched += n;
     read_scalars(h, sc);
     if (h.done) break;
   }
@@ -524,6 +597,69 @@ void Engine::set_profiling(bool on) {
   prof_ku_ms = 0.0;
   prof_ku_launches = 0;
   prof_pcg_its = 0;
+  sev_used = 0;
+  for (int i = 0; i < SEC_COUNT; ++i) {
+    sec_ms[i] = 0.0;
+    sec_n[i] = 0;
+  }
+}
+
+void Engine::run_graph(const std::string& key, const std::function<void()>& body) {
+  if (prof_ || !use_graphs) {
+    body();
+    return;
+  }
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    cudaGraph_t g = nullptr;
+    TOPX_CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    TOPX_CUDA_OK(cudaStreamEndCapture(st, &g));
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    TOPX_CUDA_OK(e);
+    it = graphs_.emplace(key, ex).first;
+  }
+  TOPX_CUDA_OK(cudaGraphLaunch(it->second, st));
+}
+
+const char* Engine::section_name(int s) {
+  static const char* names[SEC_COUNT] = {"ku",        "pcg_update", "restrict",       "coarse_solve", "prolong",
+                                         "diag",      "galerkin_l2", "galerkin_span2", "slab_assemble", "schur",
+                                         "spd_inverse", "filter",    "oc",             "compliance"};
+  return (s >= 0 && s < SEC_COUNT) ? names[s] : "?";
+}
+
+void Engine::sec_begin(int sec) {
+  if (!prof_) return;
+  if (sev_used + 2 > int(sev.size())) sec_harvest();
+  sec_of[sev_used / 2] = sec;
+  TOPX_CUDA_OK(cudaEventRecord(sev[sev_used], st));
+}
+
+void Engine::sec_end() {
+  if (!prof_) return;
+  TOPX_CUDA_OK(cudaEventRecord(sev[sev_used + 1], st));
+  sev_used += 2;
+}
+
+void Engine::sec_harvest() {
+  if (!prof_ || sev_used == 0) return;
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  for (int i = 0; i < sev_used; i += 2) {
+    float ms = 0.f;
+    TOPX_CUDA_OK(cudaEventElapsedTime(&ms, sev[i], sev[i + 1]));
+    sec_ms[sec_of[i / 2]] += ms;
+    sec_n[sec_of[i / 2]] += 1;
+  }
+  sev_used = 0;
 }
 
 void Engine::set_moduli_host(const double* h_E) {
@@ -625,8 +761,10 @@ bool Engine::step(IterRecord& rec) {
   TOPX_CUDA_OK(cudaEventRecord(ev[1], st));
   for (size_t lc = 0; lc < U.size(); ++lc) rec.its.push_back(solve(int(lc)));
   TOPX_CUDA_OK(cudaEventRecord(ev[2], st));
+  sec_begin(SEC_COMPLIANCE);
   compliance(ce.p);
   launch_objective(st, Ne, ce.p, xPhys.p, cSolid_, Emin, E0, pen, dc.p, objS.p, rs1);
+  sec_end();
   ObjState os{};
   TOPX_CUDA_OK(cudaMemcpyAsync(&os, objS.p, sizeof(os), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaEventRecord(ev[3], st));
@@ -635,9 +773,11 @@ bool Engine::step(IterRecord& rec) {
   rec.vol = os.xsum / double(Ne);
   if (consType_ == 0) {
     // sensitivity filter ft = 1 (TOP3D_XL.m:135-137)
+    sec_begin(SEC_FILTER);
     launch_ewise(st, EW_MUL, Ne, x.p, dc.p, tmpA.p, 0.0);
     rec.filter_its = filter(0, tmpA.p, tmpB.p);
     launch_ewise(st, EW_DIV_MAXX, Ne, tmpB.p, x.p, dc.p, 1e-3);
+    sec_end();
     TOPX_CUDA_OK(cudaEventRecord(ev[4], st));
     // OC bisection (TOP3D_XL.m:145-156)
     OcState oc{};
@@ -645,6 +785,7 @@ bool Engine::step(IterRecord& rec) {
     oc.l2 = 1e9;
     oc.fval = os.xsum / double(Ne) - V0_;
     TOPX_CUDA_OK(cudaMemcpyAsync(ocS.p, &oc, sizeof(oc), cudaMemcpyHostToDevice, st));
+    sec_begin(SEC_OC);
     const uint8_t* pas = passive.p;
     for (int chunk = 0; chunk < 8; ++chunk) {
       for (int k = 0; k < 32; ++k) launch_oc_step(st, Ne, x.p, dc.p, pas, ocS.p, rs1, 0.2);
@@ -653,6 +794,7 @@ bool Engine::step(IterRecord& rec) {
       if (oc.converged) break;
     }
     launch_oc_final(st, Ne, x.p, dc.p, pas, xPhys.p, ocS.p, rs1, rs2, 0.2);
+    sec_end();
     TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
     TOPX_CUDA_OK(cudaEventRecord(ev[5], st));
     TOPX_CUDA_OK(cudaStreamSynchronize(st));
@@ -666,6 +808,7 @@ bool Engine::step(IterRecord& rec) {
   } else {
     step_local(rec, os);
   }
+  sec_harvest();
   change_ = rec.change;
   sharp_ = rec.sharp;
   rec.t_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_host0).count();

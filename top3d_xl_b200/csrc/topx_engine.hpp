@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -133,6 +135,13 @@ class Engine {
   void timer_start();
   double timer_stop_ms();
   void set_profiling(bool on);
+  // per-section device time (ms) and launch-group counts since profiling was switched on
+  enum Section { SEC_KU = 0, SEC_UPDATE, SEC_RESTRICT, SEC_COARSE_SOLVE, SEC_PROLONG, SEC_DIAG, SEC_GALERKIN2,
+                 SEC_GALERKIN3, SEC_SLAB_ASSEMBLE, SEC_SCHUR, SEC_INVERSE, SEC_FILTER, SEC_OC, SEC_COMPLIANCE,
+                 SEC_COUNT };
+  static const char* section_name(int s);
+  double sec_ms[SEC_COUNT] = {};
+  int64_t sec_n[SEC_COUNT] = {};
   double prof_ku_ms = 0.0;
   int64_t prof_ku_launches = 0;
   int64_t prof_pcg_its = 0;
@@ -157,6 +166,7 @@ class Engine {
   int filter_t(FWork<TF>& f, int slot, const double* d_src, double* d_out);
   void step_local(IterRecord& rec, const ObjState& os);
   void factor_coarsest();
+  void assemble_launches();
   void read_scalars(PcgScalars& h, const PcgScalars* d) const;
 
   // level-1 static data
@@ -172,7 +182,9 @@ class Engine {
   DevBuf<double> fl_F;
   int nflag = 0;
   SlabInfo si;
-  DevBuf<double> slabA, slabBup, slabSinv, slabT, gjP, gjR, gjC, slabW, slabV;
+  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gjP, gjR, gjC;
+  DevBuf<float> slabSinv32, slabL32, slabLT32;  // FP32 copies applied by the mixed-precision V-cycle
+  DevBuf<double> slabBS, slabW, slabV, slabXS;  // slab-ordered vectors of one coarse solve
   // workspaces
   KrylovWork kw;
   VWork<double> v64;
@@ -202,6 +214,19 @@ class Engine {
   std::vector<cudaEvent_t> ev;
   bool prof_ = false;
   std::vector<cudaEvent_t> pev;  // pairs around K*u launches of one chunk
+  // section profiler: event pairs recorded on the stream, harvested at sync points
+  std::vector<cudaEvent_t> sev;
+  std::vector<int> sec_of;
+  int sev_used = 0;
+  void sec_begin(int sec);
+  void sec_end();
+  void sec_harvest();
+  // CUDA graphs of fixed launch sequences, keyed by name; captured on first use and replayed
+  // (direct launches while profiling, so the section events stay on the stream)
+  std::map<std::string, cudaGraphExec_t> graphs_;
+  void run_graph(const std::string& key, const std::function<void()>& body);
+ public:
+  bool use_graphs = true;
   cudaEvent_t tev[2] = {nullptr, nullptr};
 };
 

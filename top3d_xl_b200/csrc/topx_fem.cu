@@ -38,135 +38,161 @@ static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
 // ---------------------------------------------------------------------------
 // K*u, level 1 (Solving_KbyU_MatrixFree, TOP3D_XL.m:684-725).
 //
-// Node-centric gather: one thread per grid node owns its 3 DOFs.  A CTA
-// stages a (32+2)x(4+2)x(2+2) halo tile of u (masked by the free-DOF mask) and
-// the 33x5x3 element moduli in shared memory, then sums, for each of the 8
-// surrounding hexes, the node's 3 rows of E_e*Ke times the hex's 24 DOFs.  No
-// atomics: the result is deterministic.  The reference's per-element BC
+// Node-centric gather: one thread per grid node owns its 3 DOFs.  A CTA of
+// 32x8 nodes marches 16 node planes along z, keeping a ring of three
+// (32+2)x(8+2) planes of u (masked by the free-DOF mask) and two planes of
+// element moduli in shared memory, and sums, for each of the 8 surrounding
+// hexes, the node's 3 rows of E_e*Ke times the hex's 24 DOFs (Ke entries are
+// constant-bank operands).  No atomics: the result is deterministic.  The reference's per-element BC
 // matrices (uniqueKesFree_/uniqueKesFixed_) reduce exactly to
 //     y = m .* K_E (m .* u) + (1-m) .* cfix .* u
 // with m the free-DOF mask and cfix(node) = sum over its hexes of 1/nAdj.
 // The PCG mode forms the direction p = z (+ beta*p) on the fly (the update
 // kernel stores it) and reduces p'q.
 // ---------------------------------------------------------------------------
-constexpr int KTY = 32, KTX = 4, KTZ = 2;
-constexpr int KNT = KTY * KTX * KTZ;
+constexpr int KY = 32, KX = 8, KZC = 16;  // CTA = KY x KX nodes, marching KZC node planes along z
+constexpr int KNT = KY * KX;
+
+// Node value seen by the operator: u (plain) or the PCG direction p = z (+ beta p_old).
+template <typename T, int MODE>
+__device__ __forceinline__ void ku_fetch(const T* __restrict__ in, const T* __restrict__ zin, int64_t n, int64_t S,
+                                         bool first, T beta, T& v0, T& v1, T& v2) {
+  if (MODE == KU_PLAIN) {
+    v0 = in[n];
+    v1 = in[n + S];
+    v2 = in[n + 2 * S];
+  } else if (first) {
+    v0 = zin[n];
+    v1 = zin[n + S];
+    v2 = zin[n + 2 * S];
+  } else {
+    v0 = zin[n] + beta * in[n];
+    v1 = zin[n + S] + beta * in[n + S];
+    v2 = zin[n + 2 * S] + beta * in[n + 2 * S];
+  }
+}
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(KNT) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
-                                                T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
-                                                const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
-                                                PcgScalars* sc, RedScratch rs) {
+__global__ void __launch_bounds__(KNT, 2) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
+                                                  T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
+                                                  const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
+                                                  PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
-  __shared__ T su[3][KTZ + 2][KTX + 2][KTY + 2];
-  __shared__ T sp[3][KTZ][KTX][KTY];
-  __shared__ T se[KTZ + 1][KTX + 1][KTY + 1];
+  __shared__ T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
+  __shared__ T spu[3][3][KX][KY];         // unmasked values of the CTA's own nodes per plane
+  __shared__ T se[2][KX + 1][KY + 1];     // ring of 2 element planes
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
-  const int y0 = blockIdx.x * KTY, x0 = blockIdx.y * KTX, z0 = blockIdx.z * KTZ;
-  const int tid = threadIdx.x + KTY * (threadIdx.y + KTX * threadIdx.z);
+  const int y0 = blockIdx.x * KY, x0 = blockIdx.y * KX, zc0 = blockIdx.z * KZC;
+  const int ty = threadIdx.x, tx = threadIdx.y;
+  const int tid = ty + KY * tx;
   const bool first = (MODE != KU_PLAIN) && sc->first;
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
-  constexpr int NSU = (KTZ + 2) * (KTX + 2) * (KTY + 2);
-  for (int i = tid; i < NSU; i += KNT) {
-    const int sy = i % (KTY + 2), r = i / (KTY + 2), sx = r % (KTX + 2), sz = r / (KTX + 2);
-    const int gy = y0 - 1 + sy, gx = x0 - 1 + sx, gz = z0 - 1 + sz;
-    T v0 = T(0), v1 = T(0), v2 = T(0);
-    if (gy >= 0 && gy < nny && gx >= 0 && gx < nnx && gz >= 0 && gz < nnz) {
-      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
-      if (MODE == KU_PLAIN) {
-        v0 = in[n];
-        v1 = in[n + S];
-        v2 = in[n + 2 * S];
-      } else if (first) {
-        v0 = zin[n];
-        v1 = zin[n + S];
-        v2 = zin[n + 2 * S];
-      } else {
-        v0 = zin[n] + beta * in[n];
-        v1 = zin[n + S] + beta * in[n + S];
-        v2 = zin[n + 2 * S] + beta * in[n + 2 * S];
+
+  auto load_nodes = [&](int zp, int slot) {
+    for (int i = tid; i < (KX + 2) * (KY + 2); i += KNT) {
+      const int sy = i % (KY + 2), sx = i / (KY + 2);
+      const int gy = y0 - 1 + sy, gx = x0 - 1 + sx;
+      T v0 = T(0), v1 = T(0), v2 = T(0);
+      if (zp >= 0 && zp < nnz && gy >= 0 && gy < nny && gx >= 0 && gx < nnx) {
+        const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * zp);
+        ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
+        if (sy >= 1 && sy <= KY && sx >= 1 && sx <= KX) {
+          spu[slot][0][sx - 1][sy - 1] = v0;
+          spu[slot][1][sx - 1][sy - 1] = v1;
+          spu[slot][2][sx - 1][sy - 1] = v2;
+        }
+        const uint8_t fb = fixbits[n];
+        if (fb & 1) v0 = T(0);
+        if (fb & 2) v1 = T(0);
+        if (fb & 4) v2 = T(0);
       }
-      const bool interior = sy >= 1 && sy <= KTY && sx >= 1 && sx <= KTX && sz >= 1 && sz <= KTZ;
-      if (interior) {
-        sp[0][sz - 1][sx - 1][sy - 1] = v0;
-        sp[1][sz - 1][sx - 1][sy - 1] = v1;
-        sp[2][sz - 1][sx - 1][sy - 1] = v2;
-      }
-      const uint8_t fb = fixbits[n];
-      if (fb & 1) v0 = T(0);
-      if (fb & 2) v1 = T(0);
-      if (fb & 4) v2 = T(0);
+      su[slot][0][sx][sy] = v0;
+      su[slot][1][sx][sy] = v1;
+      su[slot][2][sx][sy] = v2;
     }
-    su[0][sz][sx][sy] = v0;
-    su[1][sz][sx][sy] = v1;
-    su[2][sz][sx][sy] = v2;
-  }
-  constexpr int NSE = (KTZ + 1) * (KTX + 1) * (KTY + 1);
-  for (int i = tid; i < NSE; i += KNT) {
-    const int sy = i % (KTY + 1), r = i / (KTY + 1), sx = r % (KTX + 1), sz = r / (KTX + 1);
-    const int ey = y0 - 1 + sy, ex = x0 - 1 + sx, ez = z0 - 1 + sz;
-    T v = T(0);
-    if (ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz)
-      v = E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)];
-    se[sz][sx][sy] = v;
-  }
-  __syncthreads();
-  const int ty = threadIdx.x, tx = threadIdx.y, tz = threadIdx.z;
-  const int gy = y0 + ty, gx = x0 + tx, gz = z0 + tz;
+  };
+  auto load_elems = [&](int ez, int slot) {
+    for (int i = tid; i < (KX + 1) * (KY + 1); i += KNT) {
+      const int sy = i % (KY + 1), sx = i / (KY + 1);
+      const int ey = y0 - 1 + sy, ex = x0 - 1 + sx;
+      T v = T(0);
+      if (ez >= 0 && ez < g.nz && ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx)
+        v = E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)];
+      se[slot][sx][sy] = v;
+    }
+  };
+
+  load_nodes(zc0 - 1, 0);
+  load_nodes(zc0, 1);
+  load_elems(zc0 - 1, 0);
+  const int gy = y0 + ty, gx = x0 + tx;
+  const bool own = gy < nny && gx < nnx;
   double dot = 0.0;
-  if (gy < nny && gx < nnx && gz < nnz) {
-    T acc[8][3];
+  for (int k = 0; k < KZC; ++k) {
+    const int z = zc0 + k;
+    if (z >= nnz) break;
+    load_nodes(z + 1, (k + 2) % 3);
+    load_elems(z, (k + 1) % 2);
+    __syncthreads();
+    if (own) {
+      const T(*pl[3])[KX + 2][KY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
+      const T(*el[2])[KY + 1] = {se[k % 2], se[(k + 1) % 2]};
+      T acc[8][3];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
+      for (int e = 0; e < 8; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+      for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx)
+        for (int dx = -1; dx <= 1; ++dx)
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const T u0 = su[0][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
-          const T u1 = su[1][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
-          const T u2 = su[2][tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
+          for (int dy = -1; dy <= 1; ++dy) {
+            const T u0 = pl[dz + 1][0][tx + 1 + dx][ty + 1 + dy];
+            const T u1 = pl[dz + 1][1][tx + 1 + dx][ty + 1 + dy];
+            const T u2 = pl[dz + 1][2][tx + 1 + dx][ty + 1 + dy];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
-            const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
-            if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
-            const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
+            for (int e = 0; e < 8; ++e) {
+              const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
+              const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
+              if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
+              const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              T s = acc[e][i];
-              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
-              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
-              s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
-              acc[e][i] = s;
+              for (int i = 0; i < 3; ++i) {
+                T s = acc[e][i];
+                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
+                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
+                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
+                acc[e][i] = s;
+              }
             }
           }
-        }
-    // combine the 8 hexes in the reference's local-node order
-    T y[3] = {T(0), T(0), T(0)};
+      // combine the 8 hexes in the reference's local-node order
+      T y[3] = {T(0), T(0), T(0)};
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
-      const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
-      const T Ee = se[tz + 1 + oz][tx + 1 + ox][ty + 1 + oy];
+      for (int a = 0; a < 8; ++a) {
+        const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
+        const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
+        const T Ee = el[oz + 1][tx + 1 + ox][ty + 1 + oy];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
+        for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
+      }
+      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * z);
+      const uint8_t fb = fixbits[n];
+      const int cs = (k + 1) % 3;
+      const T p0 = spu[cs][0][tx][ty], p1 = spu[cs][1][tx][ty], p2 = spu[cs][2][tx][ty];
+      if (fb) {
+        const T cf = cfix[n];
+        if (fb & 1) y[0] = cf * p0;
+        if (fb & 2) y[1] = cf * p1;
+        if (fb & 4) y[2] = cf * p2;
+      }
+      out[n] = y[0];
+      out[n + S] = y[1];
+      out[n + 2 * S] = y[2];
+      if (MODE != KU_PLAIN)
+        dot += double(p0) * double(y[0]) + double(p1) * double(y[1]) + double(p2) * double(y[2]);
     }
-    const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
-    const uint8_t fb = fixbits[n];
-    const T p0 = sp[0][tz][tx][ty], p1 = sp[1][tz][tx][ty], p2 = sp[2][tz][tx][ty];
-    if (fb) {
-      const T cf = cfix[n];
-      if (fb & 1) y[0] = cf * p0;
-      if (fb & 2) y[1] = cf * p1;
-      if (fb & 4) y[2] = cf * p2;
-    }
-    out[n] = y[0];
-    out[n + S] = y[1];
-    out[n + 2 * S] = y[2];
-    if (MODE != KU_PLAIN) dot = double(p0) * double(y[0]) + double(p1) * double(y[1]) + double(p2) * double(y[2]);
+    __syncthreads();
   }
   if (MODE != KU_PLAIN) {
     double v[1] = {dot}, tot[1];
@@ -177,8 +203,8 @@ __global__ void __launch_bounds__(KNT) k_ku_l1(Grid g, const T* __restrict__ in,
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
-  dim3 blk(KTY, KTX, KTZ);
-  dim3 grd((g.nny() + KTY - 1) / KTY, (g.nnx() + KTX - 1) / KTX, (g.nnz() + KTZ - 1) / KTZ);
+  dim3 blk(KY, KX, 1);
+  dim3 grd((g.nny() + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + KZC - 1) / KZC);
   if (mode == KU_PLAIN)
     k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs);
   else

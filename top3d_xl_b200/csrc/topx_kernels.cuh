@@ -94,11 +94,16 @@ struct SlabInfo {
 };
 void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks, const uint8_t* present, double* A,
                           double* Bup);
-void launch_slab_schur(cudaStream_t st, SlabInfo si, int s, const double* Sinv_prev, const double* Bup_prev,
-                       const double* A_s, double* T, double* S_out);
+// in-place inverse of an SPD m x m matrix; Pinv 64x64, R 64 x m, C m x 64 scratch
 void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C);
-template <typename T>
-void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const double* Sinv, const double* Bup, const T* b,
-                       double* w, double* v, T* x, const PcgScalars* sc);
+// twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
+// Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes);
+// gj_scratch holds 2 * (64*64 + 128*m) doubles
+void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const double* Bup, double* Inv, double* X,
+                        double* XT, double* gj_scratch);
+// x = K_coarsest^{-1} b; bs, W, V, xs are ns*m FP64 scratch vectors in slab order
+template <typename T, typename TM>
+void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT, const T* b,
+                       double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc);
 
 }  // namespace topx

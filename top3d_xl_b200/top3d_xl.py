@@ -202,7 +202,9 @@ class Context:
     def profile(self):
         p = L.Profile()
         self._check(self.lib.topx_get_profile(self._h, C.byref(p)))
-        return dict(ku_ms=p.ku_ms, ku_launches=p.ku_launches, pcg_iterations=p.pcg_iterations)
+        sections = {self.lib.topx_profile_section_name(i).decode(): (p.section_ms[i], p.section_count[i])
+                    for i in range(L.NSECTIONS)}
+        return dict(ku_ms=p.ku_ms, ku_launches=p.ku_launches, pcg_iterations=p.pcg_iterations, sections=sections)
 
     def density(self):
         out = np.empty(self.numElements)
