@@ -164,16 +164,16 @@ void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const ui
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-// Jacobi diagonal of a coarse level from its element operators (TOP3D_XL.m:1000-1018)
+// Jacobi diagonal of a coarse level from its element operators (TOP3D_XL.m:1000-1018),
+// stored as its reciprocal (0 on absent nodes) so the smoother multiplies
 template <typename T>
 __global__ void k_diag_coarse(Grid g, const double* __restrict__ Ks, const uint8_t* __restrict__ present,
                               T* __restrict__ d) {
   const int64_t N = g.nnodes();
   const int nny = g.ny + 1, nnx = g.nx + 1;
   for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
-    double s[3] = {1.0, 1.0, 1.0};
+    double s[3] = {0.0, 0.0, 0.0};
     if (present[n]) {
-      s[0] = s[1] = s[2] = 0.0;
       const int gy = int(n % nny), gx = int((n / nny) % nnx), gz = int(n / (int64_t(nny) * nnx));
       for (int a = 0; a < 8; ++a) {
         const int ey = gy - hex_ly(a), ex = gx - hex_lx(a), ez = gz - hex_lz(a);
@@ -181,6 +181,7 @@ __global__ void k_diag_coarse(Grid g, const double* __restrict__ Ks, const uint8
         const int64_t e = ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez);
         for (int c = 0; c < 3; ++c) s[c] += Ks[e * 576 + (3 * a + c) * 25];
       }
+      for (int c = 0; c < 3; ++c) s[c] = 1.0 / s[c];
     }
     for (int c = 0; c < 3; ++c) d[n + c * g.stride] = T(s[c]);
   }
@@ -397,9 +398,11 @@ __global__ void __launch_bounds__(256) k_gj_pivot(int m, int k0, int kb, GJSet s
   const bool z1 = blockIdx.z != 0;
   const double* __restrict__ A = z1 ? set.A[1] : set.A[0];
   double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
-  __shared__ double colb[2][GJB], rowb[2][GJB], rpb[2];
+  // rowb is padded by one slot per 16 columns: the four column groups a warp reads
+  // at the same q then fall into different banks
+  __shared__ double colb[2][GJB], rowb[2][GJB + 4], rpb[2];
   const int tid = threadIdx.x;
-  const int r = tid >> 2, c0 = (tid & 3) * 16;
+  const int r = tid >> 2, c0 = (tid & 3) * 16, cpad = c0 + (c0 >> 4);
   double a[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(256) k_gj_pivot(int m, int k0, int kb, GJSet s
       }
       if (r == t) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) rowb[buf][c0 + q] = a[q];
+        for (int q = 0; q < 16; ++q) rowb[buf][cpad + q] = a[q];
       }
       __syncthreads();
       const double rp = rpb[buf];
@@ -426,7 +429,7 @@ __global__ void __launch_bounds__(256) k_gj_pivot(int m, int k0, int kb, GJSet s
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int c = c0 + q;
-        const double rc = rowb[buf][c];
+        const double rc = rowb[buf][cpad + q];
         double v;
         if (r == t)
           v = (c == t) ? rp : -rc * rp;
@@ -546,12 +549,29 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, GJSet 
   for (int q = 0; q < 4; ++q) {
     const int ii = i0 + 4 * ty + q;
     if (ii >= m) continue;
+    const int jb = j0 + 4 * tx;
+    double* Ar = A + int64_t(ii) * m;
+    // 16-byte path only when the absolute address is 16-byte aligned (matrix bases
+    // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
+    if (jb + 3 < m && (reinterpret_cast<uintptr_t>(Ar + jb) & 15) == 0) {
+      double2 v0 = *reinterpret_cast<double2*>(Ar + jb), v1 = *reinterpret_cast<double2*>(Ar + jb + 2);
+      if (jK) {
+        v0 = make_double2(acc[q][0], acc[q][1]);
+        v1 = make_double2(acc[q][2], acc[q][3]);
+      } else {
+        v0.x += acc[q][0];
+        v0.y += acc[q][1];
+        v1.x += acc[q][2];
+        v1.y += acc[q][3];
+      }
+      *reinterpret_cast<double2*>(Ar + jb) = v0;
+      *reinterpret_cast<double2*>(Ar + jb + 2) = v1;
+    } else {
 #pragma unroll
-    for (int w = 0; w < 4; ++w) {
-      const int j = j0 + 4 * tx + w;
-      if (j >= m) continue;
-      const int64_t k = int64_t(ii) * m + j;
-      A[k] = jK ? acc[q][w] : A[k] + acc[q][w];
+      for (int w = 0; w < 4; ++w) {
+        const int j = jb + w;
+        if (j < m) Ar[j] = jK ? acc[q][w] : Ar[j] + acc[q][w];
+      }
     }
   }
 }

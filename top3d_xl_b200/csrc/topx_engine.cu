@@ -707,8 +707,9 @@ void Engine::get_diag(int level, double* h_d) const {
     TOPX_CUDA_OK(cudaMemcpy(f.data(), src, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < f.size(); ++i) dense[i] = f[i];
   }
+  // the engine stores reciprocal diagonals
   for (int64_t k = 0; k < L.numNodes; ++k)
-    for (int c = 0; c < 3; ++c) h_d[3 * k + c] = dense[(L.nodMapBack[k] - 1) + c * g.stride];
+    for (int c = 0; c < 3; ++c) h_d[3 * k + c] = 1.0 / dense[(L.nodMapBack[k] - 1) + c * g.stride];
 }
 
 // ---------------------------------------------------------------------------

@@ -72,14 +72,57 @@ __device__ __forceinline__ void ku_fetch(const T* __restrict__ in, const T* __re
   }
 }
 
+// Accumulate, for the four hexes on one side of the node plane (upper: oz = 0,
+// lower: oz = -1), the node's 3 rows of Ke times the hex's 24 DOFs, then add
+// E_e * acc to y in the reference's local-node order.
+template <typename T, int OZ>
+__device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], const T (*const el[2])[KY + 1],
+                                        int tx, int ty, T (&y)[3]) {
+  T acc[4][3];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
+#pragma unroll
+  for (int dz = OZ; dz <= OZ + 1; ++dz)
+#pragma unroll
+    for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        const T u0 = pl[dz + 1][0][tx + 1 + dx][ty + 1 + dy];
+        const T u1 = pl[dz + 1][1][tx + 1 + dx][ty + 1 + dy];
+        const T u2 = pl[dz + 1][2][tx + 1 + dx][ty + 1 + dy];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1;
+          const int ly = dy - oy, lx = dx - ox, lz = dz - OZ;
+          if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
+          const int a = hex_local(-oy, -ox, -OZ), b = hex_local(ly, lx, lz);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            T s = acc[e][i];
+            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
+            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
+            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
+            acc[e][i] = s;
+          }
+        }
+      }
+#pragma unroll
+  for (int a = (OZ == 0 ? 0 : 4); a < (OZ == 0 ? 4 : 8); ++a) {
+    const int oy = -hex_ly(a), ox = -hex_lx(a);
+    const int e = (oy + 1) + 2 * (ox + 1);
+    const T Ee = el[OZ + 1][tx + 1 + ox][ty + 1 + oy];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
+  }
+}
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(KNT, 2) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
+__global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
                                                   T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
                                                   PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
-  __shared__ T spu[3][3][KX][KY];         // unmasked values of the CTA's own nodes per plane
   __shared__ T se[2][KX + 1][KY + 1];     // ring of 2 element planes
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
@@ -97,11 +140,6 @@ __global__ void __launch_bounds__(KNT, 2) k_ku_l1(Grid g, const T* __restrict__ 
       if (zp >= 0 && zp < nnz && gy >= 0 && gy < nny && gx >= 0 && gx < nnx) {
         const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * zp);
         ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
-        if (sy >= 1 && sy <= KY && sx >= 1 && sx <= KX) {
-          spu[slot][0][sx - 1][sy - 1] = v0;
-          spu[slot][1][sx - 1][sy - 1] = v1;
-          spu[slot][2][sx - 1][sy - 1] = v2;
-        }
         const uint8_t fb = fixbits[n];
         if (fb & 1) v0 = T(0);
         if (fb & 2) v1 = T(0);
@@ -136,50 +174,15 @@ __global__ void __launch_bounds__(KNT, 2) k_ku_l1(Grid g, const T* __restrict__ 
     load_elems(z, (k + 1) % 2);
     __syncthreads();
     if (own) {
-      const T(*pl[3])[KX + 2][KY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
-      const T(*el[2])[KY + 1] = {se[k % 2], se[(k + 1) % 2]};
-      T acc[8][3];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
-#pragma unroll
-      for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-        for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll
-          for (int dy = -1; dy <= 1; ++dy) {
-            const T u0 = pl[dz + 1][0][tx + 1 + dx][ty + 1 + dy];
-            const T u1 = pl[dz + 1][1][tx + 1 + dx][ty + 1 + dy];
-            const T u2 = pl[dz + 1][2][tx + 1 + dx][ty + 1 + dy];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
-              const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
-              if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
-              const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
-#pragma unroll
-              for (int i = 0; i < 3; ++i) {
-                T s = acc[e][i];
-                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
-                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
-                s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
-                acc[e][i] = s;
-              }
-            }
-          }
-      // combine the 8 hexes in the reference's local-node order
+      const T(*const pl[3])[KX + 2][KY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
+      const T(*const el[2])[KY + 1] = {se[k % 2], se[(k + 1) % 2]};
       T y[3] = {T(0), T(0), T(0)};
-#pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
-        const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
-        const T Ee = el[oz + 1][tx + 1 + ox][ty + 1 + oy];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
-      }
+      ku_half<T, 0>(pl, el, tx, ty, y);   // hexes above the node: local nodes 1-4
+      ku_half<T, -1>(pl, el, tx, ty, y);  // hexes below the node: local nodes 5-8
       const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * z);
       const uint8_t fb = fixbits[n];
-      const int cs = (k + 1) % 3;
-      const T p0 = spu[cs][0][tx][ty], p1 = spu[cs][1][tx][ty], p2 = spu[cs][2][tx][ty];
+      T p0 = T(0), p1 = T(0), p2 = T(0);
+      if (fb || MODE != KU_PLAIN) ku_fetch<T, MODE>(in, zin, n, S, first, beta, p0, p1, p2);
       if (fb) {
         const T cf = cfix[n];
         if (fb & 1) y[0] = cf * p0;
@@ -214,8 +217,8 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
 
 // ---------------------------------------------------------------------------
 // Finest-level Jacobi diagonal (TOP3D_XL.m:1020-1050): sum over the node's
-// hexes, in local-node order, of E_e * diag(Ke); fixed DOFs take cfix; absent
-// nodes get 1 so that r./d stays 0 there.
+// hexes, in local-node order, of E_e * diag(Ke); fixed DOFs take cfix.  Stored
+// as its reciprocal (0 on absent nodes) so the smoother multiplies.
 // ---------------------------------------------------------------------------
 template <typename TE, typename T>
 __global__ void k_diag_l1(Grid g, const TE* __restrict__ E, const uint8_t* __restrict__ fixbits,
@@ -223,7 +226,7 @@ __global__ void k_diag_l1(Grid g, const TE* __restrict__ E, const uint8_t* __res
   const int64_t N = g.nnodes();
   const int nny = g.ny + 1, nnx = g.nx + 1;
   for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
-    double v[3] = {1.0, 1.0, 1.0};
+    double v[3] = {0.0, 0.0, 0.0};
     if (present[n]) {
       const int gy = int(n % nny), gx = int((n / nny) % nnx), gz = int(n / (int64_t(nny) * nnx));
       double s[3] = {0.0, 0.0, 0.0};
@@ -234,7 +237,7 @@ __global__ void k_diag_l1(Grid g, const TE* __restrict__ E, const uint8_t* __res
         for (int c = 0; c < 3; ++c) s[c] += double(ke<double>((3 * a + c) * 25)) * Ee;
       }
       const uint8_t fb = fixbits[n];
-      for (int c = 0; c < 3; ++c) v[c] = (fb >> c) & 1 ? double(cfix[n]) : s[c];
+      for (int c = 0; c < 3; ++c) v[c] = 1.0 / ((fb >> c) & 1 ? double(cfix[n]) : s[c]);
     }
     for (int c = 0; c < 3; ++c) d[n + c * g.stride] = T(v[c]);
   }
@@ -282,6 +285,17 @@ void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
 template <typename T, typename TY>
 __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z, T* __restrict__ p,
                              T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs) {
@@ -290,18 +304,31 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
   const T beta = T(sc->beta);
   const double lam = sc->x1 / sc->pq;
   const T lamT = T(lam);
-  const int64_t N = g.nnodes(), S = g.stride;
+  const TY lamY = TY(lam);
+  const int64_t S = g.stride;  // a multiple of 32, so node pairs are aligned
+  const int64_t npair = (g.nnodes() + 1) / 2;
   double rr = 0.0;
-  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+  using V2 = typename Vec2<T>::type;
+  using Y2 = typename Vec2<TY>::type;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npair; i += int64_t(gridDim.x) * blockDim.x) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t k = n + c * S;
-      const T pv = first ? z[k] : z[k] + beta * p[k];
-      p[k] = pv;
-      y[k] = y[k] + TY(lam) * TY(pv);
-      const T rv = r[k] - lamT * q[k];
-      r[k] = rv;
-      rr += double(rv) * double(rv);
+      const int64_t k = 2 * i + c * S;
+      const V2 zv = *reinterpret_cast<const V2*>(z + k);
+      V2 pv = *reinterpret_cast<const V2*>(p + k);
+      pv.x = first ? zv.x : zv.x + beta * pv.x;
+      pv.y = first ? zv.y : zv.y + beta * pv.y;
+      *reinterpret_cast<V2*>(p + k) = pv;
+      Y2 yv = *reinterpret_cast<const Y2*>(y + k);
+      yv.x = yv.x + lamY * TY(pv.x);
+      yv.y = yv.y + lamY * TY(pv.y);
+      *reinterpret_cast<Y2*>(y + k) = yv;
+      const V2 qv = *reinterpret_cast<const V2*>(q + k);
+      V2 rv = *reinterpret_cast<const V2*>(r + k);
+      rv.x = rv.x - lamT * qv.x;
+      rv.y = rv.y - lamT * qv.y;
+      *reinterpret_cast<V2*>(r + k) = rv;
+      rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y);
     }
   }
   double v[1] = {rr}, tot[1];
@@ -388,18 +415,19 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
 // The level-1 instance also reduces z'r and updates beta/x1 (TOP3D_XL.m:626-630).
 // ---------------------------------------------------------------------------
 template <typename TX, typename T, typename TD, int S, bool DOT>
-__global__ void k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __restrict__ r, const TD* __restrict__ d,
-                                 const uint8_t* __restrict__ present, T* __restrict__ x, Grid gf, T omega,
-                                 PcgScalars* sc, RedScratch rs, int init) {
+__global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __restrict__ r,
+                                                        const TD* __restrict__ dinv,
+                                                        const uint8_t* __restrict__ present, T* __restrict__ x,
+                                                        Grid gf, T omega, PcgScalars* sc, RedScratch rs, int init) {
   if (DOT && sc->done) return;
-  const int64_t N = gf.nnodes();
-  const int fny = gf.nny(), fnx = gf.nnx();
+  const int fny = gf.nny(), fnx = gf.nnx(), fnz = gf.nnz();
   const int cny = gc.nny(), cnx = gc.nnx();
+  const int fy = blockIdx.x * 32 + threadIdx.x, fx = blockIdx.y * 4 + threadIdx.y, fz = blockIdx.z * 2 + threadIdx.z;
   double zr = 0.0;
-  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+  if (fy < fny && fx < fnx && fz < fnz) {
+    const int64_t n = fy + int64_t(fny) * (fx + int64_t(fnx) * fz);
     T v[3] = {T(0), T(0), T(0)};
     if (present[n]) {
-      const int fy = int(n % fny), fx = int((n / fny) % fnx), fz = int(n / (int64_t(fny) * fnx));
       const int Y = fy / S, X = fx / S, Z = fz / S;
       const int ty = fy - S * Y, tx = fx - S * X, tz = fz - S * Z;
       T pc[3] = {T(0), T(0), T(0)};
@@ -418,10 +446,10 @@ __global__ void k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const T rv = r[n + c * gf.stride], dv = T(d[n + c * gf.stride]);
-        T t = omega * (rv / dv);
+        const T rv = r[n + c * gf.stride], di = T(dinv[n + c * gf.stride]);
+        T t = omega * (rv * di);
         t = t + pc[c];
-        t = t + (omega * rv) / dv;
+        t = t + (omega * rv) * di;
         v[c] = t;
         if (DOT) zr += double(t) * double(rv);
       }
@@ -431,7 +459,7 @@ __global__ void k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __
   }
   if (DOT) {
     double vv[1] = {zr}, tot[1];
-    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0) {
+    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
       if (init) {
         sc->x1 = tot[0];
       } else {
@@ -446,18 +474,19 @@ template <typename TX, typename T, typename TD>
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
                            PcgScalars* sc, RedScratch rs) {
-  const unsigned nb = grid1d(gf.nnodes(), 256);
+  const dim3 nb((gf.nny() + 31) / 32, (gf.nnx() + 3) / 4, (gf.nnz() + 1) / 2);
+  const dim3 blk(32, 4, 2);
   const T w = T(omega);
   if (span == 4) {
     if (dot)
-      k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      k_prolong_smooth<TX, T, TD, 4, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
     else
-      k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      k_prolong_smooth<TX, T, TD, 4, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
   } else {
     if (dot)
-      k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      k_prolong_smooth<TX, T, TD, 2, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
     else
-      k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      k_prolong_smooth<TX, T, TD, 2, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
