@@ -8,9 +8,10 @@ rMin=sqrt(3) -- TOP3D_XL(true(128,256,128),'GLOBAL',0.12,50,sqrt(3)).  One
 factorisation, multigrid PCG, compliance, PDE sensitivity filter, OC update),
 with all state resident in HBM.
 
-`value` is the mixed-precision engine (FP32 inner PCG in FP64 defect
-correction); the same run in plain FP64 is measured beside it and the
-per-iteration relative compliance error of mixed vs FP64 is reported.
+`value` is the mixed-precision engine (FP64 Krylov iteration and operator,
+FP32 multigrid preconditioner and filter); the same run in plain FP64 is
+measured beside it and the per-iteration relative compliance error of mixed
+vs FP64 is reported.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
 
@@ -39,6 +40,11 @@ WORKLOADS = {
     "cuboid25": dict(shape=(25, 50, 25), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
 }
 METRIC = "OC iterations/s (GLOBAL, mixed precision; FP64 beside it)"
+# DRAM bytes (read + write) per node of one K*u launch in PCG mode, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum); None until measured.
+KU_TRAFFIC_PER_NODE = None
+# Nominal FP64 rate of a B200 on CUDA cores: 148 SMs x 64 FMA/clk x 2 flop x 1.965 GHz.
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def peaks():
@@ -116,12 +122,14 @@ def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False
     hist = []
     for _ in range(warmup):
         hist.append(ctx.step())
+    launches0 = ctx.launch_count()
     ctx.timer_start()
     t0 = time.perf_counter()
     for _ in range(steps):
         hist.append(ctx.step())
     ms = ctx.timer_stop()
     wall = time.perf_counter() - t0
+    launches = ctx.launch_count() - launches0
     prof = None
     if profile_steps:
         ctx.set_profiling(True)
@@ -131,7 +139,7 @@ def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False
         prof = ctx.profile()
         prof["steps"] = profile_steps
         ctx.set_profiling(False)
-    out = dict(ms=ms, wall=wall, hist=hist, prof=prof, ne=ctx.numElements, ndof=ctx.numDOFs,
+    out = dict(ms=ms, wall=wall, hist=hist, prof=prof, launches=launches, ne=ctx.numElements, ndof=ctx.numDOFs,
                nnodes=int(ctx.info.numNodes))
     if keep:
         out["ctx"] = ctx
@@ -242,8 +250,6 @@ def main(argv=None):
         its_per_oc, fits = 40.0, 6.0
         t0 = time.perf_counter()
         cb = cpu_sample(wl, its_per_oc, fits)
-        for _ in range(max(0, a.warmup - 1)):
-            pass
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "OC iterations/s",
                 "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / cb["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -287,12 +293,17 @@ def main(argv=None):
     cd = np.array([h["c"] for h in fp64["hist"]])
     n = min(len(cm), len(cd))
     relerr = float(np.max(np.abs(cm[:n] - cd[:n]) / np.abs(cd[:n])))
-    # roofline of the dominant kernel: level-1 K*u (FP32 in the mixed path)
+    # roofline of the dominant kernel: level-1 K*u in PCG mode (FP64 in both arms).
+    # Per launch it reads p_old and z and writes q (3 doubles per node each), reads the
+    # moduli (1 double per element) and the free-DOF bits (1 byte per node): 73 B/node +
+    # 8 B/element; per node 8 hexes x 3 rows x 24 DOFs + 24 scalings = 600 FMA.
     prof = mixed["prof"]
     nn = mixed["nnodes"]
-    alg_bytes = 2 * 3 * nn * 4 + mixed["ne"] * 4  # read p + write q (FP32, 3 DOFs/node) + moduli
+    alg_bytes = 73 * nn + 8 * mixed["ne"]
+    flop = 2 * 600 * nn
     ku_ms = prof["ku_ms"] / max(1, prof["ku_launches"])
     achieved = alg_bytes / (ku_ms * 1e-3) / 1e9
+    tflops = flop / (ku_ms * 1e-3) / 1e12
     peak, kind = peaks()
     its_mixed = [k for h in mixed["hist"][a.warmup:] for k in h["its"]]
     its64 = [k for h in fp64["hist"][a.warmup:] for k in h["its"]]
@@ -304,7 +315,8 @@ def main(argv=None):
         return {k: 1000.0 * float(np.mean([h[k] for h in hs])) for k in ("t_assemble", "t_cg", "t_filter", "t_opt")}
     line = {"metric": METRIC, "value": value, "unit": "OC iterations/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (FP64 outer residual, dots, coarse solve, compliance/OC sums)",
+            "vs_baseline": None,
+            "dtype": "f64 (Krylov iteration, operator, dots, compliance, OC) + f32 (multigrid preconditioner, filter)",
             "data": "synthetic (built-in cuboid BCs)", "config": cfg,
             "fp64": {"value": a.steps / (fp64["ms"] / 1000.0), "ms_per_step": fp64["ms"] / a.steps,
                      "pcg_its_per_step": float(np.mean(its64))},
@@ -314,11 +326,14 @@ def main(argv=None):
             "phases_ms": {"mixed": phases(mixed), "fp64": phases(fp64)},
             "sections_ms_per_step": {k: round(v[0] / prof["steps"], 3) for k, v in prof["sections"].items()},
             "section_groups_per_step": {k: round(v[1] / prof["steps"], 1) for k, v in prof["sections"].items()},
-            "gpu_launches": None,
-            "roofline": {"kernel": "k_ku_l1<float> (level-1 K*u, PCG mode)", "bound": "hbm",
+            "gpu_launches": mixed["launches"],
+            "roofline": {"kernel": "k_ku_l1<double, KU_P_UPDATE> (level-1 K*u, PCG mode)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": kind, "algorithmic_bytes_per_launch": alg_bytes,
-                         "ms_per_launch": ku_ms, "traffic": None},
+                         "ms_per_launch": ku_ms, "traffic": KU_TRAFFIC_PER_NODE * nn if KU_TRAFFIC_PER_NODE else None,
+                         "fp64_pipe": {"flop_per_launch": flop, "achieved_tflops": tflops,
+                                       "nominal_peak_tflops": FP64_NOMINAL_TFLOPS,
+                                       "frac_of_nominal": tflops / FP64_NOMINAL_TFLOPS}},
             "e2e": {"value": e2e["value"], "unit": "OC iterations/s", "h2d_bytes_per_step": e2e["h2d"],
                     "d2h_bytes_per_step": e2e["d2h"]},
             "clocks": clk.summary()}

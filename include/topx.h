@@ -175,6 +175,8 @@ topx_status topx_timer_stop(topx_ctx* ctx, double* ms);
 /* per-launch timing of the K*u kernel (events around each launch); on != 0 resets the counters */
 topx_status topx_set_profiling(topx_ctx* ctx, int on);
 topx_status topx_get_profile(topx_ctx* ctx, topx_profile* out);
+/* kernels this library has launched in this process so far (graph replays count their kernels) */
+int64_t topx_launch_count(void);
 
 #ifdef __cplusplus
 }

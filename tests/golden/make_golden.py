@@ -53,7 +53,7 @@ def save(name, hist, extra=None):
 
 
 def main():
-    # configs[0] of the reference: TOP3D_XL(true(25,50,25),'GLOBAL',0.12,50,sqrt(3)), first 10 iterations
+    # the small cuboid case: TOP3D_XL(true(25,50,25),'GLOBAL',0.12,50,sqrt(3)), first 10 iterations
     run = lambda: O.run_global(np.ones((25, 50, 25), bool), 0.12, 50, np.sqrt(3), max_loops=10)  # noqa: E731
     h = run()
     h["c"] = np.array(h["c"])

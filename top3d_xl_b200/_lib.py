@@ -88,6 +88,7 @@ SIGNATURES = {
     "topx_set_profiling": [_P, C.c_int],
     "topx_get_profile": [_P, C.POINTER(Profile)],
     "topx_profile_section_name": [C.c_int],
+    "topx_launch_count": [],
 }
 
 _lib = None
@@ -105,6 +106,6 @@ def load(path: str = LIB_PATH):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version", "topx_profile_section_name") \
-            else C.c_int
+            else C.c_int64 if name == "topx_launch_count" else C.c_int
     _lib = lib
     return lib

@@ -494,4 +494,6 @@ topx_status topx_get_profile(topx_ctx* ctx, topx_profile* out) {
   });
 }
 
+int64_t topx_launch_count(void) { return topx::launch_counter().load(); }
+
 }  // extern "C"

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(GL2_THREADS) k_galerkin_l2(Grid gc, const doub
 
 void launch_galerkin_l2(cudaStream_t st, Grid gc, const double* Efine, const double* Tm, double* Ks) {
   const int64_t nb = (gc.nelems() + GL2_ELEMS - 1) / GL2_ELEMS;
-  k_galerkin_l2<<<unsigned(nb), GL2_THREADS, 0, st>>>(gc, Efine, Tm, Ks);
+  (k_galerkin_l2<<<unsigned(nb), GL2_THREADS, 0, st>>>(gc, Efine, Tm, Ks), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(GL2_THREADS) k_galerkin_l2_flagged(Grid gc, co
 void launch_galerkin_l2_flagged(cudaStream_t st, Grid gc, const double* Efine, int nflag, const int32_t* fl_elem,
                                 const int32_t* fl_tsel, const double* fl_F, const double* Tall, double* Ks) {
   if (nflag <= 0) return;
-  k_galerkin_l2_flagged<<<nflag, GL2_THREADS, 0, st>>>(gc, Efine, fl_elem, fl_tsel, fl_F, Tall, Ks);
+  (k_galerkin_l2_flagged<<<nflag, GL2_THREADS, 0, st>>>(gc, Efine, fl_elem, fl_tsel, fl_F, Tall, Ks), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) k_galerkin_span2(Grid gc, const double* _
 
 void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* P8,
                            double* Ks) {
-  k_galerkin_span2<<<unsigned(gc.nelems()), 256, 0, st>>>(gc, Ksf, cpresent, P8, Ks);
+  (k_galerkin_span2<<<unsigned(gc.nelems()), 256, 0, st>>>(gc, Ksf, cpresent, P8, Ks), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -189,7 +189,7 @@ __global__ void k_diag_coarse(Grid g, const double* __restrict__ Ks, const uint8
 
 template <typename T>
 void launch_diag_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* present, T* d) {
-  k_diag_coarse<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, Ks, present, d);
+  (k_diag_coarse<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, Ks, present, d), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -265,7 +265,7 @@ void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks
                           double* Bup) {
   TOPX_CUDA_OK(cudaMemsetAsync(A, 0, sizeof(double) * size_t(si.m) * si.m * si.ns, st));
   const int64_t N = int64_t(si.nu) * si.nv * 18 * si.ns;
-  k_slab_assemble<<<grid1d(N, 256), 256, 0, st>>>(g, si, Ks, present, A, Bup);
+  (k_slab_assemble<<<grid1d(N, 256), 256, 0, st>>>(g, si, Ks, present, A, Bup), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -580,9 +580,9 @@ static void spd_inverse_batched(cudaStream_t st, int m, int nset, const GJSet& s
   const unsigned nt = (m + GJB - 1) / GJB;
   for (int k0 = 0; k0 < m; k0 += GJB) {
     const int kb = (m - k0) < GJB ? (m - k0) : GJB;
-    k_gj_pivot<<<dim3(1, 1, nset), 256, 0, st>>>(m, k0, kb, set);
-    k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set);
-    k_gj_update<<<dim3(nt, nt, nset), 256, 0, st>>>(m, k0, kb, set);
+    (k_gj_pivot<<<dim3(1, 1, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
+    (k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
+    (k_gj_update<<<dim3(nt, nt, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -624,7 +624,7 @@ void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const dou
       set.A[nset] = Sinv + s * mm;
       ++nset;
     }
-    k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]);
+    (k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]), topx::count_launch());
     spd_inverse_batched(st, m, nset, set);
     if (k < ntop) {  // L_k = B_k^T S_k^{-1}
       fo[nform++] = FormOp{Bup + k * bs, Sinv + k * mm, X + k * mm, XT + k * mm, 0};
@@ -633,13 +633,13 @@ void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const dou
       const int s = ns - 1 - k;
       fo[nform++] = FormOp{Bup + (s - 1) * bs, Sinv + s * mm, X + (s - 1) * mm, XT + (s - 1) * mm, 1};
     }
-    if (nform) k_form<<<dim3(nbm, nform), 256, 0, st>>>(si, fo[0], fo[1]);
+    if (nform) (k_form<<<dim3(nbm, nform), 256, 0, st>>>(si, fo[0], fo[1]), topx::count_launch());
   }
   // middle slab
   SchurOp sm{A + mid * mm, Sinv + mid * mm, mid > 0 ? X + (mid - 1) * mm : nullptr,
              mid > 0 ? Bup + (mid - 1) * bs : nullptr, mid < ns - 1 ? X + mid * mm : nullptr,
              mid < ns - 1 ? Bup + mid * bs : nullptr};
-  k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm);
+  (k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm), topx::count_launch());
   set.A[0] = Sinv + mid * mm;
   spd_inverse_batched(st, m, 1, set);
   TOPX_CUDA_OK(cudaGetLastError());
@@ -752,7 +752,7 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
   const int64_t N = int64_t(ns) * m;
   const int ntop = mid, nbot = ns - 1 - mid;
   const unsigned nb1 = unsigned((m + 1) / 2);
-  k_slab_gather<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, b, bs, sc);
+  (k_slab_gather<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, b, bs, sc), topx::count_launch());
   // chain heads
   if (ntop > 0) TOPX_CUDA_OK(cudaMemcpyAsync(W, bs, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
   if (nbot > 0)
@@ -770,7 +770,7 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
       ops[n++] = GemvOp{X + s * mm, W + int64_t(s + 1) * m, nullptr, nullptr, bs + int64_t(s) * m,
                         W + int64_t(s) * m, 1};
     }
-    k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc);
+    (k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc), topx::count_launch());
   }
   {  // middle
     GemvOp op{nullptr, nullptr, nullptr, nullptr, bs + int64_t(mid) * m, W + int64_t(mid) * m, 1};
@@ -788,13 +788,13 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
       }
     }
     if (op.M1)
-      k_slab_gemv<TM><<<dim3(nb1, 1), 256, 0, st>>>(m, op, op, sc);
+      (k_slab_gemv<TM><<<dim3(nb1, 1), 256, 0, st>>>(m, op, op, sc), topx::count_launch());
     else
       TOPX_CUDA_OK(cudaMemcpyAsync(W + int64_t(mid) * m, bs + int64_t(mid) * m, sizeof(double) * m,
                                    cudaMemcpyDeviceToDevice, st));
   }
   GemvOp ov{Inv, W, nullptr, nullptr, nullptr, V, ns};
-  k_slab_gemv<TM><<<dim3(grid1d(N / 2 + 1, 1, 148 * 32), 1), 256, 0, st>>>(m, ov, ov, sc);
+  (k_slab_gemv<TM><<<dim3(grid1d(N / 2 + 1, 1, 148 * 32), 1), 256, 0, st>>>(m, ov, ov, sc), topx::count_launch());
   TOPX_CUDA_OK(cudaMemcpyAsync(xs + int64_t(mid) * m, V + int64_t(mid) * m, sizeof(double) * m,
                                cudaMemcpyDeviceToDevice, st));
   // backward chains outward from the middle
@@ -811,9 +811,9 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
       ops[n++] = GemvOp{XT + (s - 1) * mm, xs + int64_t(s - 1) * m, nullptr, nullptr, V + int64_t(s) * m,
                         xs + int64_t(s) * m, 1};
     }
-    k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc);
+    (k_slab_gemv<TM><<<dim3(nb1, n), 256, 0, st>>>(m, ops[0], ops[1], sc), topx::count_launch());
   }
-  k_slab_scatter<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, xs, x, sc);
+  (k_slab_scatter<T><<<grid1d(N, 256), 256, 0, st>>>(g, si, xs, x, sc), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

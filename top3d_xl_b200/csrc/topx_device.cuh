@@ -7,12 +7,22 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 
 namespace topx {
 
 constexpr int kWarp = 32;
+
+// Process-wide count of this library's kernel launches.  Every launch site adds one;
+// launches recorded into a CUDA graph are taken back out after the capture, and each
+// replay of that graph adds its kernel-node count instead.
+inline std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> c{0};
+  return c;
+}
+inline void count_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
 
 // Device-resident scalars of one PCG solve (TOP3D_XL.m:600-639).  Written by
 // the last block of each reduction kernel, read by every later kernel, so a

@@ -272,7 +272,7 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
 }
 
 Engine::~Engine() {
-  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
   for (auto e : ev) cudaEventDestroy(e);
   for (auto e : sev) cudaEventDestroy(e);
   for (auto e : pev) cudaEventDestroy(e);
@@ -612,6 +612,7 @@ void Engine::run_graph(const std::string& key, const std::function<void()>& body
   auto it = graphs_.find(key);
   if (it == graphs_.end()) {
     cudaGraph_t g = nullptr;
+    const long long before = launch_counter().load();
     TOPX_CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
       body();
@@ -621,13 +622,16 @@ void Engine::run_graph(const std::string& key, const std::function<void()>& body
       throw;
     }
     TOPX_CUDA_OK(cudaStreamEndCapture(st, &g));
+    const long long recorded = launch_counter().load() - before;
+    launch_counter().fetch_sub(recorded);
     cudaGraphExec_t ex = nullptr;
     const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     TOPX_CUDA_OK(e);
-    it = graphs_.emplace(key, ex).first;
+    it = graphs_.emplace(key, GraphExec{ex, recorded}).first;
   }
-  TOPX_CUDA_OK(cudaGraphLaunch(it->second, st));
+  TOPX_CUDA_OK(cudaGraphLaunch(it->second.exec, st));
+  launch_counter().fetch_add(it->second.kernels);
 }
 
 const char* Engine::section_name(int s) {

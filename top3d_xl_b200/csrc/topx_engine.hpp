@@ -223,7 +223,11 @@ class Engine {
   void sec_harvest();
   // CUDA graphs of fixed launch sequences, keyed by name; captured on first use and replayed
   // (direct launches while profiling, so the section events stay on the stream)
-  std::map<std::string, cudaGraphExec_t> graphs_;
+  struct GraphExec {
+    cudaGraphExec_t exec;
+    long long kernels;  // kernel launches recorded into it
+  };
+  std::map<std::string, GraphExec> graphs_;
   void run_graph(const std::string& key, const std::function<void()>& body);
  public:
   bool use_graphs = true;

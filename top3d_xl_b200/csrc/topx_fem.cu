@@ -209,9 +209,9 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
   dim3 blk(KY, KX, 1);
   dim3 grd((g.nny() + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + KZC - 1) / KZC);
   if (mode == KU_PLAIN)
-    k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs);
+    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   else
-    k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs);
+    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -246,7 +246,7 @@ __global__ void k_diag_l1(Grid g, const TE* __restrict__ E, const uint8_t* __res
 template <typename TE, typename T>
 void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
                     const uint8_t* present, T* d) {
-  k_diag_l1<TE, T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, E, fixbits, cfix, present, d);
+  (k_diag_l1<TE, T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, E, fixbits, cfix, present, d), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -281,7 +281,7 @@ __global__ void k_residual_init(Grid g, const T* __restrict__ b, const T* __rest
 template <typename T>
 void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r, PcgScalars* sc, RedScratch rs,
                           double tol, int maxIT) {
-  k_residual_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, Ay, r, sc, rs, tol, maxIT);
+  (k_residual_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, Ay, r, sc, rs, tol, maxIT), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -347,7 +347,7 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
                        RedScratch rs) {
-  k_pcg_update<T, TY><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs);
+  (k_pcg_update<T, TY><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -395,15 +395,15 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
   const int cy = gc.nny(), cx = gc.nnx(), cz = gc.nnz();
   const int64_t s1 = int64_t(cy) * fx * fz, s2 = int64_t(cy) * cx * fz;
   if (span == 4) {
-    k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz);
-    k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz);
-    k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz);
+    (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz), topx::count_launch());
+    (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz), topx::count_launch());
+    (k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
+                                                                             cx, cz), topx::count_launch());
   } else {
-    k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz);
-    k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz);
-    k_restrict_axis<T, T, 2, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz);
+    (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz), topx::count_launch());
+    (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz), topx::count_launch());
+    (k_restrict_axis<T, T, 2, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
+                                                                             cx, cz), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -479,14 +479,14 @@ void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, con
   const T w = T(omega);
   if (span == 4) {
     if (dot)
-      k_prolong_smooth<TX, T, TD, 4, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
     else
-      k_prolong_smooth<TX, T, TD, 4, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
   } else {
     if (dot)
-      k_prolong_smooth<TX, T, TD, 2, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
     else
-      k_prolong_smooth<TX, T, TD, 2, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init);
+      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -501,7 +501,7 @@ __global__ void k_convert(const TA* __restrict__ a, TB* __restrict__ b, int64_t 
 }
 template <typename TA, typename TB>
 void launch_convert(cudaStream_t st, const TA* a, TB* b, int64_t n) {
-  k_convert<TA, TB><<<grid1d(n, 256), 256, 0, st>>>(a, b, n);
+  (k_convert<TA, TB><<<grid1d(n, 256), 256, 0, st>>>(a, b, n), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -517,7 +517,7 @@ __global__ void k_c2g_nodes(const double* __restrict__ src, T* __restrict__ dst,
 template <typename T>
 void launch_compact_to_grid_nodes(cudaStream_t st, const double* src, T* dst, Grid g, const int32_t* nodMapBack0,
                                   int64_t numNodes) {
-  k_c2g_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes);
+  (k_c2g_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 template <typename T>
@@ -531,7 +531,7 @@ __global__ void k_g2c_nodes(const T* __restrict__ src, double* __restrict__ dst,
 template <typename T>
 void launch_grid_to_compact_nodes(cudaStream_t st, const T* src, double* dst, Grid g, const int32_t* nodMapBack0,
                                   int64_t numNodes) {
-  k_g2c_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes);
+  (k_g2c_nodes<T><<<grid1d(numNodes, 256), 256, 0, st>>>(src, dst, g, nodMapBack0, numNodes), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -548,7 +548,7 @@ __global__ void k_simp_scatter(const double* __restrict__ x, const int32_t* __re
 }
 void launch_simp_scatter(cudaStream_t st, const double* xPhys, const int32_t* eleMapBack0, int64_t Ne, double Emin,
                          double E0, double penal, double* Ed, float* Ef) {
-  k_simp_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(xPhys, eleMapBack0, Ne, Emin, E0, penal, Ed, Ef);
+  (k_simp_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(xPhys, eleMapBack0, Ne, Emin, E0, penal, Ed, Ef), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -580,7 +580,7 @@ __global__ void k_unit_compliance(Grid g, const double* __restrict__ U, const in
 }
 void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int32_t* eleMapBack0, int64_t Ne,
                             double weight, bool accumulate, double* ce) {
-  k_unit_compliance<<<grid1d(Ne, 128), 128, 0, st>>>(g, U, eleMapBack0, Ne, weight, accumulate ? 1 : 0, ce);
+  (k_unit_compliance<<<grid1d(Ne, 128), 128, 0, st>>>(g, U, eleMapBack0, Ne, weight, accumulate ? 1 : 0, ce), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -627,7 +627,7 @@ __global__ void k_fill_scatter(const int32_t* __restrict__ emb0, int64_t Ne, dou
   }
 }
 void launch_fill_scatter(cudaStream_t st, const int32_t* eleMapBack0, int64_t Ne, double val, double* Ed, float* Ef) {
-  k_fill_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(eleMapBack0, Ne, val, Ed, Ef);
+  (k_fill_scatter<<<grid1d(Ne, 256), 256, 0, st>>>(eleMapBack0, Ne, val, Ed, Ef), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

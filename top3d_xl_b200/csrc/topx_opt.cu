@@ -55,7 +55,7 @@ __global__ void k_filter_e2n(Grid g, const T* __restrict__ srcE, T* __restrict__
 }
 template <typename T>
 void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node) {
-  k_filter_e2n<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, srcE, node);
+  (k_filter_e2n<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, srcE, node), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -77,7 +77,7 @@ __global__ void k_filter_diag(Grid g, const uint8_t* __restrict__ solid, int slo
 }
 template <typename T>
 void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, int slot, T* dp) {
-  k_filter_diag<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, solid, slot, dp);
+  (k_filter_diag<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, solid, slot, dp), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -166,9 +166,9 @@ void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, int slot, const T* i
   dim3 blk(FTY, FTX, FTZ);
   dim3 grd((g.nny() + FTY - 1) / FTY, (g.nnx() + FTX - 1) / FTX, (g.nnz() + FTZ - 1) / FTZ);
   if (mode == KU_PLAIN)
-    k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs);
+    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs), topx::count_launch());
   else
-    k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs);
+    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -203,7 +203,7 @@ __global__ void k_filter_init(Grid g, const T* __restrict__ b, const T* __restri
 template <typename T>
 void launch_filter_residual_init(cudaStream_t st, Grid g, const T* b, const T* dp, T* r, T* z, T* y, PcgScalars* sc,
                                  RedScratch rs, double tol, int maxIT) {
-  k_filter_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, dp, r, z, y, sc, rs, tol, maxIT);
+  (k_filter_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, dp, r, z, y, sc, rs, tol, maxIT), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -249,7 +249,7 @@ __global__ void k_filter_update(Grid g, T* __restrict__ y, T* __restrict__ p, T*
 template <typename T>
 void launch_filter_update(cudaStream_t st, Grid g, T* y, T* p, T* r, const T* q, const T* dp, T* z, PcgScalars* sc,
                           RedScratch rs) {
-  k_filter_update<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, r, q, dp, z, sc, rs);
+  (k_filter_update<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, r, q, dp, z, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -270,7 +270,7 @@ __global__ void k_filter_n2e(Grid g, const T* __restrict__ node, const int32_t* 
 }
 template <typename T>
 void launch_filter_n2e(cudaStream_t st, Grid g, const T* node, const int32_t* eleMapBack0, int64_t Ne, double* out) {
-  k_filter_n2e<T><<<grid1d(Ne, 256), 256, 0, st>>>(g, node, eleMapBack0, Ne, out);
+  (k_filter_n2e<T><<<grid1d(Ne, 256), 256, 0, st>>>(g, node, eleMapBack0, Ne, out), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -282,7 +282,7 @@ __global__ void k_scatter_elems(const double* __restrict__ src, const int32_t* _
 }
 template <typename T>
 void launch_scatter_elems_t(cudaStream_t st, const double* src, const int32_t* eleMapBack0, int64_t Ne, T* dstE) {
-  k_scatter_elems<T><<<grid1d(Ne, 256), 256, 0, st>>>(src, eleMapBack0, Ne, dstE);
+  (k_scatter_elems<T><<<grid1d(Ne, 256), 256, 0, st>>>(src, eleMapBack0, Ne, dstE), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -310,7 +310,7 @@ __global__ void k_objective(int64_t Ne, const double* __restrict__ ce, const dou
 }
 void launch_objective(cudaStream_t st, int64_t Ne, const double* ce, const double* xPhys, double cSolid, double Emin,
                       double E0, double penal, double* dc, ObjState* os, RedScratch rs) {
-  k_objective<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, ce, xPhys, cSolid, Emin, E0, penal, dc, os, rs);
+  (k_objective<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, ce, xPhys, cSolid, Emin, E0, penal, dc, os, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -323,7 +323,7 @@ __global__ void k_dot(int64_t n, const double* __restrict__ a, const double* __r
   if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) *out = tot[0];
 }
 void launch_sum(cudaStream_t st, int64_t n, const double* a, const double* b, double* out, RedScratch rs) {
-  k_dot<<<grid1d(n, 256), 256, 0, st>>>(n, a, b, out, rs);
+  (k_dot<<<grid1d(n, 256), 256, 0, st>>>(n, a, b, out, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -345,7 +345,7 @@ __global__ void k_ewise(int op, int64_t n, const double* __restrict__ a, const d
   }
 }
 void launch_ewise(cudaStream_t st, int op, int64_t n, const double* a, const double* b, double* out, double s) {
-  k_ewise<<<grid1d(n, 256), 256, 0, st>>>(op, n, a, b, out, s);
+  (k_ewise<<<grid1d(n, 256), 256, 0, st>>>(op, n, a, b, out, s), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -383,7 +383,7 @@ __global__ void k_oc_step(int64_t Ne, const double* __restrict__ x, const double
 }
 void launch_oc_step(cudaStream_t st, int64_t Ne, const double* x, const double* dc, const uint8_t* passive,
                     OcState* os, RedScratch rs, double move) {
-  k_oc_step<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, os, rs, move);
+  (k_oc_step<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, os, rs, move), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -409,7 +409,7 @@ __global__ void k_oc_final(int64_t Ne, double* __restrict__ x, const double* __r
 }
 void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* dc, const uint8_t* passive, double* xPhys,
                      OcState* os, RedScratch rs, RedScratch rs2, double move) {
-  k_oc_final<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, xPhys, os, rs, rs2, move);
+  (k_oc_final<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, xPhys, os, rs, rs2, move), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -514,8 +514,8 @@ void launch_mma_gensub(cudaStream_t st, int64_t n, int iter, double move, const 
                        double* xold1, double* xold2, double* low, double* upp, const double* dfdx, const double* dgdx,
                        double gx, int64_t nact, double* alpha, double* beta, double* p0, double* q0, double* pij,
                        double* qij, MmaState* ms, RedScratch rs) {
-  k_mma_gensub<<<grid1d(n, 256), 256, 0, st>>>(n, iter, move, xval, passive, xold1, xold2, low, upp, dfdx, dgdx, gx,
-                                                nact, alpha, beta, p0, q0, pij, qij, ms, rs);
+  (k_mma_gensub<<<grid1d(n, 256), 256, 0, st>>>(n, iter, move, xval, passive, xold1, xold2, low, upp, dfdx, dgdx, gx,
+                                                nact, alpha, beta, p0, q0, pij, qij, ms, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -582,7 +582,7 @@ __global__ void k_mma_newton(int64_t n, const uint8_t* __restrict__ passive, con
 void launch_mma_newton(cudaStream_t st, int64_t n, const uint8_t* passive, const double* low, const double* upp,
                        const double* alpha, const double* beta, const double* p0, const double* q0, const double* pij,
                        const double* qij, MmaState* ms, RedScratch rs) {
-  k_mma_newton<<<grid1d(n, 256), 256, 0, st>>>(n, passive, low, upp, alpha, beta, p0, q0, pij, qij, ms, rs);
+  (k_mma_newton<<<grid1d(n, 256), 256, 0, st>>>(n, passive, low, upp, alpha, beta, p0, q0, pij, qij, ms, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -628,7 +628,7 @@ __global__ void k_mma_residual(int64_t n, const uint8_t* __restrict__ passive, c
 void launch_mma_residual(cudaStream_t st, int64_t n, const uint8_t* passive, const double* low, const double* upp,
                          const double* alpha, const double* beta, const double* p0, const double* q0,
                          const double* pij, const double* qij, double* x, MmaState* ms, RedScratch rs) {
-  k_mma_residual<<<grid1d(n, 256), 256, 0, st>>>(n, passive, low, upp, alpha, beta, p0, q0, pij, qij, x, ms, rs);
+  (k_mma_residual<<<grid1d(n, 256), 256, 0, st>>>(n, passive, low, upp, alpha, beta, p0, q0, pij, qij, x, ms, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -650,7 +650,7 @@ __global__ void k_mma_finish(int64_t n, const uint8_t* __restrict__ passive, con
 
 void launch_mma_finish(cudaStream_t st, int64_t n, const uint8_t* passive, const double* xmma, const double* xold1,
                        double* x, MmaState* ms, RedScratch rs) {
-  k_mma_finish<<<grid1d(n, 256), 256, 0, st>>>(n, passive, xmma, xold1, x, ms, rs);
+  (k_mma_finish<<<grid1d(n, 256), 256, 0, st>>>(n, passive, xmma, xold1, x, ms, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -668,7 +668,7 @@ __global__ void k_pnorm(int64_t Ne, const double* __restrict__ xhat, double Ve0,
 }
 void launch_pnorm_terms(cudaStream_t st, int64_t Ne, const double* xhat, double Ve0, int pPIO, double* out_sum,
                         RedScratch rs) {
-  k_pnorm<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xhat, Ve0, double(pPIO), out_sum, rs);
+  (k_pnorm<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xhat, Ve0, double(pPIO), out_sum, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -689,8 +689,8 @@ __global__ void k_local_sens(int64_t Ne, const double* __restrict__ xhat, const 
 void launch_local_sens(cudaStream_t st, int64_t Ne, const double* xhat, const double* xTilde, const double* dc,
                        double Ve0, int pPIO, double pn, double betaPIO, double etaPIO, double* dfdx_pde, double* dx,
                        double* dcdx) {
-  k_local_sens<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xhat, xTilde, dc, Ve0, double(pPIO), pn, betaPIO, etaPIO,
-                                                dfdx_pde, dx, dcdx);
+  (k_local_sens<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xhat, xTilde, dc, Ve0, double(pPIO), pn, betaPIO, etaPIO,
+                                                dfdx_pde, dx, dcdx), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -709,7 +709,7 @@ __global__ void k_heaviside(int64_t Ne, const double* __restrict__ xTilde, const
 }
 void launch_heaviside(cudaStream_t st, int64_t Ne, const double* xTilde, const uint8_t* passive, double betaPIO,
                       double etaPIO, double* xPhys, double* sharpsum, RedScratch rs) {
-  k_heaviside<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xTilde, passive, betaPIO, etaPIO, xPhys, sharpsum, rs);
+  (k_heaviside<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, xTilde, passive, betaPIO, etaPIO, xPhys, sharpsum, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

@@ -206,6 +206,10 @@ class Context:
                     for i in range(L.NSECTIONS)}
         return dict(ku_ms=p.ku_ms, ku_launches=p.ku_launches, pcg_iterations=p.pcg_iterations, sections=sections)
 
+    def launch_count(self):
+        """Kernels launched by the library in this process so far (graph replays included)."""
+        return int(self.lib.topx_launch_count())
+
     def density(self):
         out = np.empty(self.numElements)
         self._check(self.lib.topx_get_density(self._h, _dptr(out), out.size))
