@@ -40,9 +40,10 @@ WORKLOADS = {
     "cuboid25": dict(shape=(25, 50, 25), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
 }
 METRIC = "OC iterations/s (GLOBAL, mixed precision; FP64 beside it)"
-# DRAM bytes (read + write) per node of one K*u launch in PCG mode, from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum); None until measured.
-KU_TRAFFIC_PER_NODE = None
+# DRAM bytes (read + write) per grid node of one K*u launch in PCG mode, from an ncu capture of
+# the 128x256x128 cuboid (dram__bytes_read.sum + dram__bytes_write.sum = 259.68 MB + 86.09 MB
+# over 4,276,737 nodes); the traffic of a launch scales with its node count.
+KU_TRAFFIC_PER_NODE = 345.77e6 / 4276737
 # Nominal FP64 rate of a B200 on CUDA cores: 148 SMs x 64 FMA/clk x 2 flop x 1.965 GHz.
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
@@ -139,7 +140,7 @@ def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False
         prof = ctx.profile()
         prof["steps"] = profile_steps
         ctx.set_profiling(False)
-    out = dict(ms=ms, wall=wall, hist=hist, prof=prof, launches=launches, ne=ctx.numElements, ndof=ctx.numDOFs,
+    out = dict(ms=ms, wall=wall, hist=hist, prof=prof, launches=launches, launches_before=launches0, ne=ctx.numElements, ndof=ctx.numDOFs,
                nnodes=int(ctx.info.numNodes))
     if keep:
         out["ctx"] = ctx
@@ -266,6 +267,7 @@ def main(argv=None):
     if a.only:
         r = run_native(wl, a.only, a.steps, a.warmup, device, profile_steps=1)
         print(json.dumps({"only": a.only, "ms_per_step": r["ms"] / max(1, a.steps),
+                          "launches_before_timed": r["launches_before"], "launches_timed": r["launches"],
                           "pcg_its": [k for h in r["hist"] for k in h["its"]],
                           "ku_ms_per_launch": r["prof"]["ku_ms"] / max(1, r["prof"]["ku_launches"]),
                           "sections_ms_per_profiled_step": {k: v[0] for k, v in r["prof"]["sections"].items()}}),
