@@ -131,6 +131,16 @@ topx_status topx_get_load(const topx_ctx* ctx, int lc, double* out, size_t n);
 topx_status topx_set_moduli(topx_ctx* ctx, const double* E, size_t n);
 /* Solving_KbyU_MatrixFree, level 1 (TX:641-725): y = K(E) u, FP64 */
 topx_status topx_ku(topx_ctx* ctx, const double* u, double* y, size_t ndof);
+/* No counterpart in the reference.  y = K(E) u exactly like topx_ku, but u and y are device
+   pointers (ndof doubles each, on the context's GPU) and the call allocates no device memory:
+   topx_ku allocates temporary device buffers on every call, which callers whose device memory
+   is owned by another allocator (MATLAB gpuArray, a framework's caching pool) or whose loop may
+   not call cudaMalloc/cudaFree cannot accept.  Its scratch is one fixed 32 MiB static device
+   array, enough for level-1 grids of up to 699,040 padded nodes; larger models get
+   TOPX_ERR_ARG.  The context's device state must exist already (e.g. after topx_set_moduli).
+   The first call on each GPU looks up the array's address; make it before any stream capture.
+   All calls share the array: calls that overlap on the GPU race.  Returns after y is written. */
+topx_status topx_ku_noalloc(topx_ctx* ctx, const double* u_dev, double* y_dev, size_t ndof);
 /* Solving_AssembleFEAstencil (TX:919-1066) for the current moduli */
 topx_status topx_assemble(topx_ctx* ctx);
 /* Solving_Vcycle (TX:747-781): z = M r in the context's precision */

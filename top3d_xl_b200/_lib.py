@@ -70,6 +70,7 @@ SIGNATURES = {
     "topx_get_load": [_P, C.c_int, _D, _SZ],
     "topx_set_moduli": [_P, _D, _SZ],
     "topx_ku": [_P, _D, _D, _SZ],
+    "topx_ku_noalloc": [_P, C.c_void_p, C.c_void_p, _SZ],
     "topx_assemble": [_P],
     "topx_vcycle": [_P, _D, _D, _SZ],
     "topx_get_diag": [_P, C.c_int, _D, _SZ],

@@ -101,6 +101,30 @@ void fill_iter(topx_iter* out, const topx::IterRecord& r) {
   out->t_total = r.t_total;
 }
 
+// Restores the caller's current device when the call returns or throws.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    TOPX_CUDA_OK(cudaGetDevice(&prev));
+    if (prev != dev) TOPX_CUDA_OK(cudaSetDevice(dev));
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Accept only memory that kernels on `dev` can dereference at this address.
+bool on_device(const void* p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 }  // namespace
 
 extern "C" {
@@ -311,6 +335,31 @@ topx_status topx_ku(topx_ctx* ctx, const double* u, double* y, size_t ndof) {
     if (s != TOPX_OK) return s;
     if (!u || !y || ndof != size_t(ctx->engine->Nn) * 3) return fail(ctx, TOPX_ERR_ARG, "DOF size mismatch");
     ctx->engine->apply_K(u, y);
+    return TOPX_OK;
+  });
+}
+
+topx_status topx_ku_noalloc(topx_ctx* ctx, const double* u_dev, double* y_dev, size_t ndof) {
+  return guarded(ctx, [&]() -> topx_status {
+    if (!ctx->engine)
+      return fail(ctx, TOPX_ERR_STATE,
+                  "topx_ku_noalloc: the context has no device state yet; create it first with an allocating "
+                  "call such as topx_set_moduli");
+    topx::Engine& eng = *ctx->engine;
+    if (!u_dev || !y_dev || ndof != size_t(eng.Nn) * 3) return fail(ctx, TOPX_ERR_ARG, "DOF size mismatch");
+    const size_t grid = size_t(eng.G[0].stride) * 3;
+    const size_t need = 2 * grid * sizeof(double);
+    if (need > topx::noalloc_scratch_bytes())
+      return fail(ctx, TOPX_ERR_ARG,
+                  "topx_ku_noalloc: this model needs " + std::to_string(need) + " bytes of scratch (2 x 3 x " +
+                      std::to_string(eng.G[0].stride) + " padded grid nodes x 8 B); the fixed scratch holds " +
+                      std::to_string(topx::noalloc_scratch_bytes()) + " bytes; use topx_ku for this model");
+    DeviceScope scope(ctx->params.device);
+    if (!on_device(u_dev, ctx->params.device) || !on_device(y_dev, ctx->params.device))
+      return fail(ctx, TOPX_ERR_ARG, "topx_ku_noalloc: u and y must be device (or managed) memory of the "
+                                     "context's GPU");
+    double* s = topx::noalloc_scratch(ctx->params.device);
+    eng.apply_K_device(u_dev, y_dev, s, s + grid);
     return TOPX_OK;
   });
 }

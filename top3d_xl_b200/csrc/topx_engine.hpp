@@ -119,6 +119,8 @@ class Engine {
   void compliance_host(const double* h_U, double* h_ce);
   // for tests: y = K u (FP64), z = M r (V-cycle in the engine precision)
   void apply_K(const double* h_u, double* h_y);
+  // y = K u on device vectors (compact DOF order) with caller-provided grid scratch; topx_noalloc.cu
+  void apply_K_device(const double* d_u, double* d_y, double* grid_u, double* grid_y);
   void apply_vcycle(const double* h_r, double* h_z);
   void get_diag(int level, double* h_d) const;
 
@@ -233,5 +235,10 @@ class Engine {
   bool use_graphs = true;
   cudaEvent_t tev[2] = {nullptr, nullptr};
 };
+
+// Fixed device scratch of the allocation-free operator call (topx_noalloc.cu): its size in
+// bytes, and its device address on `device`, which must be current (looked up once per device).
+size_t noalloc_scratch_bytes();
+double* noalloc_scratch(int device);
 
 }  // namespace topx
