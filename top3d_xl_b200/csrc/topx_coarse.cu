@@ -370,14 +370,21 @@ __global__ void k_form(SlabInfo si, FormOp op0, FormOp op1) {
 // batched over up to two matrices (grid z).  One exchange step on pivot block K:
 //   [P B; C D] -> [P^-1, -P^-1 B; C P^-1, D - C P^-1 B]
 // After all blocks the matrix holds its inverse.  No pivoting is needed for SPD.
+// Three launches per step:
+//   k_gj_pivot   CTA 0: P^-1 (register-blocked exchange on the 64x64 block);
+//                CTAs 1..: Ct = (old column panel A[:, K])^T, through a shared transpose
+//   k_gj_panel   R = -P^-1 A[K, :]
+//   k_gj_update  A[i, j] += C_i R_j,  A[i, K] = C_i P^-1,  A[K, :] = R (P^-1 on the diagonal)
 // ---------------------------------------------------------------------------
 constexpr int GJB = 64;  // pivot block width (= update tile)
+constexpr int GJ_PIVOT_THREADS = 128;
+constexpr size_t GJ_UPDATE_SMEM = 2 * GJB * GJB * sizeof(double);
 
 struct GJSet {
   double* A[2];
   double* Pinv[2];
-  double* R[2];
-  double* C[2];
+  double* R[2];   // 64 x m
+  double* Ct[2];  // 64 x m
 };
 
 // 1/v by Newton-Raphson iteration x <- x (2 - v x) from a single-precision seed
@@ -390,94 +397,123 @@ __device__ __forceinline__ double recip_newton(double v) {
   return x;
 }
 
-// pivot block P = A[K,K] -> Pinv.  One CTA of 256 threads; thread t holds row
-// t/4, columns 16*(t%4)..+15 of the block in registers; each exchange step
-// publishes the pivot row/column through double-buffered shared arrays (one
-// barrier per step).
-__global__ void __launch_bounds__(256) k_gj_pivot(int m, int k0, int kb, GJSet set) {
-  const bool z1 = blockIdx.z != 0;
-  const double* __restrict__ A = z1 ? set.A[1] : set.A[0];
-  double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
-  // rowb is padded by one slot per 16 columns: the four column groups a warp reads
-  // at the same q then fall into different banks
-  __shared__ double colb[2][GJB], rowb[2][GJB + 4], rpb[2];
+// CTA 0: P = A[K,K] -> Pinv.  Thread (ri, ci) = (tid / 16, tid % 16) holds rows 8ri..8ri+7 and
+// columns 4ci..4ci+3 of the block in registers.  Each exchange step publishes the pivot row,
+// the pivot column and 1/pivot through double-buffered shared arrays (one barrier per step);
+// every element then takes one FMA and the owners of the pivot row and column overwrite theirs.
+// Rows and columns >= kb hold the identity, which the exchange leaves unchanged.
+// CTAs 1..: 64 rows each of the old column panel, transposed into Ct.
+__global__ void __launch_bounds__(GJ_PIVOT_THREADS) k_gj_pivot(int m, int k0, int kb, GJSet set) {
+  const int z = blockIdx.z;
+  const double* __restrict__ A = z ? set.A[1] : set.A[0];
   const int tid = threadIdx.x;
-  const int r = tid >> 2, c0 = (tid & 3) * 16, cpad = c0 + (c0 >> 4);
-  double a[16];
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int c = c0 + q;
-    a[q] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
+  if (blockIdx.x > 0) {
+    __shared__ double tile[GJB][GJB + 1];
+    double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
+    const int i0 = (blockIdx.x - 1) * GJB;
+#pragma unroll 8
+    for (int e = tid; e < GJB * GJB; e += GJ_PIVOT_THREADS) {
+      const int rr = e / GJB, t = e % GJB;
+      const int ii = i0 + rr;
+      tile[rr][t] = (ii < m && t < kb) ? A[int64_t(ii) * m + k0 + t] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int e = tid; e < GJB * GJB; e += GJ_PIVOT_THREADS) {
+      const int t = e / GJB, rr = e % GJB;
+      const int ii = i0 + rr;
+      if (ii < m && t < kb) Ct[int64_t(t) * m + ii] = tile[rr][t];
+    }
+    return;
   }
-  for (int tb = 0; tb < GJB / 16; ++tb) {
+  double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
+  __shared__ __align__(16) double rowb[2][GJB];
+  __shared__ __align__(16) double colb[2][GJB];
+  __shared__ double rpb[2];
+  const int ci = tid & 15, ri = tid >> 4;
+  double a[8][4];
 #pragma unroll
-    for (int qq = 0; qq < 16; ++qq) {
-      const int t = 16 * tb + qq;
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = 8 * ri + i, c = 4 * ci + q;
+      a[i][q] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
+    }
+  for (int tb = 0; tb < GJB / 8; ++tb) {
+    if (8 * tb >= kb) break;
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) {
+      const int t = 8 * tb + qq;
       if (t >= kb) break;
-      const int buf = t & 1;
-      if (c0 == 16 * tb) {
-        colb[buf][r] = a[qq];
-        if (r == t) rpb[buf] = recip_newton(a[qq]);
+      const int buf = qq & 1;  // = t & 1
+      const int cq = qq & 3;   // local column of pivot column t in its owners
+      const bool rowOwner = (ri == tb);
+      const bool colOwner = (ci == 2 * tb + (qq >> 2));
+      if (rowOwner) {
+        *reinterpret_cast<double2*>(&rowb[buf][4 * ci]) = make_double2(a[qq][0], a[qq][1]);
+        *reinterpret_cast<double2*>(&rowb[buf][4 * ci + 2]) = make_double2(a[qq][2], a[qq][3]);
+        if (colOwner) rpb[buf] = recip_newton(a[qq][cq]);
       }
-      if (r == t) {
+      if (colOwner) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) rowb[buf][cpad + q] = a[q];
+        for (int i = 0; i < 8; i += 2)
+          *reinterpret_cast<double2*>(&colb[buf][8 * ri + i]) = make_double2(a[i][cq], a[i + 1][cq]);
       }
       __syncthreads();
       const double rp = rpb[buf];
-      const double cr = colb[buf][r] * rp;
+      const double2 r01 = *reinterpret_cast<const double2*>(&rowb[buf][4 * ci]);
+      const double2 r23 = *reinterpret_cast<const double2*>(&rowb[buf][4 * ci + 2]);
+      const double rc[4] = {r01.x, r01.y, r23.x, r23.y};
+      double cr[8];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int c = c0 + q;
-        const double rc = rowb[buf][cpad + q];
-        double v;
-        if (r == t)
-          v = (c == t) ? rp : -rc * rp;
-        else
-          v = (c == t) ? cr : fma(-cr, rc, a[q]);
-        a[q] = v;
+      for (int i = 0; i < 8; i += 2) {
+        const double2 cv = *reinterpret_cast<const double2*>(&colb[buf][8 * ri + i]);
+        cr[i] = cv.x * rp;
+        cr[i + 1] = cv.y * rp;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[i][q] = fma(-cr[i], rc[q], a[i][q]);
+      if (rowOwner) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[qq][q] = -rc[q] * rp;
+      }
+      if (colOwner) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i][cq] = cr[i];
+        if (rowOwner) a[qq][cq] = rp;
       }
     }
   }
 #pragma unroll
-  for (int q = 0; q < 16; ++q) Pinv[r * GJB + c0 + q] = a[q];
-}
-
-// 64x64 tile product helper: acc[4][4] += X[rows 4ty..][t] * Y[t][cols 4tx..] over 32 values of t
-__device__ __forceinline__ void tile_fma(const double (*sX)[33], const double (*sY)[68], int ty, int tx,
-                                         double (&acc)[4][4]) {
-#pragma unroll 8
-  for (int t = 0; t < 32; ++t) {
-    double xv[4], yv[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = sX[4 * ty + q][t];
-    const double2 y01 = *reinterpret_cast<const double2*>(&sY[t][4 * tx]);
-    const double2 y23 = *reinterpret_cast<const double2*>(&sY[t][4 * tx + 2]);
-    yv[0] = y01.x;
-    yv[1] = y01.y;
-    yv[2] = y23.x;
-    yv[3] = y23.y;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int w = 0; w < 4; ++w) acc[q][w] = fma(xv[q], yv[w], acc[q][w]);
+  for (int i = 0; i < 8; ++i) {
+    double* dst = Pinv + (8 * ri + i) * GJB + 4 * ci;
+    *reinterpret_cast<double2*>(dst) = make_double2(a[i][0], a[i][1]);
+    *reinterpret_cast<double2*>(dst + 2) = make_double2(a[i][2], a[i][3]);
   }
 }
 
-// row panel R[:, j] = -Pinv A[K, j] (j not in K): CTA (x: 64 columns, y: 16 of the kb rows),
-// and the old column panel C[j, :] = A[j, K] for 16 of the CTA's 64 rows
+// row panel R[kt][j] = -sum_t Pinv[kt][t] A[k0 + t][j] for the columns outside the pivot block.
+// CTA (x: 64 columns, y: 16 of the 64 pivot rows); thread: one row, four columns.
 __global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet set) {
-  const bool z1 = blockIdx.z != 0;
-  const double* __restrict__ A = z1 ? set.A[1] : set.A[0];
-  const double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
-  double* __restrict__ R = z1 ? set.R[1] : set.R[0];
-  double* __restrict__ C = z1 ? set.C[1] : set.C[0];
-  __shared__ double sP[16][GJB + 1];
-  __shared__ __align__(16) double sA[GJB][68];
-  const int tid = threadIdx.x;
+  const int z = blockIdx.z;
   const int j0 = blockIdx.x * GJB, r0 = blockIdx.y * 16;
-  for (int i = tid; i < 16 * GJB; i += 256) sP[i / GJB][i % GJB] = Pinv[(r0 + i / GJB) * GJB + i % GJB];
-  for (int i = tid; i < GJB * GJB; i += 256) {
+  if (j0 == k0 || r0 >= kb) return;
+  const double* __restrict__ A = z ? set.A[1] : set.A[0];
+  const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
+  double* __restrict__ R = z ? set.R[1] : set.R[0];
+  __shared__ double sP[16][GJB + 1];
+  __shared__ __align__(16) double sA[GJB][GJB + 4];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int i = tid + 256 * e;
+    sP[i / GJB][i % GJB] = Pinv[(r0 + i / GJB) * GJB + i % GJB];
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int i = tid + 256 * e;
     const int t = i / GJB, cc = i % GJB;
     const int j = j0 + cc;
     sA[t][cc] = (t < kb && j < m) ? A[int64_t(k0 + t) * m + j] : 0.0;
@@ -485,7 +521,8 @@ __global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet s
   __syncthreads();
   const int rr = tid >> 4, cx = (tid & 15) * 4;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int t = 0; t < kb; ++t) {
+#pragma unroll 16
+  for (int t = 0; t < GJB; ++t) {
     const double p = sP[rr][t];
     const double2 a01 = *reinterpret_cast<const double2*>(&sA[t][cx]);
     const double2 a23 = *reinterpret_cast<const double2*>(&sA[t][cx + 2]);
@@ -498,24 +535,23 @@ __global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet s
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
       const int j = j0 + cx + w;
-      if (j < m && (j < k0 || j >= k0 + kb)) R[int64_t(r0 + rr) * m + j] = -acc[w];
+      if (j < m) R[int64_t(r0 + rr) * m + j] = -acc[w];
     }
-  }
-  for (int i = tid; i < 16 * GJB; i += 256) {
-    const int row = j0 + r0 + i / GJB, t = i % GJB;
-    if (row < m && (row < k0 || row >= k0 + kb) && t < kb) C[int64_t(row) * GJB + t] = A[int64_t(row) * m + k0 + t];
   }
 }
 
-// rank-kb exchange update of every 64x64 tile (4x4 outputs per thread)
-__global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, GJSet set) {
-  const bool z1 = blockIdx.z != 0;
-  double* __restrict__ A = z1 ? set.A[1] : set.A[0];
-  const double* __restrict__ Pinv = z1 ? set.Pinv[1] : set.Pinv[0];
-  const double* __restrict__ R = z1 ? set.R[1] : set.R[0];
-  const double* __restrict__ C = z1 ? set.C[1] : set.C[0];
-  __shared__ double sX[GJB][33];
-  __shared__ __align__(16) double sY[32][68];
+// rank-kb exchange update of one 64x64 tile per CTA (4x4 outputs per thread); both rank-64
+// operands (Ct rows of this tile, R or Pinv columns) come in with one round of loads, and the
+// old tile is fetched into registers before the product.
+__global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJSet set) {
+  extern __shared__ __align__(16) double gj_smem[];
+  double(*sC)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem);            // [kt][row]
+  double(*sR)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem + GJB * GJB);  // [kt][col]
+  const int z = blockIdx.z;
+  double* __restrict__ A = z ? set.A[1] : set.A[0];
+  const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
+  const double* __restrict__ R = z ? set.R[1] : set.R[0];
+  const double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int i0 = blockIdx.y * GJB, j0 = blockIdx.x * GJB;
   const bool iK = (i0 == k0), jK = (j0 == k0);
@@ -527,23 +563,48 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, GJSet 
     }
     return;
   }
-  double acc[4][4] = {};
-  for (int h = 0; h < 2; ++h) {
-    for (int i = tid; i < GJB * 32; i += 256) {
-      const int rr = i / 32, t = i % 32;
-      const int ii = i0 + rr, kt = 32 * h + t;
-      sX[rr][t] = (ii < m && kt < kb) ? C[int64_t(ii) * GJB + kt] : 0.0;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int i = tid + 256 * e;
+    const int kt = i >> 6, rr = i & 63;
+    const int ii = i0 + rr;
+    sC[kt][rr] = (kt < kb && ii < m) ? Ct[int64_t(kt) * m + ii] : 0.0;
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int i = tid + 256 * e;
+    const int kt = i >> 6, cc = i & 63;
+    const int j = j0 + cc;
+    double v = 0.0;
+    if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + cc] : R[int64_t(kt) * m + j];
+    sR[kt][cc] = v;
+  }
+  double old[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int ii = i0 + 4 * ty + q, j = j0 + 4 * tx + w;
+      old[q][w] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
     }
-    for (int i = tid; i < 32 * GJB; i += 256) {
-      const int t = i / GJB, cc = i % GJB;
-      const int kt = 32 * h + t, j = j0 + cc;
-      double v = 0.0;
-      if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + cc] : R[int64_t(kt) * m + j];
-      sY[t][cc] = v;
-    }
-    __syncthreads();
-    tile_fma(sX, sY, ty, tx, acc);
-    __syncthreads();
+  __syncthreads();
+  double acc[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) acc[q][w] = old[q][w];
+#pragma unroll 8
+  for (int k = 0; k < GJB; ++k) {
+    const double2 c01 = *reinterpret_cast<const double2*>(&sC[k][4 * ty]);
+    const double2 c23 = *reinterpret_cast<const double2*>(&sC[k][4 * ty + 2]);
+    const double2 r01 = *reinterpret_cast<const double2*>(&sR[k][4 * tx]);
+    const double2 r23 = *reinterpret_cast<const double2*>(&sR[k][4 * tx + 2]);
+    const double cv[4] = {c01.x, c01.y, c23.x, c23.y};
+    const double rv[4] = {r01.x, r01.y, r23.x, r23.y};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) acc[q][w] = fma(cv[q], rv[w], acc[q][w]);
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -551,44 +612,36 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int k0, int kb, GJSet 
     if (ii >= m) continue;
     const int jb = j0 + 4 * tx;
     double* Ar = A + int64_t(ii) * m;
-    // 16-byte path only when the absolute address is 16-byte aligned (matrix bases
+    // 16-byte stores only where the absolute address is 16-byte aligned (matrix bases
     // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
     if (jb + 3 < m && (reinterpret_cast<uintptr_t>(Ar + jb) & 15) == 0) {
-      double2 v0 = *reinterpret_cast<double2*>(Ar + jb), v1 = *reinterpret_cast<double2*>(Ar + jb + 2);
-      if (jK) {
-        v0 = make_double2(acc[q][0], acc[q][1]);
-        v1 = make_double2(acc[q][2], acc[q][3]);
-      } else {
-        v0.x += acc[q][0];
-        v0.y += acc[q][1];
-        v1.x += acc[q][2];
-        v1.y += acc[q][3];
-      }
-      *reinterpret_cast<double2*>(Ar + jb) = v0;
-      *reinterpret_cast<double2*>(Ar + jb + 2) = v1;
+      *reinterpret_cast<double2*>(Ar + jb) = make_double2(acc[q][0], acc[q][1]);
+      *reinterpret_cast<double2*>(Ar + jb + 2) = make_double2(acc[q][2], acc[q][3]);
     } else {
 #pragma unroll
-      for (int w = 0; w < 4; ++w) {
-        const int j = jb + w;
-        if (j < m) Ar[j] = jK ? acc[q][w] : Ar[j] + acc[q][w];
-      }
+      for (int w = 0; w < 4; ++w)
+        if (jb + w < m) Ar[jb + w] = acc[q][w];
     }
   }
+}
+
+void prepare_coarse_kernels() {
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(GJ_UPDATE_SMEM)));
 }
 
 static void spd_inverse_batched(cudaStream_t st, int m, int nset, const GJSet& set) {
   const unsigned nt = (m + GJB - 1) / GJB;
   for (int k0 = 0; k0 < m; k0 += GJB) {
     const int kb = (m - k0) < GJB ? (m - k0) : GJB;
-    (k_gj_pivot<<<dim3(1, 1, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
+    (k_gj_pivot<<<dim3(1 + nt, 1, nset), GJ_PIVOT_THREADS, 0, st>>>(m, k0, kb, set), topx::count_launch());
     (k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
-    (k_gj_update<<<dim3(nt, nt, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
+    (k_gj_update<<<dim3(nt, nt, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C) {
-  GJSet set{{A, A}, {Pinv, Pinv}, {R, R}, {C, C}};
+void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* Ct) {
+  GJSet set{{A, A}, {Pinv, Pinv}, {R, R}, {Ct, Ct}};
   spd_inverse_batched(st, m, 1, set);
 }
 
@@ -598,13 +651,13 @@ void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const dou
   const int64_t mm = int64_t(m) * m;
   const int64_t bs = int64_t(si.nu) * si.nv * 81;
   const unsigned nbm = grid1d(mm, 256);
-  // per chain scratch: Pinv 64x64, R 64xm, C mx64
+  // per chain scratch: Pinv 64x64, R 64xm, Ct 64xm
   const int64_t gjs = 64 * 64 + 2 * 64 * int64_t(m);
   GJSet set{};
   for (int c = 0; c < 2; ++c) {
     set.Pinv[c] = gj_scratch + c * gjs;
     set.R[c] = set.Pinv[c] + 64 * 64;
-    set.C[c] = set.R[c] + 64 * int64_t(m);
+    set.Ct[c] = set.R[c] + 64 * int64_t(m);
   }
   const int ntop = mid, nbot = ns - 1 - mid;
   for (int k = 0; k < std::max(ntop, nbot); ++k) {

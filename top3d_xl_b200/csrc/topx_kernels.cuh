@@ -95,7 +95,9 @@ struct SlabInfo {
 void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks, const uint8_t* present, double* A,
                           double* Bup);
 // in-place inverse of an SPD m x m matrix; Pinv 64x64, R 64 x m, C m x 64 scratch
-void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* C);
+void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* Ct);
+// one-time per-device kernel attributes of the coarse factorisation (call outside stream capture)
+void prepare_coarse_kernels();
 // twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
 // Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes);
 // gj_scratch holds 2 * (64*64 + 128*m) doubles
