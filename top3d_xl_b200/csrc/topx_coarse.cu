@@ -870,6 +870,285 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// The same coarse solve as one cooperative launch: one CTA per SM, the chain steps
+// separated by a grid-wide barrier instead of kernel boundaries.  Each warp takes one
+// matrix row per step (dot against the step's input vectors, staged in shared memory)
+// and prefetches the rows of its next step into L2 before it waits at the barrier.
+// ---------------------------------------------------------------------------
+constexpr int COOP_THREADS = 512;
+constexpr int COOP_WARPS = COOP_THREADS / 32;
+// polls of the barrier word before a CTA gives up (well under a second in all)
+constexpr unsigned kCoopSpinLimit = 1u << 20;
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_volatile_int(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// Grid-wide barrier with a bounded wait.  Returns false in every thread of the CTA once any
+// CTA has given up (bar->err set); the kernel then returns, so it always ends.
+__device__ bool coop_barrier(CoopBarrier* bar) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = ld_volatile_int(&bar->err) == 0;
+    if (ok) {
+      const unsigned gen = ld_acquire_gpu(&bar->gen);
+      __threadfence();
+      if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+        atomicExch(&bar->count, 0u);
+        __threadfence();
+        atomicAdd(&bar->gen, 1u);
+      } else {
+        unsigned it = 0;
+        while (ld_acquire_gpu(&bar->gen) == gen) {
+          if (++it > kCoopSpinLimit || ld_volatile_int(&bar->err)) {
+            atomicExch(&bar->err, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <typename TM>
+__device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const double* __restrict__ u, int m,
+                                               int lane) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int j = lane;
+  for (; j + 96 < m; j += 128) {
+    a0 = fma(double(__ldg(Mr + j)), u[j], a0);
+    a1 = fma(double(__ldg(Mr + j + 32)), u[j + 32], a1);
+    a2 = fma(double(__ldg(Mr + j + 64)), u[j + 64], a2);
+    a3 = fma(double(__ldg(Mr + j + 96)), u[j + 96], a3);
+  }
+  for (; j < m; j += 32) a0 = fma(double(__ldg(Mr + j)), u[j], a0);
+  return warp_sum((a0 + a1) + (a2 + a3));
+}
+
+template <typename TM>
+__device__ __forceinline__ void warp_prefetch_row(const TM* Mr, int m, int lane) {
+  const char* p = reinterpret_cast<const char*>(Mr);
+  const int bytes = m * int(sizeof(TM));
+  for (int off = lane * 128; off < bytes; off += 32 * 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
+}
+
+// One chain step: up to two independent row blocks y = a - M u (M: m x m), both staged.
+struct ChainOp {
+  const void* M;
+  const double* u;
+  const double* a;
+  double* y;
+};
+
+template <typename TM>
+__device__ __forceinline__ void chain_prefetch(const ChainOp (&op)[2], int nop, int m, int gw, int nw, int lane) {
+  for (int r = gw; r < nop * m; r += nw) {
+    const int o = r / m, rr = r - o * m;
+    warp_prefetch_row(static_cast<const TM*>(op[o].M) + int64_t(rr) * m, m, lane);
+  }
+}
+
+template <typename TM>
+__device__ __forceinline__ void chain_step(const ChainOp (&op)[2], int nop, int m, double* su, int gw, int nw,
+                                           int lane) {
+  for (int o = 0; o < nop; ++o)
+    for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[o * m + j] = __ldcg(op[o].u + j);
+  __syncthreads();
+  for (int r = gw; r < nop * m; r += nw) {
+    const int o = r / m, rr = r - o * m;
+    const double d = warp_row_dot(static_cast<const TM*>(op[o].M) + int64_t(rr) * m, su + o * m, m, lane);
+    if (lane == 0) op[o].y[rr] = __ldcg(op[o].a + rr) - d;
+  }
+}
+
+// forward step k: top W_{k+1} = bs_{k+1} - L_k W_k; bottom W_s = bs_s - U_s W_{s+1}, s = ns-2-k
+template <typename TM>
+__device__ __forceinline__ int forward_ops(int k, const SlabInfo& si, const TM* X, const double* bs, double* W,
+                                           ChainOp (&op)[2]) {
+  const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
+  const int64_t mm = int64_t(m) * m;
+  int n = 0;
+  if (k + 1 < ntop) op[n++] = ChainOp{X + k * mm, W + int64_t(k) * m, bs + int64_t(k + 1) * m, W + int64_t(k + 1) * m};
+  if (k + 1 < nbot) {
+    const int s = ns - 2 - k;
+    op[n++] = ChainOp{X + s * mm, W + int64_t(s + 1) * m, bs + int64_t(s) * m, W + int64_t(s) * m};
+  }
+  return n;
+}
+
+// backward step k: top x_s = V_s - L_s^T x_{s+1}, s = mid-1-k; bottom x_s = V_s - U_{s-1}^T x_{s-1}, s = mid+1+k
+template <typename TM>
+__device__ __forceinline__ int backward_ops(int k, const SlabInfo& si, const TM* XT, const double* V, double* xs,
+                                            ChainOp (&op)[2]) {
+  const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
+  const int64_t mm = int64_t(m) * m;
+  int n = 0;
+  if (k < ntop) {
+    const int s = mid - 1 - k;
+    op[n++] = ChainOp{XT + s * mm, xs + int64_t(s + 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+  }
+  if (k < nbot) {
+    const int s = mid + 1 + k;
+    op[n++] = ChainOp{XT + (s - 1) * mm, xs + int64_t(s - 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+  }
+  return n;
+}
+
+template <typename T, typename TM>
+__global__ void __launch_bounds__(COOP_THREADS, 1)
+    k_slab_solve_coop(Grid g, SlabInfo si, const TM* __restrict__ Inv, const TM* __restrict__ X,
+                      const TM* __restrict__ XT, const T* __restrict__ b, double* bs, double* W, double* V,
+                      double* xs, T* __restrict__ x, const PcgScalars* sc, CoopBarrier* bar) {
+  if (sc && sc->done) return;
+  extern __shared__ double su[];  // 2 m doubles
+  const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
+  const int nsteps = max(ntop, nbot);
+  const int64_t mm = int64_t(m) * m, N = int64_t(ns) * m;
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * COOP_WARPS + warp, nw = gridDim.x * COOP_WARPS;
+  const int64_t tid = int64_t(blockIdx.x) * COOP_THREADS + threadIdx.x, nth = int64_t(gridDim.x) * COOP_THREADS;
+  ChainOp op[2];
+  int nop;
+
+  // gather into slab order; chain heads (and a lone middle slab) take b directly
+  for (int64_t t = tid; t < N; t += nth) {
+    const int s = int(t / m), row = int(t - int64_t(s) * m);
+    const int c = row / 3, k = row - 3 * c;
+    int gy, gx, gz;
+    slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
+    const double v = double(b[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride]);
+    bs[t] = v;
+    if ((s == 0 && ntop > 0) || (s == ns - 1 && nbot > 0) || (ntop == 0 && nbot == 0)) W[t] = v;
+  }
+  nop = forward_ops(0, si, X, bs, W, op);
+  chain_prefetch<TM>(op, nop, m, gw, nw, lane);
+  if (!coop_barrier(bar)) return;
+
+  // forward chains toward the middle
+  for (int k = 0; k + 1 < nsteps; ++k) {
+    nop = forward_ops(k, si, X, bs, W, op);
+    chain_step<TM>(op, nop, m, su, gw, nw, lane);
+    ChainOp nx[2];
+    const int nn = forward_ops(k + 1, si, X, bs, W, nx);
+    chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
+    if (!coop_barrier(bar)) return;
+  }
+  // middle slab: W_mid = b_mid - L_{mid-1} W_{mid-1} - U_mid W_{mid+1}
+  if (ntop > 0 || nbot > 0) {
+    nop = 0;
+    if (ntop > 0) op[nop++] = ChainOp{X + (mid - 1) * mm, W + int64_t(mid - 1) * m, nullptr, nullptr};
+    if (nbot > 0) op[nop++] = ChainOp{X + mid * mm, W + int64_t(mid + 1) * m, nullptr, nullptr};
+    for (int o = 0; o < nop; ++o)
+      for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[o * m + j] = __ldcg(op[o].u + j);
+    __syncthreads();
+    for (int r = gw; r < m; r += nw) {
+      double d = 0.0;
+      for (int o = 0; o < nop; ++o)
+        d += warp_row_dot(static_cast<const TM*>(op[o].M) + int64_t(r) * m, su + o * m, m, lane);
+      if (lane == 0) W[int64_t(mid) * m + r] = __ldcg(bs + int64_t(mid) * m + r) - d;
+    }
+    if (!coop_barrier(bar)) return;
+  }
+  // V_s = Inv_s W_s for all slabs, each CTA over a contiguous row range; x_mid = V_mid
+  {
+    const int64_t r0 = N * blockIdx.x / gridDim.x, r1 = N * (blockIdx.x + 1) / gridDim.x;
+    for (int64_t rs = r0; rs < r1;) {
+      const int s = int(rs / m);
+      const int64_t re = min(r1, int64_t(s + 1) * m);
+      for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[j] = __ldcg(W + int64_t(s) * m + j);
+      __syncthreads();
+      for (int64_t r = rs + warp; r < re; r += COOP_WARPS) {
+        const int rr = int(r - int64_t(s) * m);
+        const double d = warp_row_dot(Inv + s * mm + int64_t(rr) * m, su, m, lane);
+        if (lane == 0) {
+          V[r] = d;
+          if (s == mid) xs[r] = d;
+        }
+      }
+      __syncthreads();
+      rs = re;
+    }
+  }
+  nop = backward_ops(0, si, XT, V, xs, op);
+  chain_prefetch<TM>(op, nop, m, gw, nw, lane);
+  if (!coop_barrier(bar)) return;
+  // backward chains outward from the middle
+  for (int k = 0; k < nsteps; ++k) {
+    nop = backward_ops(k, si, XT, V, xs, op);
+    chain_step<TM>(op, nop, m, su, gw, nw, lane);
+    if (k + 1 < nsteps) {
+      ChainOp nx[2];
+      const int nn = backward_ops(k + 1, si, XT, V, xs, nx);
+      chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
+    }
+    if (!coop_barrier(bar)) return;
+  }
+  // scatter to the grid
+  for (int64_t t = tid; t < N; t += nth) {
+    const int s = int(t / m), row = int(t - int64_t(s) * m);
+    const int c = row / 3, k = row - 3 * c;
+    int gy, gx, gz;
+    slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
+    x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(__ldcg(xs + t));
+  }
+}
+
+int slab_solve_coop_ctas(int m) {
+  int dev = 0, coop = 0, nsm = 0, per = 0;
+  TOPX_CUDA_OK(cudaGetDevice(&dev));
+  TOPX_CUDA_OK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  TOPX_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (!coop) return 0;
+  const size_t smem = size_t(2) * m * sizeof(double);
+  if (smem > size_t(200) * 1024) return 0;
+  const void* kernels[2] = {reinterpret_cast<const void*>(&k_slab_solve_coop<double, double>),
+                            reinterpret_cast<const void*>(&k_slab_solve_coop<float, float>)};
+  for (int i = 0; i < 2; ++i) {
+    TOPX_CUDA_OK(cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int b = 0;
+    TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernels[i], COOP_THREADS, smem));
+    per = i == 0 ? b : std::min(per, b);
+  }
+  return per >= 1 ? nsm : 0;
+}
+
+template <typename T, typename TM>
+void launch_slab_solve_coop(cudaStream_t st, int nctas, Grid g, SlabInfo si, const TM* Inv, const TM* X,
+                            const TM* XT, const T* b, double* bs, double* W, double* V, double* xs, T* x,
+                            const PcgScalars* sc, CoopBarrier* bar) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(nctas));
+  cfg.blockDim = dim3(COOP_THREADS);
+  cfg.dynamicSmemBytes = size_t(2) * si.m * sizeof(double);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  TOPX_CUDA_OK(cudaLaunchKernelEx(&cfg, k_slab_solve_coop<T, TM>, g, si, Inv, X, XT, b, bs, W, V, xs, x, sc, bar));
+  topx::count_launch();
+}
+
+template void launch_slab_solve_coop<double, double>(cudaStream_t, int, Grid, SlabInfo, const double*, const double*,
+                                                     const double*, const double*, double*, double*, double*,
+                                                     double*, double*, const PcgScalars*, CoopBarrier*);
+template void launch_slab_solve_coop<float, float>(cudaStream_t, int, Grid, SlabInfo, const float*, const float*,
+                                                   const float*, const float*, double*, double*, double*, double*,
+                                                   float*, const PcgScalars*, CoopBarrier*);
+
 template void launch_diag_coarse<double>(cudaStream_t, Grid, const double*, const uint8_t*, double*);
 template void launch_diag_coarse<float>(cudaStream_t, Grid, const double*, const uint8_t*, float*);
 template void launch_slab_solve<double, double>(cudaStream_t, Grid, SlabInfo, const double*, const double*,

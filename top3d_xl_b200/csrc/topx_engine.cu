@@ -208,6 +208,8 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
     slabBup.alloc(size_t(si.nu) * si.nv * 81 * nsm1);
     gjP.alloc(2 * (64 * 64 + size_t(128) * si.m));
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
+    coopBar.alloc(1);
+    coopCtas = slab_solve_coop_ctas(si.m);
   }
   // ---- workspaces ------------------------------------------------------------
   {
@@ -236,6 +238,7 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
   mmaS.alloc(1);
   dscal.alloc(16);
   TOPX_CUDA_OK(cudaMallocHost(&h_sc, sizeof(PcgScalars)));
+  TOPX_CUDA_OK(cudaMallocHost(&h_bar, sizeof(CoopBarrier)));
   // ---- optimiser state -------------------------------------------------------
   for (DevBuf<double>* b : {&x, &xPhys, &dc, &ce, &tmpA, &tmpB, &xTilde, &xhat, &dfdx, &dxv, &volMax})
     b->alloc(size_t(Ne));
@@ -280,6 +283,7 @@ Engine::~Engine() {
   for (auto e : tev)
     if (e) cudaEventDestroy(e);
   if (h_sc) cudaFreeHost(h_sc);
+  if (h_bar) cudaFreeHost(h_bar);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -314,8 +318,23 @@ void Engine::alloc_fwork(FWork<TF>& f) {
 
 void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
   TOPX_CUDA_OK(cudaMemcpyAsync(h_sc, d, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   h = *h_sc;
+  if (coopCtas && h_bar->err) {
+    TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
+    throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
+  }
+}
+
+void Engine::check_coop_barrier() {
+  if (!coopCtas) return;
+  TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  if (h_bar->err) {
+    TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
+    throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -409,13 +428,18 @@ void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
     launch_restrict<TC, TC>(st, M.levels[l].span, v.rl[l - 1].p, G[l - 1], v.tmp1.p, v.tmp2.p, v.rl[l].p, G[l]);
   sec_end();
   sec_begin(SEC_COARSE_SOLVE);
-  if (std::is_same<TC, double>::value)
-    launch_slab_solve<TC, TC>(st, G[nl - 1], si, (const TC*)slabSinv.p, (const TC*)slabL.p, (const TC*)slabLT.p,
-                              v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc);
-  else
-    launch_slab_solve<TC, TC>(st, G[nl - 1], si, (const TC*)slabSinv32.p, (const TC*)slabL32.p,
-                              (const TC*)slabLT32.p, v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p,
-                              v.xl[nl - 1].p, sc);
+  {
+    const bool f64 = std::is_same<TC, double>::value;
+    const TC* Inv = f64 ? (const TC*)slabSinv.p : (const TC*)slabSinv32.p;
+    const TC* Lf = f64 ? (const TC*)slabL.p : (const TC*)slabL32.p;
+    const TC* LT = f64 ? (const TC*)slabLT.p : (const TC*)slabLT32.p;
+    if (coopCtas)
+      launch_slab_solve_coop<TC, TC>(st, coopCtas, G[nl - 1], si, Inv, Lf, LT, v.rl[nl - 1].p, slabBS.p, slabW.p,
+                                     slabV.p, slabXS.p, v.xl[nl - 1].p, sc, coopBar.p);
+    else
+      launch_slab_solve<TC, TC>(st, G[nl - 1], si, Inv, Lf, LT, v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p,
+                                slabXS.p, v.xl[nl - 1].p, sc);
+  }
   sec_end();
   sec_begin(SEC_PROLONG);
   const double om = M.S.weightFactorJacobi;
@@ -581,7 +605,7 @@ void Engine::apply_vcycle(const double* h_r, double* h_z) {
   launch_compact_to_grid_nodes<double>(st, cu.p, kw.r.p, G[0], nodMapBack0.p, Nn);
   vcycle(true, scE.p);
   launch_grid_to_compact_nodes<double>(st, kw.z.p, cu.p, G[0], nodMapBack0.p, Nn);
-  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  check_coop_barrier();
   TOPX_CUDA_OK(cudaMemcpy(h_z, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
 }
 

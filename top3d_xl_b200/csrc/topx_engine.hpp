@@ -187,6 +187,9 @@ class Engine {
   DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gjP, gjR, gjC;
   DevBuf<float> slabSinv32, slabL32, slabLT32;  // FP32 copies applied by the mixed-precision V-cycle
   DevBuf<double> slabBS, slabW, slabV, slabXS;  // slab-ordered vectors of one coarse solve
+  DevBuf<CoopBarrier> coopBar;  // barrier of the cooperative coarse solve
+  int coopCtas = 0;             // its CTA count; 0: multi-launch coarse solve
+  void check_coop_barrier();    // throws after a barrier wait gave up (and re-arms the barrier)
   // workspaces
   KrylovWork kw;
   VWork<double> v64;
@@ -203,6 +206,7 @@ class Engine {
   DevBuf<MmaState> mmaS;
   DevBuf<double> dscal;
   PcgScalars* h_sc = nullptr;  // pinned
+  CoopBarrier* h_bar = nullptr;  // pinned
   // optimiser state (compact, FP64)
   DevBuf<double> x, xPhys, dc, ce, tmpA, tmpB, xTilde, xhat, dfdx, dxv, volMax;
   DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;

@@ -420,14 +420,25 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
                                                         const uint8_t* __restrict__ present, T* __restrict__ x,
                                                         Grid gf, T omega, PcgScalars* sc, RedScratch rs, int init) {
   if (DOT && sc->done) return;
-  const int fny = gf.nny(), fnx = gf.nnx(), fnz = gf.nnz();
+  const int fny = gf.nny(), fnx = gf.nnx();
+  const int64_t nn = gf.nnodes();
   const int cny = gc.nny(), cnx = gc.nnx();
-  const int fy = blockIdx.x * 32 + threadIdx.x, fx = blockIdx.y * 4 + threadIdx.y, fz = blockIdx.z * 2 + threadIdx.z;
   double zr = 0.0;
-  if (fy < fny && fx < fnx && fz < fnz) {
-    const int64_t n = fy + int64_t(fny) * (fx + int64_t(fnx) * fz);
+  // grid-stride over the flattened fine grid: no idle lanes on odd extents, and one
+  // reduction tail per CTA instead of one per 256 nodes
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < nn; n += int64_t(gridDim.x) * blockDim.x) {
+    T rv[3], di[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      rv[c] = r[n + c * gf.stride];
+      di[c] = T(dinv[n + c * gf.stride]);
+    }
     T v[3] = {T(0), T(0), T(0)};
     if (present[n]) {
+      const int64_t q = n / fny;
+      const int fy = int(n - q * fny);
+      const int fz = int(q / fnx);
+      const int fx = int(q - int64_t(fz) * fnx);
       const int Y = fy / S, X = fx / S, Z = fz / S;
       const int ty = fy - S * Y, tx = fx - S * X, tz = fz - S * Z;
       T pc[3] = {T(0), T(0), T(0)};
@@ -446,12 +457,11 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const T rv = r[n + c * gf.stride], di = T(dinv[n + c * gf.stride]);
-        T t = omega * (rv * di);
+        T t = omega * (rv[c] * di[c]);
         t = t + pc[c];
-        t = t + (omega * rv) * di;
+        t = t + (omega * rv[c]) * di[c];
         v[c] = t;
-        if (DOT) zr += double(t) * double(rv);
+        if (DOT) zr += double(t) * double(rv[c]);
       }
     }
 #pragma unroll
@@ -459,7 +469,7 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
   }
   if (DOT) {
     double vv[1] = {zr}, tot[1];
-    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0) {
       if (init) {
         sc->x1 = tot[0];
       } else {
@@ -474,19 +484,18 @@ template <typename TX, typename T, typename TD>
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
                            PcgScalars* sc, RedScratch rs) {
-  const dim3 nb((gf.nny() + 31) / 32, (gf.nnx() + 3) / 4, (gf.nnz() + 1) / 2);
-  const dim3 blk(32, 4, 2);
+  const unsigned nb = grid1d(gf.nnodes(), 256, 148 * 8);
   const T w = T(omega);
   if (span == 4) {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
   } else {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, blk, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }

@@ -108,4 +108,21 @@ template <typename T, typename TM>
 void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT, const T* b,
                        double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc);
 
+// State of the grid-wide barrier of the cooperative coarse solve (zeroed before first use;
+// err != 0 after a CTA gave up waiting, and then count must be zeroed again).
+struct CoopBarrier {
+  unsigned count;
+  unsigned gen;
+  int err;
+  int pad;
+};
+// CTAs of launch_slab_solve_coop on the current device (one per SM), or 0 when cooperative
+// launch is unavailable; sets the kernels' shared-memory limit (call outside stream capture).
+int slab_solve_coop_ctas(int m);
+// the coarse solve above as one cooperative launch (same factors; rows summed in another order)
+template <typename T, typename TM>
+void launch_slab_solve_coop(cudaStream_t st, int nctas, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT,
+                            const T* b, double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc,
+                            CoopBarrier* bar);
+
 }  // namespace topx
