@@ -155,3 +155,24 @@ def test_gpu_call_without_device_fails_loudly():
         ctx.assemble()
     assert "TOPX_ERR_CUDA" in str(e.value)
     ctx.close()
+
+
+def test_ke_value_classes_header_is_current_and_matches_ke():
+    """The level-1 operator reads Ke through topx_ke_classes.h: the committed header must
+    be what its generator writes, and every entry of the element stiffness must equal
+    sign * value of its class to rounding."""
+    import importlib.util
+    csrc = os.path.join(ROOT, "top3d_xl_b200", "csrc")
+    spec = importlib.util.spec_from_file_location("gen_ke_classes", os.path.join(csrc, "gen_ke_classes.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    with open(os.path.join(csrc, "topx_ke_classes.h")) as fh:
+        assert fh.read() == gen.header()
+    table, n = gen.classes()
+    Ke = O.element_stiffness(0.3, 1.0).ravel()
+    first = {}
+    for idx, code in enumerate(table):
+        c = abs(code) - 1
+        first.setdefault(c, Ke[idx] * np.sign(code))
+        assert abs(Ke[idx] - np.sign(code) * first[c]) <= 1e-15 * abs(first[c])
+    assert n == 10

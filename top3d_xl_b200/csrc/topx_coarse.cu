@@ -888,32 +888,29 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 }
 __device__ __forceinline__ int ld_volatile_int(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
-// Grid-wide barrier with a bounded wait.  Returns false in every thread of the CTA once any
-// CTA has given up (bar->err set); the kernel then returns, so it always ends.
-__device__ bool coop_barrier(CoopBarrier* bar) {
+// Grid-wide barrier with a bounded wait.  bar->count only grows within a launch: barrier
+// number i (1, 2, ...) is passed once it reaches i * gridDim.x, so an arrival is one
+// fire-and-forget release add and the wait polls that single word (no reset round trip).
+// The last CTA to leave the kernel (coop_exit) zeroes the words for the next launch.
+// Returns false in every thread of the CTA once any CTA has given up (bar->err set); the
+// kernel then returns, so it always ends.
+__device__ bool coop_barrier(CoopBarrier* bar, unsigned& epoch) {
   __shared__ int s_ok;
   __syncthreads();
+  ++epoch;
   if (threadIdx.x == 0) {
     int ok = ld_volatile_int(&bar->err) == 0;
     if (ok) {
-      const unsigned gen = ld_acquire_gpu(&bar->gen);
-      __threadfence();
-      if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
-        atomicExch(&bar->count, 0u);
-        __threadfence();
-        atomicAdd(&bar->gen, 1u);
-      } else {
-        unsigned it = 0;
-        while (ld_acquire_gpu(&bar->gen) == gen) {
-          if (++it > kCoopSpinLimit || ld_volatile_int(&bar->err)) {
-            atomicExch(&bar->err, 1);
-            ok = 0;
-            break;
-          }
-          __nanosleep(32);
+      const unsigned target = epoch * gridDim.x;
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&bar->count) : "memory");
+      unsigned it = 0;
+      while (ld_acquire_gpu(&bar->count) < target) {
+        if (++it > kCoopSpinLimit || ld_volatile_int(&bar->err)) {
+          atomicExch(&bar->err, 1);
+          ok = 0;
+          break;
         }
       }
-      __threadfence();
     }
     s_ok = ok;
   }
@@ -921,19 +918,42 @@ __device__ bool coop_barrier(CoopBarrier* bar) {
   return s_ok != 0;
 }
 
+// Called once by every CTA on every exit path after its first barrier: the last one out
+// re-arms the barrier words (all other CTAs have left their waits by then).
+__device__ void coop_exit(CoopBarrier* bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&bar->gen, 1u) == gridDim.x - 1) {
+      atomicExch(&bar->count, 0u);
+      atomicExch(&bar->gen, 0u);
+    }
+  }
+}
+
+// Dot of one matrix row with a shared-memory vector by one warp.  The row is read in
+// pieces of 32 x 32 elements whose loads are all issued before the first use, so a row
+// of up to 1024 entries costs one memory round trip.
 template <typename TM>
 __device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const double* __restrict__ u, int m,
                                                int lane) {
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int j = lane;
-  for (; j + 96 < m; j += 128) {
-    a0 = fma(double(__ldg(Mr + j)), u[j], a0);
-    a1 = fma(double(__ldg(Mr + j + 32)), u[j + 32], a1);
-    a2 = fma(double(__ldg(Mr + j + 64)), u[j + 64], a2);
-    a3 = fma(double(__ldg(Mr + j + 96)), u[j + 96], a3);
+  constexpr int PIECE = 32;
+  double a0 = 0.0, a1 = 0.0;
+  for (int base = 0; base < m; base += 32 * PIECE) {
+    TM v[PIECE];
+#pragma unroll
+    for (int i = 0; i < PIECE; ++i) {
+      const int j = base + lane + 32 * i;
+      v[i] = j < m ? __ldg(Mr + j) : TM(0);
+    }
+#pragma unroll
+    for (int i = 0; i < PIECE; i += 2) {
+      const int j = base + lane + 32 * i;
+      if (j < m) a0 = fma(double(v[i]), u[j], a0);
+      if (j + 32 < m) a1 = fma(double(v[i + 1]), u[j + 32], a1);
+    }
   }
-  for (; j < m; j += 32) a0 = fma(double(__ldg(Mr + j)), u[j], a0);
-  return warp_sum((a0 + a1) + (a2 + a3));
+  return warp_sum(a0 + a1);
 }
 
 template <typename TM>
@@ -951,24 +971,56 @@ struct ChainOp {
   double* y;
 };
 
+// (op[0] / op[1] picked by value so the descriptors stay in registers)
 template <typename TM>
 __device__ __forceinline__ void chain_prefetch(const ChainOp (&op)[2], int nop, int m, int gw, int nw, int lane) {
   for (int r = gw; r < nop * m; r += nw) {
-    const int o = r / m, rr = r - o * m;
-    warp_prefetch_row(static_cast<const TM*>(op[o].M) + int64_t(rr) * m, m, lane);
+    const int o = r >= m ? 1 : 0, rr = r - o * m;
+    const ChainOp c = o ? op[1] : op[0];
+    warp_prefetch_row(static_cast<const TM*>(c.M) + int64_t(rr) * m, m, lane);
   }
 }
 
 template <typename TM>
 __device__ __forceinline__ void chain_step(const ChainOp (&op)[2], int nop, int m, double* su, int gw, int nw,
                                            int lane) {
-  for (int o = 0; o < nop; ++o)
-    for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[o * m + j] = __ldcg(op[o].u + j);
+  // the warp's first row (up to 1024 entries) is requested before the input vectors are
+  // staged, so the two memory round trips overlap
+  constexpr int PIECE = 32;
+  TM v[PIECE];
+  const int r0 = gw;
+  const bool have = r0 < nop * m;
+  const int o0 = r0 >= m ? 1 : 0;
+  const ChainOp c0 = o0 ? op[1] : op[0];
+  const TM* M0 = static_cast<const TM*>(c0.M) + int64_t(r0 - o0 * m) * m;
+#pragma unroll
+  for (int i = 0; i < PIECE; ++i) {
+    const int j = lane + 32 * i;
+    v[i] = (have && j < m) ? __ldg(M0 + j) : TM(0);
+  }
+  for (int j = threadIdx.x; j < nop * m; j += COOP_THREADS) su[j] = __ldcg((j >= m ? op[1].u - m : op[0].u) + j);
   __syncthreads();
-  for (int r = gw; r < nop * m; r += nw) {
-    const int o = r / m, rr = r - o * m;
-    const double d = warp_row_dot(static_cast<const TM*>(op[o].M) + int64_t(rr) * m, su + o * m, m, lane);
-    if (lane == 0) op[o].y[rr] = __ldcg(op[o].a + rr) - d;
+  if (have) {
+    const double* u = su + o0 * m;
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < PIECE; i += 2) {
+      const int j = lane + 32 * i;
+      if (j < m) a0 = fma(double(v[i]), u[j], a0);
+      if (j + 32 < m) a1 = fma(double(v[i + 1]), u[j + 32], a1);
+    }
+    for (int base = 32 * PIECE; base < m; base += 32) {
+      const int j = base + lane;
+      if (j < m) a0 = fma(double(__ldg(M0 + j)), u[j], a0);
+    }
+    const double d = warp_sum(a0 + a1);
+    if (lane == 0) c0.y[r0 - o0 * m] = __ldcg(c0.a + (r0 - o0 * m)) - d;
+  }
+  for (int r = gw + nw; r < nop * m; r += nw) {
+    const int o = r >= m ? 1 : 0, rr = r - o * m;
+    const ChainOp c = o ? op[1] : op[0];
+    const double d = warp_row_dot(static_cast<const TM*>(c.M) + int64_t(rr) * m, su + o * m, m, lane);
+    if (lane == 0) c.y[rr] = __ldcg(c.a + rr) - d;
   }
 }
 
@@ -979,10 +1031,18 @@ __device__ __forceinline__ int forward_ops(int k, const SlabInfo& si, const TM* 
   const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
   const int64_t mm = int64_t(m) * m;
   int n = 0;
-  if (k + 1 < ntop) op[n++] = ChainOp{X + k * mm, W + int64_t(k) * m, bs + int64_t(k + 1) * m, W + int64_t(k + 1) * m};
+  if (k + 1 < ntop) {
+    op[0] = ChainOp{X + k * mm, W + int64_t(k) * m, bs + int64_t(k + 1) * m, W + int64_t(k + 1) * m};
+    n = 1;
+  }
   if (k + 1 < nbot) {
     const int s = ns - 2 - k;
-    op[n++] = ChainOp{X + s * mm, W + int64_t(s + 1) * m, bs + int64_t(s) * m, W + int64_t(s) * m};
+    const ChainOp c{X + s * mm, W + int64_t(s + 1) * m, bs + int64_t(s) * m, W + int64_t(s) * m};
+    if (n)
+      op[1] = c;
+    else
+      op[0] = c;
+    ++n;
   }
   return n;
 }
@@ -996,11 +1056,17 @@ __device__ __forceinline__ int backward_ops(int k, const SlabInfo& si, const TM*
   int n = 0;
   if (k < ntop) {
     const int s = mid - 1 - k;
-    op[n++] = ChainOp{XT + s * mm, xs + int64_t(s + 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+    op[0] = ChainOp{XT + s * mm, xs + int64_t(s + 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+    n = 1;
   }
   if (k < nbot) {
     const int s = mid + 1 + k;
-    op[n++] = ChainOp{XT + (s - 1) * mm, xs + int64_t(s - 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+    const ChainOp c{XT + (s - 1) * mm, xs + int64_t(s - 1) * m, V + int64_t(s) * m, xs + int64_t(s) * m};
+    if (n)
+      op[1] = c;
+    else
+      op[0] = c;
+    ++n;
   }
   return n;
 }
@@ -1021,6 +1087,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
   const int64_t tid = int64_t(blockIdx.x) * COOP_THREADS + threadIdx.x, nth = int64_t(gridDim.x) * COOP_THREADS;
   ChainOp op[2];
   int nop;
+  unsigned epoch = 0;
 
   // gather into slab order; chain heads (and a lone middle slab) take b directly
   for (int64_t t = tid; t < N; t += nth) {
@@ -1034,7 +1101,10 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
   }
   nop = forward_ops(0, si, X, bs, W, op);
   chain_prefetch<TM>(op, nop, m, gw, nw, lane);
-  if (!coop_barrier(bar)) return;
+  if (!coop_barrier(bar, epoch)) {
+    coop_exit(bar);
+    return;
+  }
 
   // forward chains toward the middle
   for (int k = 0; k + 1 < nsteps; ++k) {
@@ -1043,23 +1113,29 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     ChainOp nx[2];
     const int nn = forward_ops(k + 1, si, X, bs, W, nx);
     chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
-    if (!coop_barrier(bar)) return;
+    if (!coop_barrier(bar, epoch)) {
+    coop_exit(bar);
+    return;
+  }
   }
   // middle slab: W_mid = b_mid - L_{mid-1} W_{mid-1} - U_mid W_{mid+1}
   if (ntop > 0 || nbot > 0) {
-    nop = 0;
-    if (ntop > 0) op[nop++] = ChainOp{X + (mid - 1) * mm, W + int64_t(mid - 1) * m, nullptr, nullptr};
-    if (nbot > 0) op[nop++] = ChainOp{X + mid * mm, W + int64_t(mid + 1) * m, nullptr, nullptr};
-    for (int o = 0; o < nop; ++o)
-      for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[o * m + j] = __ldcg(op[o].u + j);
+    const ChainOp up{X + (mid - 1) * mm, W + int64_t(mid - 1) * m, nullptr, nullptr};
+    const ChainOp dn{X + mid * mm, W + int64_t(mid + 1) * m, nullptr, nullptr};
+    nop = (ntop > 0) + (nbot > 0);
+    op[0] = ntop > 0 ? up : dn;
+    op[1] = dn;
+    for (int j = threadIdx.x; j < nop * m; j += COOP_THREADS) su[j] = __ldcg((j >= m ? op[1].u - m : op[0].u) + j);
     __syncthreads();
     for (int r = gw; r < m; r += nw) {
-      double d = 0.0;
-      for (int o = 0; o < nop; ++o)
-        d += warp_row_dot(static_cast<const TM*>(op[o].M) + int64_t(r) * m, su + o * m, m, lane);
+      double d = warp_row_dot(static_cast<const TM*>(op[0].M) + int64_t(r) * m, su, m, lane);
+      if (nop > 1) d += warp_row_dot(static_cast<const TM*>(op[1].M) + int64_t(r) * m, su + m, m, lane);
       if (lane == 0) W[int64_t(mid) * m + r] = __ldcg(bs + int64_t(mid) * m + r) - d;
     }
-    if (!coop_barrier(bar)) return;
+    if (!coop_barrier(bar, epoch)) {
+    coop_exit(bar);
+    return;
+  }
   }
   // V_s = Inv_s W_s for all slabs, each CTA over a contiguous row range; x_mid = V_mid
   {
@@ -1083,7 +1159,10 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
   }
   nop = backward_ops(0, si, XT, V, xs, op);
   chain_prefetch<TM>(op, nop, m, gw, nw, lane);
-  if (!coop_barrier(bar)) return;
+  if (!coop_barrier(bar, epoch)) {
+    coop_exit(bar);
+    return;
+  }
   // backward chains outward from the middle
   for (int k = 0; k < nsteps; ++k) {
     nop = backward_ops(k, si, XT, V, xs, op);
@@ -1093,7 +1172,10 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
       const int nn = backward_ops(k + 1, si, XT, V, xs, nx);
       chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
     }
-    if (!coop_barrier(bar)) return;
+    if (!coop_barrier(bar, epoch)) {
+    coop_exit(bar);
+    return;
+  }
   }
   // scatter to the grid
   for (int64_t t = tid; t < N; t += nth) {
@@ -1103,6 +1185,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
     x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(__ldcg(xs + t));
   }
+  coop_exit(bar);
 }
 
 int slab_solve_coop_ctas(int m) {

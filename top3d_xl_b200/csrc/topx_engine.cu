@@ -20,6 +20,7 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
   // blocking stream: ordered with the synchronous cudaMemset/cudaMemcpy calls of the set-up code
   TOPX_CUDA_OK(cudaStreamCreate(&st));
   prepare_coarse_kernels();
+  prepare_fem_kernels();
   nl = M.numLevels;
   if (nl < 3 || int(M.levels.size()) != nl) throw std::runtime_error("model hierarchy not built");
   for (int l = 0; l < nl; ++l) {

@@ -1,8 +1,11 @@
 // Level-1 elasticity kernels of the TOP3D_XL B200 path: matrix-free K*u,
 // Jacobi diagonal, PCG vector algebra, trilinear multigrid transfers, SIMP,
 // unit compliance.  FP64 (plain path) and FP32 (mixed path) instantiations.
+#include <cmath>
+#include <stdexcept>
 #include <type_traits>
 
+#include "topx_ke_classes.h"
 #include "topx_kernels.cuh"
 
 namespace topx {
@@ -21,11 +24,53 @@ __device__ __forceinline__ float ke<float>(int i) {
   return c_Ke32[i];
 }
 
+// The ten values of Ke (topx_ke_classes.h): the level-1 operator addresses these instead of
+// 576 constants, so they stay in uniform registers for the whole launch.
+__constant__ double c_Kc64[kKeClasses];
+__constant__ float c_Kc32[kKeClasses];
+
+template <typename T>
+__device__ __forceinline__ T kcls(int c);
+template <>
+__device__ __forceinline__ double kcls<double>(int c) {
+  return c_Kc64[c];
+}
+template <>
+__device__ __forceinline__ float kcls<float>(int c) {
+  return c_Kc32[c];
+}
+// entry idx of Ke from its class (idx is a compile-time constant once the loops are unrolled)
+template <typename T>
+__device__ __forceinline__ T kcl(int idx) {
+  const int code = ke_class_code(idx);
+  return code > 0 ? kcls<T>(code - 1) : -kcls<T>(-code - 1);
+}
+
 void upload_ke(const double* Ke576) {
   float f[576];
   for (int i = 0; i < 576; ++i) f[i] = float(Ke576[i]);
   TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Ke64, Ke576, sizeof(double) * 576));
   TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Ke32, f, sizeof(float) * 576));
+  // class values from the first entry of each class; every other entry must agree to rounding
+  double v[kKeClasses];
+  bool seen[kKeClasses] = {};
+  for (int i = 0; i < 576; ++i) {
+    const int code = ke_class_code(i), c = (code > 0 ? code : -code) - 1;
+    if (!seen[c]) {
+      v[c] = code > 0 ? Ke576[i] : -Ke576[i];
+      seen[c] = true;
+    }
+  }
+  for (int i = 0; i < 576; ++i) {
+    const int code = ke_class_code(i), c = (code > 0 ? code : -code) - 1;
+    const double e = code > 0 ? v[c] : -v[c];
+    if (!(std::fabs(Ke576[i] - e) <= 1e-13 * std::fabs(v[c])))
+      throw std::runtime_error("element stiffness does not have the hex8 value classes");
+  }
+  float vf[kKeClasses];
+  for (int c = 0; c < kKeClasses; ++c) vf[c] = float(v[c]);
+  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Kc64, v, sizeof(v)));
+  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_Kc32, vf, sizeof(vf)));
 }
 
 static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
@@ -42,8 +87,8 @@ static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
 // 32x8 nodes marches 16 node planes along z, keeping a ring of three
 // (32+2)x(8+2) planes of u (masked by the free-DOF mask) and two planes of
 // element moduli in shared memory, and sums, for each of the 8 surrounding
-// hexes, the node's 3 rows of E_e*Ke times the hex's 24 DOFs (Ke entries are
-// constant-bank operands).  No atomics: the result is deterministic.  The reference's per-element BC
+// hexes, the node's 3 rows of E_e*Ke times the hex's 24 DOFs (Ke addressed through
+// its ten value classes, held in uniform registers).  No atomics: the result is deterministic.  The reference's per-element BC
 // matrices (uniqueKesFree_/uniqueKesFixed_) reduce exactly to
 //     y = m .* K_E (m .* u) + (1-m) .* cfix .* u
 // with m the free-DOF mask and cfix(node) = sum over its hexes of 1/nAdj.
@@ -99,9 +144,9 @@ __device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], 
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             T s = acc[e][i];
-            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
-            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
-            s = fma(ke<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
+            s = fma(kcl<T>((3 * a + i) * 24 + 3 * b + 0), u0, s);
+            s = fma(kcl<T>((3 * a + i) * 24 + 3 * b + 1), u1, s);
+            s = fma(kcl<T>((3 * a + i) * 24 + 3 * b + 2), u2, s);
             acc[e][i] = s;
           }
         }
@@ -116,102 +161,202 @@ __device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], 
   }
 }
 
+// Plane loads are asynchronous copies one plane ahead: the raw values of node plane z+2
+// (u, or z and p_old in PCG mode) land in a staging area and element plane z+1 in a third
+// element slot while plane z is computed; the next iteration forms the masked values of
+// the staged plane in the node ring.  Only the free-DOF bits ride in registers.
+constexpr int KU_NP = (KX + 2) * (KY + 2), KU_EP = (KX + 1) * (KY + 1);
+static_assert(KU_NP <= 2 * KNT && KU_EP <= 2 * KNT, "two staged positions per thread");
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_el(void* smem, const void* gmem, bool pred) {
+  static_assert(BYTES == 4 || BYTES == 8, "element copy size");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int n = pred ? BYTES : 0;  // 0: fill with zeros, read nothing
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
-                                                  T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
+__global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __restrict__ in, const T* __restrict__ zin,
+                                                  T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
                                                   PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
-  __shared__ T se[2][KX + 1][KY + 1];     // ring of 2 element planes
+  __shared__ T se[3][KX + 1][KY + 1];     // ring of 3 element planes
+  __shared__ T sa[3][KU_NP];              // staged raw plane: u (plain) or z (PCG mode)
+  __shared__ T sb[MODE == KU_PLAIN ? 1 : 3][MODE == KU_PLAIN ? 1 : KU_NP];  // staged p_old (PCG mode)
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
-  const int y0 = blockIdx.x * KY, x0 = blockIdx.y * KX, zc0 = blockIdx.z * KZC;
+  const int y0 = blockIdx.x * KY, x0 = blockIdx.y * KX, zc0 = blockIdx.z * zc;
+  const int zend = min(zc0 + zc, nnz);
   const int ty = threadIdx.x, tx = threadIdx.y;
   const int tid = ty + KY * tx;
   const bool first = (MODE != KU_PLAIN) && sc->first;
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
+  const T* const araw = MODE == KU_PLAIN ? in : zin;
+  uint8_t fbs[2];
 
-  auto load_nodes = [&](int zp, int slot) {
-    for (int i = tid; i < (KX + 2) * (KY + 2); i += KNT) {
-      const int sy = i % (KY + 2), sx = i / (KY + 2);
-      const int gy = y0 - 1 + sy, gx = x0 - 1 + sx;
-      T v0 = T(0), v1 = T(0), v2 = T(0);
-      if (zp >= 0 && zp < nnz && gy >= 0 && gy < nny && gx >= 0 && gx < nnx) {
-        const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * zp);
-        ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
-        const uint8_t fb = fixbits[n];
-        if (fb & 1) v0 = T(0);
-        if (fb & 2) v1 = T(0);
-        if (fb & 4) v2 = T(0);
+  // issue the copies of node plane zp into the staging area (and its free bits into fbs)
+  auto issue_nodes = [&](int zp) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int i = tid + s * KNT;
+      fbs[s] = 0;
+      if (i < KU_NP) {
+        const int sy = i % (KY + 2), sx = i / (KY + 2);
+        const int gy = y0 - 1 + sy, gx = x0 - 1 + sx;
+        const bool ok = zp >= 0 && zp < nnz && gy >= 0 && gy < nny && gx >= 0 && gx < nnx;
+        const int64_t n = ok ? gy + int64_t(nny) * (gx + int64_t(nnx) * zp) : 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cp_async_el<sizeof(T)>(&sa[c][i], araw + n + c * S, ok);
+          if (MODE != KU_PLAIN) cp_async_el<sizeof(T)>(&sb[c][i], in + n + c * S, ok && !first);
+        }
+        if (ok) fbs[s] = fixbits[n];
       }
-      su[slot][0][sx][sy] = v0;
-      su[slot][1][sx][sy] = v1;
-      su[slot][2][sx][sy] = v2;
     }
   };
-  auto load_elems = [&](int ez, int slot) {
-    for (int i = tid; i < (KX + 1) * (KY + 1); i += KNT) {
-      const int sy = i % (KY + 1), sx = i / (KY + 1);
-      const int ey = y0 - 1 + sy, ex = x0 - 1 + sx;
-      T v = T(0);
-      if (ez >= 0 && ez < g.nz && ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx)
-        v = E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)];
-      se[slot][sx][sy] = v;
+  auto issue_elems = [&](int ez, int slot) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int i = tid + s * KNT;
+      if (i < KU_EP) {
+        const int sy = i % (KY + 1), sx = i / (KY + 1);
+        const int ey = y0 - 1 + sy, ex = x0 - 1 + sx;
+        const bool ok = ez >= 0 && ez < g.nz && ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx;
+        const int64_t e = ok ? ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez) : 0;
+        cp_async_el<sizeof(T)>(&se[slot][sx][sy], E + e, ok);
+      }
+    }
+  };
+  // masked values of the staged plane into node slot `slot`
+  auto form_nodes = [&](int slot) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int i = tid + s * KNT;
+      if (i < KU_NP) {
+        const int sy = i % (KY + 2), sx = i / (KY + 2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T v = sa[c][i];
+          if (MODE != KU_PLAIN && !first) v = v + beta * sb[c][i];
+          su[slot][c][sx][sy] = ((fbs[s] >> c) & 1) ? T(0) : v;
+        }
+      }
     }
   };
 
-  load_nodes(zc0 - 1, 0);
-  load_nodes(zc0, 1);
-  load_elems(zc0 - 1, 0);
+  // prologue: node planes zc0-1, zc0 formed; element planes zc0-1, zc0 and node plane zc0+1 in flight
+  issue_nodes(zc0 - 1);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  form_nodes(0);
+  __syncthreads();
+  issue_nodes(zc0);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  form_nodes(1);
+  __syncthreads();
+  issue_elems(zc0 - 1, 0);
+  issue_elems(zc0, 1);
+  issue_nodes(zc0 + 1);
+  cp_async_commit();
   const int gy = y0 + ty, gx = x0 + tx;
   const bool own = gy < nny && gx < nnx;
   double dot = 0.0;
-  for (int k = 0; k < KZC; ++k) {
+  for (int k = 0; zc0 + k < zend; ++k) {
     const int z = zc0 + k;
-    if (z >= nnz) break;
-    load_nodes(z + 1, (k + 2) % 3);
-    load_elems(z, (k + 1) % 2);
+    cp_async_wait_all();
     __syncthreads();
+    form_nodes((k + 2) % 3);
+    __syncthreads();
+    if (z + 1 < zend) {
+      issue_nodes(z + 2);
+      issue_elems(z + 1, (k + 2) % 3);
+      cp_async_commit();
+    }
+    const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * z);
+    const uint8_t fbo = own ? fixbits[n] : uint8_t(0);
     if (own) {
       const T(*const pl[3])[KX + 2][KY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
-      const T(*const el[2])[KY + 1] = {se[k % 2], se[(k + 1) % 2]};
+      const T(*const el[2])[KY + 1] = {se[k % 3], se[(k + 1) % 3]};
       T y[3] = {T(0), T(0), T(0)};
       ku_half<T, 0>(pl, el, tx, ty, y);   // hexes above the node: local nodes 1-4
       ku_half<T, -1>(pl, el, tx, ty, y);  // hexes below the node: local nodes 5-8
-      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * z);
-      const uint8_t fb = fixbits[n];
-      T p0 = T(0), p1 = T(0), p2 = T(0);
-      if (fb || MODE != KU_PLAIN) ku_fetch<T, MODE>(in, zin, n, S, first, beta, p0, p1, p2);
-      if (fb) {
+      // the node's own value: masked copy in the ring for free DOFs, unmasked for fixed ones
+      T p[3] = {pl[1][0][tx + 1][ty + 1], pl[1][1][tx + 1][ty + 1], pl[1][2][tx + 1][ty + 1]};
+      if (fbo) {
+        T p0, p1, p2;
+        ku_fetch<T, MODE>(in, zin, n, S, first, beta, p0, p1, p2);
         const T cf = cfix[n];
-        if (fb & 1) y[0] = cf * p0;
-        if (fb & 2) y[1] = cf * p1;
-        if (fb & 4) y[2] = cf * p2;
+        if (fbo & 1) {
+          p[0] = p0;
+          y[0] = cf * p0;
+        }
+        if (fbo & 2) {
+          p[1] = p1;
+          y[1] = cf * p1;
+        }
+        if (fbo & 4) {
+          p[2] = p2;
+          y[2] = cf * p2;
+        }
       }
       out[n] = y[0];
       out[n + S] = y[1];
       out[n + 2 * S] = y[2];
       if (MODE != KU_PLAIN)
-        dot += double(p0) * double(y[0]) + double(p1) * double(y[1]) + double(p2) * double(y[2]);
+        dot += double(p[0]) * double(y[0]) + double(p[1]) * double(y[1]) + double(p[2]) * double(y[2]);
     }
-    __syncthreads();
   }
+  cp_async_wait_all();
   if (MODE != KU_PLAIN) {
     double v[1] = {dot}, tot[1];
     if (reduce_publish<1>(v, rs, tot) && tid == 0) sc->pq = tot[0];
   }
 }
 
+static int g_num_sms = 148;
+void prepare_fem_kernels() {
+  int dev = 0, n = 0;
+  TOPX_CUDA_OK(cudaGetDevice(&dev));
+  TOPX_CUDA_OK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  if (n > 0) g_num_sms = n;
+}
+
+// z-chunk length of the K*u launch: fewest (waves x halo-inclusive planes) for three CTAs per SM
+static int ku_z_chunk(int nny, int nnx, int nnz) {
+  const int64_t tiles = int64_t((nny + KY - 1) / KY) * ((nnx + KX - 1) / KX);
+  const int64_t slots = int64_t(g_num_sms) * 3;
+  int best = KZC;
+  int64_t bestCost = -1;
+  for (int zc = 6; zc <= 24; ++zc) {
+    const int64_t ctas = tiles * ((nnz + zc - 1) / zc);
+    const int64_t cost = ((ctas + slots - 1) / slots) * (zc + 2);
+    if (bestCost < 0 || cost < bestCost) {
+      bestCost = cost;
+      best = zc;
+    }
+  }
+  return best;
+}
+
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
+  (void)pout;
+  const int zc = ku_z_chunk(g.nny(), g.nnx(), g.nnz());
   dim3 blk(KY, KX, 1);
-  dim3 grd((g.nny() + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + KZC - 1) / KZC);
+  dim3 grd((g.nny() + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + zc - 1) / zc);
   if (mode == KU_PLAIN)
-    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   else
-    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

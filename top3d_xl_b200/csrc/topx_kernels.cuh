@@ -98,6 +98,8 @@ void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks
 void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* Ct);
 // one-time per-device kernel attributes of the coarse factorisation (call outside stream capture)
 void prepare_coarse_kernels();
+// caches the SM count used to shape the K*u launch (call once per device, outside capture)
+void prepare_fem_kernels();
 // twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
 // Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes);
 // gj_scratch holds 2 * (64*64 + 128*m) doubles
