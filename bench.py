@@ -8,10 +8,10 @@ rMin=sqrt(3) -- TOP3D_XL(true(128,256,128),'GLOBAL',0.12,50,sqrt(3)).  One
 factorisation, multigrid PCG, compliance, PDE sensitivity filter, OC update),
 with all state resident in HBM.
 
-`value` is the mixed-precision engine (FP64 Krylov iteration and operator,
-FP32 multigrid preconditioner and filter); the same run in plain FP64 is
-measured beside it and the per-iteration relative compliance error of mixed
-vs FP64 is reported.
+`value` is the FP64 engine (the reference's own precision).  The mixed-precision
+engine (FP64 Krylov iteration and operator, FP32 multigrid preconditioner and
+filter) is measured beside it, with its per-iteration relative compliance
+error against FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
 
@@ -39,7 +39,7 @@ WORKLOADS = {
     "cuboid50": dict(shape=(50, 100, 50), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
     "cuboid25": dict(shape=(25, 50, 25), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
 }
-METRIC = "OC iterations/s (GLOBAL, mixed precision; FP64 beside it)"
+METRIC = "OC iterations/s (GLOBAL, FP64; mixed precision beside it)"
 # DRAM bytes (read + write) per grid node of one K*u launch in PCG mode, from an ncu capture of
 # the 128x256x128 cuboid (dram__bytes_read.sum + dram__bytes_write.sum = 259.68 MB + 86.09 MB
 # over 4,276,737 nodes); the traffic of a launch scales with its node count.
@@ -276,8 +276,8 @@ def main(argv=None):
     if dist:
         dist.barrier()
     with Clocks(device) as clk:
-        mixed = run_native(wl, "mixed", a.steps, a.warmup, device, profile_steps=2)
-    ms_local = mixed["ms"]
+        fp64 = run_native(wl, "fp64", a.steps, a.warmup, device, profile_steps=2)
+    ms_local = fp64["ms"]
     if dist:
         t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -289,7 +289,7 @@ def main(argv=None):
         if dist:
             dist.destroy_process_group()
         return 0
-    fp64 = run_native(wl, "fp64", a.steps, a.warmup, device)
+    mixed = run_native(wl, "mixed", a.steps, a.warmup, device)
     value = ws * a.steps / (ms_max / 1000.0)
     cm = np.array([h["c"] for h in mixed["hist"]])
     cd = np.array([h["c"] for h in fp64["hist"]])
@@ -299,36 +299,36 @@ def main(argv=None):
     # Per launch it reads p_old and z and writes q (3 doubles per node each), reads the
     # moduli (1 double per element) and the free-DOF bits (1 byte per node): 73 B/node +
     # 8 B/element; per node 8 hexes x 3 rows x 24 DOFs + 24 scalings = 600 FMA.
-    prof = mixed["prof"]
-    nn = mixed["nnodes"]
-    alg_bytes = 73 * nn + 8 * mixed["ne"]
+    prof = fp64["prof"]
+    nn = fp64["nnodes"]
+    alg_bytes = 73 * nn + 8 * fp64["ne"]
     flop = 2 * 600 * nn
     ku_ms = prof["ku_ms"] / max(1, prof["ku_launches"])
     achieved = alg_bytes / (ku_ms * 1e-3) / 1e9
     tflops = flop / (ku_ms * 1e-3) / 1e12
     peak, kind = peaks()
-    its_mixed = [k for h in mixed["hist"][a.warmup:] for k in h["its"]]
     its64 = [k for h in fp64["hist"][a.warmup:] for k in h["its"]]
-    fits = [h["filter_its"] for h in mixed["hist"][a.warmup:]]
-    e2e = run_e2e(wl, "mixed", max(3, a.steps // 2), 2, device)
+    its_mixed = [k for h in mixed["hist"][a.warmup:] for k in h["its"]]
+    fits = [h["filter_its"] for h in fp64["hist"][a.warmup:]]
+    e2e = run_e2e(wl, "fp64", max(3, a.steps // 2), 2, device)
 
     def phases(run):
         hs = run["hist"][a.warmup:]
         return {k: 1000.0 * float(np.mean([h[k] for h in hs])) for k in ("t_assemble", "t_cg", "t_filter", "t_opt")}
     line = {"metric": METRIC, "value": value, "unit": "OC iterations/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f64 (Krylov iteration, operator, dots, compliance, OC) + f32 (multigrid preconditioner, filter)",
+            "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (built-in cuboid BCs)", "config": cfg,
-            "fp64": {"value": a.steps / (fp64["ms"] / 1000.0), "ms_per_step": fp64["ms"] / a.steps,
-                     "pcg_its_per_step": float(np.mean(its64))},
-            "mixed_vs_fp64": {"speedup": (a.steps / (ms_local / 1000.0)) / (a.steps / (fp64["ms"] / 1000.0)),
-                              "max_rel_compliance_err": relerr, "iterations_compared": n},
-            "pcg_its_per_step": float(np.mean(its_mixed)), "filter_its_per_step": float(np.mean(fits)),
-            "phases_ms": {"mixed": phases(mixed), "fp64": phases(fp64)},
+            "mixed": {"value": a.steps / (mixed["ms"] / 1000.0), "ms_per_step": mixed["ms"] / a.steps,
+                      "dtype": "f64 Krylov iteration, operator, dots, compliance, OC; f32 multigrid "
+                               "preconditioner and filter",
+                      "pcg_its_per_step": float(np.mean(its_mixed)),
+                      "max_rel_compliance_err_vs_fp64": relerr, "iterations_compared": n},
+            "pcg_its_per_step": float(np.mean(its64)), "filter_its_per_step": float(np.mean(fits)),
+            "phases_ms": {"fp64": phases(fp64), "mixed": phases(mixed)},
             "sections_ms_per_step": {k: round(v[0] / prof["steps"], 3) for k, v in prof["sections"].items()},
             "section_groups_per_step": {k: round(v[1] / prof["steps"], 1) for k, v in prof["sections"].items()},
-            "gpu_launches": mixed["launches"],
+            "gpu_launches": fp64["launches"],
             "roofline": {"kernel": "k_ku_l1<double, KU_P_UPDATE> (level-1 K*u, PCG mode)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": kind, "algorithmic_bytes_per_launch": alg_bytes,
