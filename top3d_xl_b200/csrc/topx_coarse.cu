@@ -540,20 +540,23 @@ __global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet s
   }
 }
 
+// Tiles of one exchange update: all of them (GJ_ALL), only those in row or column block kc
+// (GJ_CRIT: what the next pivot and panel read), or all the others (GJ_REST).
+enum GJTiles { GJ_ALL = 0, GJ_CRIT = 1, GJ_REST = 2 };
+
 // rank-kb exchange update of one 64x64 tile per CTA (4x4 outputs per thread); both rank-64
 // operands (Ct rows of this tile, R or Pinv columns) come in with one round of loads, and the
 // old tile is fetched into registers before the product.
-__global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJSet set) {
-  extern __shared__ __align__(16) double gj_smem[];
+__device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSet& set, int z, int ib, int jb,
+                                               double* gj_smem) {
   double(*sC)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem);            // [kt][row]
   double(*sR)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem + GJB * GJB);  // [kt][col]
-  const int z = blockIdx.z;
   double* __restrict__ A = z ? set.A[1] : set.A[0];
   const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
   const double* __restrict__ R = z ? set.R[1] : set.R[0];
   const double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
-  const int i0 = blockIdx.y * GJB, j0 = blockIdx.x * GJB;
+  const int i0 = ib * GJB, j0 = jb * GJB;
   const bool iK = (i0 == k0), jK = (j0 == k0);
   if (iK) {  // rows of the pivot block: new row panel / Pinv
     for (int i = tid; i < GJB * GJB; i += 256) {
@@ -625,40 +628,95 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJS
   }
 }
 
-void prepare_coarse_kernels() {
-  TOPX_CUDA_OK(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(GJ_UPDATE_SMEM)));
+
+// the kernel: tiles selected by `tiles` (see GJTiles), taken in a CTA-stride loop
+__global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJSet set, int tiles, int kc) {
+  extern __shared__ __align__(16) double gj_smem[];
+  const int nt = (m + GJB - 1) / GJB;
+  const int ntiles = tiles == GJ_ALL ? nt * nt : tiles == GJ_CRIT ? 2 * nt - 1 : (nt - 1) * (nt - 1);
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    int ib, jb;
+    if (tiles == GJ_ALL) {
+      ib = b / nt;
+      jb = b - ib * nt;
+    } else if (tiles == GJ_CRIT) {
+      if (b < nt) {
+        ib = kc;
+        jb = b;
+      } else {
+        ib = b - nt;
+        ib += ib >= kc;
+        jb = kc;
+      }
+    } else {
+      ib = b / (nt - 1);
+      jb = b - ib * (nt - 1);
+      ib += ib >= kc;
+      jb += jb >= kc;
+    }
+    gj_update_tile(m, k0, kb, set, int(blockIdx.z), ib, jb, gj_smem);
+    __syncthreads();
+  }
 }
 
-static void spd_inverse_batched(cudaStream_t st, int m, int nset, const GJSet& set) {
+// The side-stream update runs on GJ_REST_CTAS CTAs that each reserve a whole SM (their shared
+// memory request leaves no room for another CTA), so the latency-bound pivot and panel of the
+// next step get SMs of their own instead of sharing FP64 pipes with update tiles.
+constexpr int GJ_REST_CTAS = 96;
+constexpr size_t GJ_REST_SMEM = 200 * 1024;
+
+void prepare_coarse_kernels() {
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(GJ_REST_SMEM)));
+}
+
+// Exchange steps with one step of lookahead: after the panel of step k, the tiles that step
+// k+1's pivot and panel read (row and column block k+1) are updated on the main stream while
+// all other tiles are updated on the side stream, overlapping step k+1's pivot and panel.
+// Steps alternate between two scratch sets, since the side stream still reads step k's
+// (Pinv, R, Ct) while step k+1 writes its own.
+static void spd_inverse_batched(cudaStream_t st, const GJStreams& gs, int m, int nset, const GJSet (&sets)[2]) {
   const unsigned nt = (m + GJB - 1) / GJB;
-  for (int k0 = 0; k0 < m; k0 += GJB) {
+  for (unsigned k = 0; k < nt; ++k) {
+    const GJSet& set = sets[k % 2];
+    const int k0 = int(k) * GJB;
     const int kb = (m - k0) < GJB ? (m - k0) : GJB;
     (k_gj_pivot<<<dim3(1 + nt, 1, nset), GJ_PIVOT_THREADS, 0, st>>>(m, k0, kb, set), topx::count_launch());
     (k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
-    (k_gj_update<<<dim3(nt, nt, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set), topx::count_launch());
+    if (k + 1 < nt) {
+      TOPX_CUDA_OK(cudaEventRecord(gs.panel[k % 2], st));
+      TOPX_CUDA_OK(cudaStreamWaitEvent(gs.side, gs.panel[k % 2], 0));
+      const unsigned nrest = std::min((nt - 1) * (nt - 1), unsigned(GJ_REST_CTAS / nset));
+      (k_gj_update<<<dim3(nrest, 1, nset), 256, GJ_REST_SMEM, gs.side>>>(m, k0, kb, set, GJ_REST, int(k + 1)),
+       topx::count_launch());
+      TOPX_CUDA_OK(cudaEventRecord(gs.rest[k % 2], gs.side));
+      if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
+      (k_gj_update<<<dim3(2 * nt - 1, 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_CRIT, int(k + 1)),
+       topx::count_launch());
+    } else {
+      if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
+      (k_gj_update<<<dim3(nt * nt, 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_ALL, 0),
+       topx::count_launch());
+    }
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* Ct) {
-  GJSet set{{A, A}, {Pinv, Pinv}, {R, R}, {Ct, Ct}};
-  spd_inverse_batched(st, m, 1, set);
-}
-
-void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const double* Bup, double* Sinv, double* X,
-                        double* XT, double* gj_scratch) {
+void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const double* A, const double* Bup,
+                        double* Sinv, double* X, double* XT, double* gj_scratch) {
   const int m = si.m, ns = si.ns, mid = ns / 2;
   const int64_t mm = int64_t(m) * m;
   const int64_t bs = int64_t(si.nu) * si.nv * 81;
   const unsigned nbm = grid1d(mm, 256);
-  // per chain scratch: Pinv 64x64, R 64xm, Ct 64xm
+  // scratch per (step parity, chain): Pinv 64x64, R 64xm, Ct 64xm
   const int64_t gjs = 64 * 64 + 2 * 64 * int64_t(m);
-  GJSet set{};
-  for (int c = 0; c < 2; ++c) {
-    set.Pinv[c] = gj_scratch + c * gjs;
-    set.R[c] = set.Pinv[c] + 64 * 64;
-    set.Ct[c] = set.R[c] + 64 * int64_t(m);
-  }
+  GJSet sets[2] = {};
+  for (int p = 0; p < 2; ++p)
+    for (int c = 0; c < 2; ++c) {
+      sets[p].Pinv[c] = gj_scratch + (2 * p + c) * gjs;
+      sets[p].R[c] = sets[p].Pinv[c] + 64 * 64;
+      sets[p].Ct[c] = sets[p].R[c] + 64 * int64_t(m);
+    }
+  GJSet& set = sets[0];
   const int ntop = mid, nbot = ns - 1 - mid;
   for (int k = 0; k < std::max(ntop, nbot); ++k) {
     SchurOp so[2] = {};
@@ -677,8 +735,10 @@ void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const dou
       set.A[nset] = Sinv + s * mm;
       ++nset;
     }
+    sets[1].A[0] = set.A[0];
+    sets[1].A[1] = set.A[1];
     (k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]), topx::count_launch());
-    spd_inverse_batched(st, m, nset, set);
+    spd_inverse_batched(st, gs, m, nset, sets);
     if (k < ntop) {  // L_k = B_k^T S_k^{-1}
       fo[nform++] = FormOp{Bup + k * bs, Sinv + k * mm, X + k * mm, XT + k * mm, 0};
     }
@@ -693,8 +753,8 @@ void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const dou
              mid > 0 ? Bup + (mid - 1) * bs : nullptr, mid < ns - 1 ? X + mid * mm : nullptr,
              mid < ns - 1 ? Bup + mid * bs : nullptr};
   (k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm), topx::count_launch());
-  set.A[0] = Sinv + mid * mm;
-  spd_inverse_batched(st, m, 1, set);
+  set.A[0] = sets[1].A[0] = Sinv + mid * mm;
+  spd_inverse_batched(st, gs, m, 1, sets);
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

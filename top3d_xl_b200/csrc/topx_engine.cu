@@ -19,6 +19,9 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
   TOPX_CUDA_OK(cudaSetDevice(device));
   // blocking stream: ordered with the synchronous cudaMemset/cudaMemcpy calls of the set-up code
   TOPX_CUDA_OK(cudaStreamCreate(&st));
+  TOPX_CUDA_OK(cudaStreamCreate(&gjs.side));
+  for (cudaEvent_t* e : {&gjs.panel[0], &gjs.panel[1], &gjs.rest[0], &gjs.rest[1]})
+    TOPX_CUDA_OK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   prepare_coarse_kernels();
   prepare_fem_kernels();
   nl = M.numLevels;
@@ -207,7 +210,7 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
       slabLT32.alloc(mm * nsm1);
     }
     slabBup.alloc(size_t(si.nu) * si.nv * 81 * nsm1);
-    gjP.alloc(2 * (64 * 64 + size_t(128) * si.m));
+    gjP.alloc(4 * (64 * 64 + size_t(128) * si.m));
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
     coopCtas = slab_solve_coop_ctas(si.m);
@@ -285,6 +288,9 @@ Engine::~Engine() {
     if (e) cudaEventDestroy(e);
   if (h_sc) cudaFreeHost(h_sc);
   if (h_bar) cudaFreeHost(h_bar);
+  for (auto e : {gjs.panel[0], gjs.panel[1], gjs.rest[0], gjs.rest[1]})
+    if (e) cudaEventDestroy(e);
+  if (gjs.side) cudaStreamDestroy(gjs.side);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -409,7 +415,7 @@ void Engine::factor_coarsest() {
   launch_slab_assemble(st, G[nl - 1], si, Ks[nl - 1].p, present[nl - 1].p, slabA.p, slabBup.p);
   sec_end();
   sec_begin(SEC_INVERSE);
-  launch_slab_factor(st, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p, gjP.p);
+  launch_slab_factor(st, gjs, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p, gjP.p);
   sec_end();
   if (prec == PREC_MIXED) {
     launch_convert<double, float>(st, slabSinv.p, slabSinv32.p, int64_t(slabSinv.n));

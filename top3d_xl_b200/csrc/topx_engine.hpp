@@ -151,6 +151,7 @@ class Engine {
   Model& M;
   int prec;
   cudaStream_t st = nullptr;
+  GJStreams gjs{};  // side stream + events of the coarse factorisation
   int nl = 0;
   std::vector<Grid> G;  // per level
   int64_t Ne = 0, Nn = 0;

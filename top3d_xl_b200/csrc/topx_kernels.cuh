@@ -94,17 +94,21 @@ struct SlabInfo {
 };
 void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks, const uint8_t* present, double* A,
                           double* Bup);
-// in-place inverse of an SPD m x m matrix; Pinv 64x64, R 64 x m, C m x 64 scratch
-void launch_spd_inverse(cudaStream_t st, int m, double* A, double* Pinv, double* R, double* Ct);
 // one-time per-device kernel attributes of the coarse factorisation (call outside stream capture)
 void prepare_coarse_kernels();
 // caches the SM count used to shape the K*u launch (call once per device, outside capture)
 void prepare_fem_kernels();
 // twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
 // Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes);
-// gj_scratch holds 2 * (64*64 + 128*m) doubles
-void launch_slab_factor(cudaStream_t st, SlabInfo si, const double* A, const double* Bup, double* Inv, double* X,
-                        double* XT, double* gj_scratch);
+// gj_scratch holds 4 * (64*64 + 128*m) doubles
+// side stream and events of the factorisation's lookahead (the side stream joins graph captures)
+struct GJStreams {
+  cudaStream_t side;
+  cudaEvent_t panel[2];
+  cudaEvent_t rest[2];
+};
+void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const double* A, const double* Bup,
+                        double* Inv, double* X, double* XT, double* gj_scratch);
 // x = K_coarsest^{-1} b; bs, W, V, xs are ns*m FP64 scratch vectors in slab order
 template <typename T, typename TM>
 void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT, const T* b,
