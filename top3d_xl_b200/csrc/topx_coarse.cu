@@ -547,104 +547,108 @@ enum GJTiles { GJ_ALL = 0, GJ_CRIT = 1, GJ_REST = 2 };
 // rank-kb exchange update of one 64x64 tile per CTA (4x4 outputs per thread); both rank-64
 // operands (Ct rows of this tile, R or Pinv columns) come in with one round of loads, and the
 // old tile is fetched into registers before the product.
-__device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSet& set, int z, int ib, int jb,
+// One TS x TS tile (TS = 64, or a 32 x 32 quarter) with origin (i0, j0): (TS/16)^2 outputs
+// per thread.  Tiles in the pivot row block take the new row panel (or Pinv); tiles in the
+// pivot column block take C_i Pinv; all others add C_i R_j.
+template <int TS>
+__device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSet& set, int z, int i0, int j0,
                                                double* gj_smem) {
-  double(*sC)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem);            // [kt][row]
-  double(*sR)[GJB] = reinterpret_cast<double(*)[GJB]>(gj_smem + GJB * GJB);  // [kt][col]
+  constexpr int PT = TS / 16;
+  double(*sC)[TS] = reinterpret_cast<double(*)[TS]>(gj_smem);            // [kt][row]
+  double(*sR)[TS] = reinterpret_cast<double(*)[TS]>(gj_smem + GJB * TS);  // [kt][col]
   double* __restrict__ A = z ? set.A[1] : set.A[0];
   const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
   const double* __restrict__ R = z ? set.R[1] : set.R[0];
   const double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
-  const int i0 = ib * GJB, j0 = jb * GJB;
-  const bool iK = (i0 == k0), jK = (j0 == k0);
+  const bool iK = (i0 >= k0 && i0 < k0 + GJB), jK = (j0 >= k0 && j0 < k0 + GJB);
   if (iK) {  // rows of the pivot block: new row panel / Pinv
-    for (int i = tid; i < GJB * GJB; i += 256) {
-      const int rr = i / GJB, cc = i % GJB;
-      const int ii = i0 + rr, j = j0 + cc;
-      if (rr < kb && j < m) A[int64_t(ii) * m + j] = jK ? Pinv[rr * GJB + cc] : R[int64_t(rr) * m + j];
+    for (int i = tid; i < TS * TS; i += 256) {
+      const int ii = i0 + i / TS, j = j0 + i % TS;
+      const int pr = ii - k0;
+      if (pr < kb && j < m) A[int64_t(ii) * m + j] = jK ? Pinv[pr * GJB + (j - k0)] : R[int64_t(pr) * m + j];
     }
     return;
   }
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
+  for (int e = 0; e < TS / 4; ++e) {
     const int i = tid + 256 * e;
-    const int kt = i >> 6, rr = i & 63;
+    const int kt = i / TS, rr = i % TS;
     const int ii = i0 + rr;
     sC[kt][rr] = (kt < kb && ii < m) ? Ct[int64_t(kt) * m + ii] : 0.0;
   }
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
+  for (int e = 0; e < TS / 4; ++e) {
     const int i = tid + 256 * e;
-    const int kt = i >> 6, cc = i & 63;
+    const int kt = i / TS, cc = i % TS;
     const int j = j0 + cc;
     double v = 0.0;
-    if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + cc] : R[int64_t(kt) * m + j];
+    if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + (j - k0)] : R[int64_t(kt) * m + j];
     sR[kt][cc] = v;
   }
-  double old[4][4];
+  double acc[PT][PT];
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < PT; ++q)
 #pragma unroll
-    for (int w = 0; w < 4; ++w) {
-      const int ii = i0 + 4 * ty + q, j = j0 + 4 * tx + w;
-      old[q][w] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
+    for (int w = 0; w < PT; ++w) {
+      const int ii = i0 + PT * ty + q, j = j0 + PT * tx + w;
+      acc[q][w] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
     }
   __syncthreads();
-  double acc[4][4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int w = 0; w < 4; ++w) acc[q][w] = old[q][w];
 #pragma unroll 8
   for (int k = 0; k < GJB; ++k) {
-    const double2 c01 = *reinterpret_cast<const double2*>(&sC[k][4 * ty]);
-    const double2 c23 = *reinterpret_cast<const double2*>(&sC[k][4 * ty + 2]);
-    const double2 r01 = *reinterpret_cast<const double2*>(&sR[k][4 * tx]);
-    const double2 r23 = *reinterpret_cast<const double2*>(&sR[k][4 * tx + 2]);
-    const double cv[4] = {c01.x, c01.y, c23.x, c23.y};
-    const double rv[4] = {r01.x, r01.y, r23.x, r23.y};
+    double cv[PT], rv[PT];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int h = 0; h < PT; h += 2) {
+      const double2 c = *reinterpret_cast<const double2*>(&sC[k][PT * ty + h]);
+      const double2 r = *reinterpret_cast<const double2*>(&sR[k][PT * tx + h]);
+      cv[h] = c.x;
+      cv[h + 1] = c.y;
+      rv[h] = r.x;
+      rv[h + 1] = r.y;
+    }
 #pragma unroll
-      for (int w = 0; w < 4; ++w) acc[q][w] = fma(cv[q], rv[w], acc[q][w]);
+    for (int q = 0; q < PT; ++q)
+#pragma unroll
+      for (int w = 0; w < PT; ++w) acc[q][w] = fma(cv[q], rv[w], acc[q][w]);
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int ii = i0 + 4 * ty + q;
+  for (int q = 0; q < PT; ++q) {
+    const int ii = i0 + PT * ty + q;
     if (ii >= m) continue;
-    const int jb = j0 + 4 * tx;
+    const int jb = j0 + PT * tx;
     double* Ar = A + int64_t(ii) * m;
     // 16-byte stores only where the absolute address is 16-byte aligned (matrix bases
     // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
-    if (jb + 3 < m && (reinterpret_cast<uintptr_t>(Ar + jb) & 15) == 0) {
-      *reinterpret_cast<double2*>(Ar + jb) = make_double2(acc[q][0], acc[q][1]);
-      *reinterpret_cast<double2*>(Ar + jb + 2) = make_double2(acc[q][2], acc[q][3]);
+    if (jb + PT - 1 < m && (reinterpret_cast<uintptr_t>(Ar + jb) & 15) == 0) {
+#pragma unroll
+      for (int w = 0; w < PT; w += 2) *reinterpret_cast<double2*>(Ar + jb + w) = make_double2(acc[q][w], acc[q][w + 1]);
     } else {
 #pragma unroll
-      for (int w = 0; w < 4; ++w)
+      for (int w = 0; w < PT; ++w)
         if (jb + w < m) Ar[jb + w] = acc[q][w];
     }
   }
 }
 
-
 // the kernel: tiles selected by `tiles` (see GJTiles), taken in a CTA-stride loop
 __global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJSet set, int tiles, int kc) {
   extern __shared__ __align__(16) double gj_smem[];
   const int nt = (m + GJB - 1) / GJB;
-  const int ntiles = tiles == GJ_ALL ? nt * nt : tiles == GJ_CRIT ? 2 * nt - 1 : (nt - 1) * (nt - 1);
+  // the critical tiles go in 32 x 32 quarters: four times the CTAs, a quarter of the latency
+  const int ntiles = tiles == GJ_ALL ? nt * nt : tiles == GJ_CRIT ? 4 * (2 * nt - 1) : (nt - 1) * (nt - 1);
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     int ib, jb;
     if (tiles == GJ_ALL) {
       ib = b / nt;
       jb = b - ib * nt;
     } else if (tiles == GJ_CRIT) {
-      if (b < nt) {
+      const int tb = b >> 2;
+      if (tb < nt) {
         ib = kc;
-        jb = b;
+        jb = tb;
       } else {
-        ib = b - nt;
+        ib = tb - nt;
         ib += ib >= kc;
         jb = kc;
       }
@@ -654,7 +658,11 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJS
       ib += ib >= kc;
       jb += jb >= kc;
     }
-    gj_update_tile(m, k0, kb, set, int(blockIdx.z), ib, jb, gj_smem);
+    if (tiles == GJ_CRIT)
+      gj_update_tile<32>(m, k0, kb, set, int(blockIdx.z), ib * GJB + 32 * ((b >> 1) & 1), jb * GJB + 32 * (b & 1),
+                         gj_smem);
+    else
+      gj_update_tile<64>(m, k0, kb, set, int(blockIdx.z), ib * GJB, jb * GJB, gj_smem);
     __syncthreads();
   }
 }
@@ -690,7 +698,8 @@ static void spd_inverse_batched(cudaStream_t st, const GJStreams& gs, int m, int
        topx::count_launch());
       TOPX_CUDA_OK(cudaEventRecord(gs.rest[k % 2], gs.side));
       if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
-      (k_gj_update<<<dim3(2 * nt - 1, 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_CRIT, int(k + 1)),
+      (k_gj_update<<<dim3(4 * (2 * nt - 1), 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_CRIT,
+                                                                                int(k + 1)),
        topx::count_launch());
     } else {
       if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
