@@ -398,9 +398,10 @@ __device__ __forceinline__ double recip_newton(double v) {
 }
 
 // CTA 0: P = A[K,K] -> Pinv.  Thread (ri, ci) = (tid / 16, tid % 16) holds rows 8ri..8ri+7 and
-// columns 4ci..4ci+3 of the block in registers.  Each exchange step publishes the pivot row,
-// the pivot column and 1/pivot through double-buffered shared arrays (one barrier per step);
-// every element then takes one FMA and the owners of the pivot row and column overwrite theirs.
+// columns 4ci..4ci+3 of the block in registers.  Each exchange step eliminates a 2x2 pivot
+// block (owned by one thread, which publishes its inverse) with the two pivot rows and columns
+// published through double-buffered shared arrays: one barrier per two pivots; every element
+// then takes two FMAs and the owners of the pivot rows and columns overwrite theirs.
 // Rows and columns >= kb hold the identity, which the exchange leaves unchanged.
 // CTAs 1..: 64 rows each of the old column panel, transposed into Ct.
 __global__ void __launch_bounds__(GJ_PIVOT_THREADS) k_gj_pivot(int m, int k0, int kb, GJSet set) {
@@ -427,9 +428,9 @@ __global__ void __launch_bounds__(GJ_PIVOT_THREADS) k_gj_pivot(int m, int k0, in
     return;
   }
   double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
-  __shared__ __align__(16) double rowb[2][GJB];
-  __shared__ __align__(16) double colb[2][GJB];
-  __shared__ double rpb[2];
+  __shared__ __align__(16) double rowb[2][2][GJB];
+  __shared__ __align__(16) double colb[2][2][GJB];
+  __shared__ double qb[2][4];
   const int ci = tid & 15, ri = tid >> 4;
   double a[8][4];
 #pragma unroll
@@ -439,50 +440,90 @@ __global__ void __launch_bounds__(GJ_PIVOT_THREADS) k_gj_pivot(int m, int k0, in
       const int r = 8 * ri + i, c = 4 * ci + q;
       a[i][q] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
     }
+  // exchange steps on 2x2 pivot blocks {t, t+1}, Q = P^-1:
+  //   A_TT <- Q,  A_Tc <- -Q A_Tc,  A_rT <- A_rT Q = w_r,  A_rc <- A_rc - w_r A_Tc
+  // (a pivot at or past kb is an identity row and column, which the exchange leaves alone)
   for (int tb = 0; tb < GJB / 8; ++tb) {
     if (8 * tb >= kb) break;
 #pragma unroll
-    for (int qq = 0; qq < 8; ++qq) {
+    for (int qq = 0; qq < 8; qq += 2) {
       const int t = 8 * tb + qq;
       if (t >= kb) break;
-      const int buf = qq & 1;  // = t & 1
-      const int cq = qq & 3;   // local column of pivot column t in its owners
+      const int buf = (qq >> 1) & 1;  // = (t / 2) & 1
+      const int cq = qq & 3;          // local column of pivot t in its owners (0 or 2)
       const bool rowOwner = (ri == tb);
       const bool colOwner = (ci == 2 * tb + (qq >> 2));
       if (rowOwner) {
-        *reinterpret_cast<double2*>(&rowb[buf][4 * ci]) = make_double2(a[qq][0], a[qq][1]);
-        *reinterpret_cast<double2*>(&rowb[buf][4 * ci + 2]) = make_double2(a[qq][2], a[qq][3]);
-        if (colOwner) rpb[buf] = recip_newton(a[qq][cq]);
+        *reinterpret_cast<double2*>(&rowb[buf][0][4 * ci]) = make_double2(a[qq][0], a[qq][1]);
+        *reinterpret_cast<double2*>(&rowb[buf][0][4 * ci + 2]) = make_double2(a[qq][2], a[qq][3]);
+        *reinterpret_cast<double2*>(&rowb[buf][1][4 * ci]) = make_double2(a[qq + 1][0], a[qq + 1][1]);
+        *reinterpret_cast<double2*>(&rowb[buf][1][4 * ci + 2]) = make_double2(a[qq + 1][2], a[qq + 1][3]);
+        if (colOwner) {
+          const double p00 = a[qq][cq], p01 = a[qq][cq + 1], p10 = a[qq + 1][cq], p11 = a[qq + 1][cq + 1];
+          const double rd = recip_newton(p00 * p11 - p01 * p10);
+          qb[buf][0] = p11 * rd;
+          qb[buf][1] = -p01 * rd;
+          qb[buf][2] = -p10 * rd;
+          qb[buf][3] = p00 * rd;
+        }
       }
       if (colOwner) {
 #pragma unroll
-        for (int i = 0; i < 8; i += 2)
-          *reinterpret_cast<double2*>(&colb[buf][8 * ri + i]) = make_double2(a[i][cq], a[i + 1][cq]);
+        for (int i = 0; i < 8; i += 2) {
+          *reinterpret_cast<double2*>(&colb[buf][0][8 * ri + i]) = make_double2(a[i][cq], a[i + 1][cq]);
+          *reinterpret_cast<double2*>(&colb[buf][1][8 * ri + i]) = make_double2(a[i][cq + 1], a[i + 1][cq + 1]);
+        }
       }
       __syncthreads();
-      const double rp = rpb[buf];
-      const double2 r01 = *reinterpret_cast<const double2*>(&rowb[buf][4 * ci]);
-      const double2 r23 = *reinterpret_cast<const double2*>(&rowb[buf][4 * ci + 2]);
-      const double rc[4] = {r01.x, r01.y, r23.x, r23.y};
-      double cr[8];
+      const double q00 = qb[buf][0], q01 = qb[buf][1], q10 = qb[buf][2], q11 = qb[buf][3];
+      double r0[4], r1[4];
+      {
+        const double2 x01 = *reinterpret_cast<const double2*>(&rowb[buf][0][4 * ci]);
+        const double2 x23 = *reinterpret_cast<const double2*>(&rowb[buf][0][4 * ci + 2]);
+        const double2 y01 = *reinterpret_cast<const double2*>(&rowb[buf][1][4 * ci]);
+        const double2 y23 = *reinterpret_cast<const double2*>(&rowb[buf][1][4 * ci + 2]);
+        r0[0] = x01.x;
+        r0[1] = x01.y;
+        r0[2] = x23.x;
+        r0[3] = x23.y;
+        r1[0] = y01.x;
+        r1[1] = y01.y;
+        r1[2] = y23.x;
+        r1[3] = y23.y;
+      }
+      double w0[8], w1[8];
 #pragma unroll
       for (int i = 0; i < 8; i += 2) {
-        const double2 cv = *reinterpret_cast<const double2*>(&colb[buf][8 * ri + i]);
-        cr[i] = cv.x * rp;
-        cr[i + 1] = cv.y * rp;
+        const double2 c0 = *reinterpret_cast<const double2*>(&colb[buf][0][8 * ri + i]);
+        const double2 c1 = *reinterpret_cast<const double2*>(&colb[buf][1][8 * ri + i]);
+        w0[i] = fma(c0.x, q00, c1.x * q10);
+        w1[i] = fma(c0.x, q01, c1.x * q11);
+        w0[i + 1] = fma(c0.y, q00, c1.y * q10);
+        w1[i + 1] = fma(c0.y, q01, c1.y * q11);
       }
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) a[i][q] = fma(-cr[i], rc[q], a[i][q]);
+        for (int q = 0; q < 4; ++q) a[i][q] = fma(-w1[i], r1[q], fma(-w0[i], r0[q], a[i][q]));
       if (rowOwner) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) a[qq][q] = -rc[q] * rp;
+        for (int q = 0; q < 4; ++q) {
+          a[qq][q] = -fma(q00, r0[q], q01 * r1[q]);
+          a[qq + 1][q] = -fma(q10, r0[q], q11 * r1[q]);
+        }
       }
       if (colOwner) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) a[i][cq] = cr[i];
-        if (rowOwner) a[qq][cq] = rp;
+        for (int i = 0; i < 8; ++i) {
+          a[i][cq] = w0[i];
+          a[i][cq + 1] = w1[i];
+        }
+        if (rowOwner) {
+          a[qq][cq] = q00;
+          a[qq][cq + 1] = q01;
+          a[qq + 1][cq] = q10;
+          a[qq + 1][cq + 1] = q11;
+        }
       }
     }
   }
