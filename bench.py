@@ -211,6 +211,60 @@ def cpu_sample(wl, its_per_oc, filter_its_per_oc, budget_s=30.0):
                 sec_per_oc=t_oc)
 
 
+def serve_stream(n_jobs, seed=5, mean_gap=0.05):
+    """The served workload: n_jobs solid cuboids with Poisson arrivals (mean gap 50 ms),
+    dimensions (16, 32, 16) x s with one common scale s log-uniform in [1, 6] (rounded), 70 %
+    GLOBAL (V0 uniform 0.08-0.2, 50 iterations) and 30 % LOCAL (V0 0.5, 100 iterations, local
+    radius 6), rMin sqrt(3).  Seeded numpy.random.default_rng."""
+    rng = np.random.default_rng(seed)
+    jobs, t = [], 0.0
+    for _ in range(n_jobs):
+        t += rng.exponential(mean_gap)
+        s = math.exp(rng.uniform(0.0, math.log(6.0)))
+        shape = (max(3, round(16 * s)), max(3, round(32 * s)), max(3, round(16 * s)))
+        if rng.uniform() < 0.7:
+            jobs.append(dict(at=t, shape=shape, cons="GLOBAL", V0=float(rng.uniform(0.08, 0.2)), nLoop=50, rHat=0.0))
+        else:
+            jobs.append(dict(at=t, shape=shape, cons="LOCAL", V0=0.5, nLoop=100, rHat=6.0))
+    return jobs
+
+
+def run_served(jobs, precision, slots, device):
+    """Submit `jobs` to a Server on their arrival schedule and wait for all; per-job latency is
+    completion minus submission on the server clock."""
+    from top3d_xl_b200 import Server
+    with Server(slots=slots, precision=precision, device=device) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for j in jobs:
+            delay = j["at"] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(j["shape"], j["cons"], j["V0"], j["nLoop"], math.sqrt(3), j["rHat"]))
+        res = [srv.wait(i) for i in ids]
+        stats = srv.stats()
+        err = srv.last_error()
+    ok = [r for r in res if r["status"] == 0]
+    lat = np.array([r["t_end"] - r["t_submit"] for r in ok])
+    span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
+    its = sum(r["loops"] for r in ok)
+    return dict(jobs=len(jobs), ok=len(ok), failed=len(res) - len(ok), error=err if len(ok) < len(res) else "",
+                p50_s=float(np.percentile(lat, 50)) if len(lat) else None,
+                p99_s=float(np.percentile(lat, 99)) if len(lat) else None,
+                oc_its=its, span_s=span, oc_its_per_s=its / span if span > 0 else None,
+                max_running=stats["max_running"], peak_bytes=stats["peak_bytes"])
+
+
+def run_sequential(jobs, precision, device):
+    """The same jobs one after another (one slot): busy time per job and OC iterations/s."""
+    from top3d_xl_b200 import Server
+    with Server(slots=1, precision=precision, device=device) as srv:
+        res = [srv.wait(srv.submit(j["shape"], j["cons"], j["V0"], j["nLoop"], math.sqrt(3), j["rHat"])) for j in jobs]
+    busy = sum(r["t_end"] - r["t_submit"] for r in res)
+    its = sum(r["loops"] for r in res if r["status"] == 0)
+    return dict(jobs=len(jobs), oc_its=its, busy_s=busy, oc_its_per_s=its / busy if busy > 0 else None)
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -234,6 +288,13 @@ def main(argv=None):
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--workload", default="cuboid128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--serve", action="store_true",
+                    help="run only the served stream (continuous batching) and print its line")
+    ap.add_argument("--serve-jobs", type=int, default=256)
+    ap.add_argument("--serve-precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-seq-jobs", type=int, default=32,
+                    help="jobs of the stream also run one at a time in FP64 for the baseline")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one precision arm only (profiling); prints its timing and exits")
     a = ap.parse_args(argv)
@@ -264,6 +325,28 @@ def main(argv=None):
         return 0
 
     device = local
+    if a.serve:
+        if rank != 0:
+            return 0
+        jobs = serve_stream(a.serve_jobs)
+        with Clocks(device) as clk:
+            served = run_served(jobs, a.serve_precision, a.serve_slots, device)
+        seq = run_sequential(jobs[:a.serve_seq_jobs], "fp64", device)
+        seq_mixed_slots = run_served(jobs[:a.serve_seq_jobs], a.serve_precision, a.serve_slots, device)
+        line = {"metric": "served design latency p50/p99 and OC iterations/s (continuous batching)",
+                "value": served["oc_its_per_s"], "unit": "OC iterations/s", "n_gpus": 1,
+                "higher_is_better": True, "dtype": "f64 Krylov/operator, f32 preconditioner (mixed)",
+                "data": "synthetic served stream (seeded Poisson arrivals, solid cuboids, built-in BCs)",
+                "config": {"workload": "%d jobs, mean gap 50 ms, dims (16,32,16)*s, s log-uniform [1,6], "
+                                       "70%% GLOBAL 50 its / 30%% LOCAL 100 its" % a.serve_jobs,
+                           "slots": a.serve_slots},
+                "p50_latency_s": served["p50_s"], "p99_latency_s": served["p99_s"], "served": served,
+                "sequential_fp64": seq, "same_jobs_served": seq_mixed_slots,
+                "served_vs_sequential_fp64": (seq_mixed_slots["oc_its_per_s"] / seq["oc_its_per_s"])
+                if seq["oc_its_per_s"] and seq_mixed_slots["oc_its_per_s"] else None,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+        return 0
     if a.only:
         r = run_native(wl, a.only, a.steps, a.warmup, device, profile_steps=1)
         print(json.dumps({"only": a.only, "ms_per_step": r["ms"] / max(1, a.steps),

@@ -61,6 +61,8 @@ typedef struct topx_params {
   int64_t coarsestResolutionControl; /* 50000 */
   int precision;           /* TOPX_FP64 or TOPX_MIXED */
   int device;              /* CUDA device ordinal */
+  int coarse_coop;         /* 1: coarsest solve as one cooperative launch when available (default);
+                              0: one launch per chain step (for engines sharing the GPU) */
 } topx_params;
 
 /* sizes of the loaded model */
@@ -187,6 +189,61 @@ topx_status topx_set_profiling(topx_ctx* ctx, int on);
 topx_status topx_get_profile(topx_ctx* ctx, topx_profile* out);
 /* kernels this library has launched in this process so far (graph replays count their kernels) */
 int64_t topx_launch_count(void);
+
+/* ---- serving: continuous batching of design jobs (no reference counterpart) -------
+   A server runs design jobs (each one TOP3D_XL call) on one GPU for many clients.  Up to
+   `slots` jobs are on the device at once, each with its own engine and stream, so their work
+   overlaps.  A queued job is admitted as soon as a slot is free and its device-memory
+   footprint fits the HBM budget; jobs are taken in arrival order, skipping one that does not
+   fit yet.  The result of a job does not depend on what runs beside it. */
+typedef struct topx_server topx_server;
+typedef struct topx_server_params {
+  int slots;                /* jobs on the device at once (worker threads), default 6 */
+  double hbm_budget_bytes;  /* device memory admitted jobs may hold; <= 0: 85% of free memory */
+  int precision;            /* TOPX_FP64 or TOPX_MIXED */
+  int device;               /* CUDA device ordinal */
+} topx_server_params;
+typedef struct topx_job {
+  int nely, nelx, nelz;     /* voxel grid; with voxels == NULL a solid cuboid (built-in BCs) */
+  const uint8_t* voxels;    /* optional column-major nely x nelx x nelz mask, copied at submit */
+  int consType;             /* TOPX_GLOBAL or TOPX_LOCAL */
+  double V0;
+  int nLoop;
+  double rMin, rHat;
+  int keep_density;         /* 1: keep the final density for topx_server_get_density */
+} topx_job;
+typedef struct topx_job_result {
+  int status;               /* TOPX_OK, or the status the job failed with */
+  int loops;                /* optimisation iterations run */
+  double cSolid;            /* compliance of the fully solid domain */
+  double c_last;            /* compliance of the last iteration */
+  int64_t pcg_its;          /* elasticity PCG iterations over the whole job */
+  int64_t numElements;
+  int64_t footprint_estimate; /* bytes used for admission */
+  int64_t footprint_bytes;    /* device bytes its engine held */
+  double t_submit, t_admit, t_end; /* seconds on the server's clock */
+} topx_job_result;
+typedef struct topx_server_stats {
+  int64_t submitted, done, failed, running, queued;
+  int max_running;          /* most jobs on the device at once so far */
+  double budget_bytes, peak_bytes; /* admission budget and peak admitted footprint */
+} topx_server_stats;
+topx_status topx_server_default_params(topx_server_params* p);
+topx_status topx_server_create(topx_server** srv, const topx_server_params* p);
+/* waits for the running jobs; queued jobs end with TOPX_ERR_STATE */
+topx_status topx_server_destroy(topx_server* srv);
+/* enqueue a job; never blocks on the device */
+topx_status topx_server_submit(topx_server* srv, const topx_job* job, int64_t* job_id);
+/* TOPX_OK and the result once the job has ended, TOPX_STOP while it is queued or running */
+topx_status topx_server_poll(topx_server* srv, int64_t job_id, topx_job_result* out);
+/* blocks until the job has ended */
+topx_status topx_server_wait(topx_server* srv, int64_t job_id, topx_job_result* out);
+/* per-iteration history of an ended job (n entries at most) */
+topx_status topx_server_get_history(topx_server* srv, int64_t job_id, topx_iter* hist, int n, int* loops);
+/* final density (numElements) of an ended job submitted with keep_density */
+topx_status topx_server_get_density(topx_server* srv, int64_t job_id, double* out, size_t n);
+topx_status topx_server_get_stats(topx_server* srv, topx_server_stats* out);
+const char* topx_server_last_error(topx_server* srv);
 
 #ifdef __cplusplus
 }

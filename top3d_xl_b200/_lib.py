@@ -24,7 +24,8 @@ class Params(C.Structure):
     _fields_ = [("modulus", C.c_double), ("poissonRatio", C.c_double), ("modulusMin", C.c_double),
                 ("SIMPpenalty", C.c_double), ("cellSize", C.c_double), ("tol", C.c_double),
                 ("maxIT", C.c_int), ("weightFactorJacobi", C.c_double),
-                ("coarsestResolutionControl", C.c_int64), ("precision", C.c_int), ("device", C.c_int)]
+                ("coarsestResolutionControl", C.c_int64), ("precision", C.c_int), ("device", C.c_int),
+                ("coarse_coop", C.c_int)]
 
 
 class Info(C.Structure):
@@ -48,6 +49,29 @@ NSECTIONS = 14
 class Profile(C.Structure):
     _fields_ = [("ku_ms", C.c_double), ("ku_launches", C.c_int64), ("pcg_iterations", C.c_int64),
                 ("section_ms", C.c_double * NSECTIONS), ("section_count", C.c_int64 * NSECTIONS)]
+
+
+class ServerParams(C.Structure):
+    _fields_ = [("slots", C.c_int), ("hbm_budget_bytes", C.c_double), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class Job(C.Structure):
+    _fields_ = [("nely", C.c_int), ("nelx", C.c_int), ("nelz", C.c_int), ("voxels", C.POINTER(C.c_uint8)),
+                ("consType", C.c_int), ("V0", C.c_double), ("nLoop", C.c_int), ("rMin", C.c_double),
+                ("rHat", C.c_double), ("keep_density", C.c_int)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("loops", C.c_int), ("cSolid", C.c_double), ("c_last", C.c_double),
+                ("pcg_its", C.c_int64), ("numElements", C.c_int64), ("footprint_estimate", C.c_int64),
+                ("footprint_bytes", C.c_int64), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_end", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("done", C.c_int64), ("failed", C.c_int64), ("running", C.c_int64),
+                ("queued", C.c_int64), ("max_running", C.c_int), ("budget_bytes", C.c_double),
+                ("peak_bytes", C.c_double)]
 
 
 # exported symbols and their argument types (checked by tests/test_abi.py)
@@ -90,6 +114,16 @@ SIGNATURES = {
     "topx_get_profile": [_P, C.POINTER(Profile)],
     "topx_profile_section_name": [C.c_int],
     "topx_launch_count": [],
+    "topx_server_default_params": [C.POINTER(ServerParams)],
+    "topx_server_create": [C.POINTER(_P), C.POINTER(ServerParams)],
+    "topx_server_destroy": [_P],
+    "topx_server_submit": [_P, C.POINTER(Job), C.POINTER(C.c_int64)],
+    "topx_server_poll": [_P, C.c_int64, C.POINTER(JobResult)],
+    "topx_server_wait": [_P, C.c_int64, C.POINTER(JobResult)],
+    "topx_server_get_history": [_P, C.c_int64, C.POINTER(Iter), C.c_int, C.POINTER(C.c_int)],
+    "topx_server_get_density": [_P, C.c_int64, _D, _SZ],
+    "topx_server_get_stats": [_P, C.POINTER(ServerStats)],
+    "topx_server_last_error": [_P],
 }
 
 _lib = None
@@ -106,7 +140,8 @@ def load(path: str = LIB_PATH):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version", "topx_profile_section_name") \
+        fn.restype = C.c_char_p if name in ("topx_last_error", "topx_version", "topx_profile_section_name",
+                                            "topx_server_last_error") \
             else C.c_int64 if name == "topx_launch_count" else C.c_int
     _lib = lib
     return lib

@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libtopx.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["topx_fem.cu", "topx_coarse.cu", "topx_opt.cu", "topx_engine.cu", "topx_noalloc.cu"]
-CXX_SOURCES = ["topx_mesh.cpp", "topx_api.cpp"]
+CXX_SOURCES = ["topx_mesh.cpp", "topx_api.cpp", "topx_server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -47,12 +47,12 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
             cmd += ["--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
-        elif src == "topx_api.cpp":
+        elif src in ("topx_api.cpp", "topx_server.cpp"):
             cmd += ["-x", "cu"]  # includes the engine's device headers
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    cmd = [NVCC, "-shared", *ARCH, "-o", LIB, *objs, "-lcudart"]
+    cmd = [NVCC, "-shared", *ARCH, "-o", LIB, *objs, "-lcudart", "-lpthread"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -80,7 +80,7 @@ topx_status need_engine(topx_ctx* c) {
   if (prop.major != 10)
     return fail(c, TOPX_ERR_CUDA, "libtopx is built for sm_100a (B200); device is sm_" +
                                       std::to_string(prop.major) + std::to_string(prop.minor));
-  c->engine.reset(new topx::Engine(*c->model, c->params.precision, c->params.device));
+  c->engine.reset(new topx::Engine(*c->model, c->params.precision, c->params.device, c->params.coarse_coop != 0));
   return TOPX_OK;
 }
 
@@ -147,6 +147,7 @@ topx_status topx_default_params(topx_params* p) {
   p->coarsestResolutionControl = S.coarsestResolutionControl;
   p->precision = TOPX_FP64;
   p->device = 0;
+  p->coarse_coop = 1;
   return TOPX_OK;
 }
 

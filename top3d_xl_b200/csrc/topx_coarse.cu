@@ -10,6 +10,7 @@
 // Cholesky with fill-reducing permutation (chol(K,'lower') with P,
 // TOP3D_XL.m:1065): same exact solve, different rounding.
 #include <algorithm>
+#include <mutex>
 
 #include "topx_kernels.cuh"
 
@@ -714,8 +715,17 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJS
 constexpr int GJ_REST_CTAS = 96;
 constexpr size_t GJ_REST_SMEM = 200 * 1024;
 
+// once per device and process: engines on several host threads share the attributes
 void prepare_coarse_kernels() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  TOPX_CUDA_OK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return;
+
   TOPX_CUDA_OK(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(GJ_REST_SMEM)));
+  if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
 // Exchange steps with one step of lookahead: after the panel of step k, the tiles that step

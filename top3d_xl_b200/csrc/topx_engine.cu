@@ -15,11 +15,13 @@ namespace topx {
 
 static int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
-Engine::Engine(Model& model, int precision, int device) : M(model), prec(precision) {
+Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(model), prec(precision) {
   TOPX_CUDA_OK(cudaSetDevice(device));
-  // blocking stream: ordered with the synchronous cudaMemset/cudaMemcpy calls of the set-up code
-  TOPX_CUDA_OK(cudaStreamCreate(&st));
-  TOPX_CUDA_OK(cudaStreamCreate(&gjs.side));
+  // non-blocking streams: no implicit ordering with the legacy default stream, so engines on
+  // other host threads (and their synchronous set-up copies) never stall or break this one's
+  // graph captures; every host-side copy below waits for this stream first
+  TOPX_CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  TOPX_CUDA_OK(cudaStreamCreateWithFlags(&gjs.side, cudaStreamNonBlocking));
   for (cudaEvent_t* e : {&gjs.panel[0], &gjs.panel[1], &gjs.rest[0], &gjs.rest[1]})
     TOPX_CUDA_OK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   prepare_coarse_kernels();
@@ -213,7 +215,7 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
     gjP.alloc(4 * (64 * 64 + size_t(128) * si.m));
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
-    coopCtas = slab_solve_coop_ctas(si.m);
+    coopCtas = coarse_coop ? slab_solve_coop_ctas(si.m) : 0;
   }
   // ---- workspaces ------------------------------------------------------------
   {
@@ -280,6 +282,9 @@ Engine::Engine(Model& model, int precision, int device) : M(model), prec(precisi
 }
 
 Engine::~Engine() {
+  // no work of this engine may still be in flight when its buffers and graphs go
+  if (st) cudaStreamSynchronize(st);
+  if (gjs.side) cudaStreamSynchronize(gjs.side);
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
   for (auto e : ev) cudaEventDestroy(e);
   for (auto e : sev) cudaEventDestroy(e);
@@ -335,10 +340,9 @@ void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
 }
 
 void Engine::check_coop_barrier() {
-  if (!coopCtas) return;
-  TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  if (h_bar->err) {
+  if (coopCtas && h_bar->err) {
     TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
     throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
   }
@@ -348,6 +352,7 @@ void Engine::check_coop_barrier() {
 // design state
 // ---------------------------------------------------------------------------
 void Engine::set_xphys(const double* h) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   TOPX_CUDA_OK(cudaMemcpy(xPhys.p, h, sizeof(double) * Ne, cudaMemcpyHostToDevice));
 }
 void Engine::get_xphys(double* h) const {
@@ -355,6 +360,7 @@ void Engine::get_xphys(double* h) const {
   TOPX_CUDA_OK(cudaMemcpy(h, xPhys.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
 }
 void Engine::get_U(int lc, double* h) const {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   DevBuf<double> tmp;
   tmp.alloc(size_t(Nn) * 3);
   launch_grid_to_compact_nodes<double>(st, U[lc].p, tmp.p, G[0], nodMapBack0.p, Nn);
@@ -362,6 +368,7 @@ void Engine::get_U(int lc, double* h) const {
   TOPX_CUDA_OK(cudaMemcpy(h, tmp.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
 }
 void Engine::set_U(int lc, const double* h) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   DevBuf<double> tmp;
   tmp.upload(h, size_t(Nn) * 3);
   TOPX_CUDA_OK(cudaMemsetAsync(U[lc].p, 0, U[lc].bytes(), st));
@@ -542,12 +549,22 @@ void Engine::compliance(double* d_ce) {
 // ---------------------------------------------------------------------------
 void Engine::setup_filter(int slot, double rmin) {
   const std::array<double, 64> KF = pde_filter_kernel(rmin, M.S.cellSize * 1.0);
-  upload_filter_kernel(KF.data(), slot);
+  filterKe64[slot] = filter_ke<double>(KF.data());
+  filterKe32[slot] = filter_ke<float>(KF.data());
   filterR[slot] = rmin;
   if (prec == PREC_FP64)
-    launch_filter_diag<double>(st, G[0], solid1.p, slot, f64.fdp[slot].p);
+    launch_filter_diag<double>(st, G[0], solid1.p, filterKe64[slot], f64.fdp[slot].p);
   else
-    launch_filter_diag<float>(st, G[0], solid1.p, slot, f32.fdp[slot].p);
+    launch_filter_diag<float>(st, G[0], solid1.p, filterKe64[slot], f32.fdp[slot].p);
+}
+
+template <>
+const FilterKe<double>& Engine::filter_ke_of<double>(int slot) const {
+  return filterKe64[slot];
+}
+template <>
+const FilterKe<float>& Engine::filter_ke_of<float>(int slot) const {
+  return filterKe32[slot];
 }
 
 template <typename T>
@@ -561,12 +578,15 @@ int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) 
   const int CH = 8;
   PcgScalars h{};
   int launched = 0;
-  const std::string key = "filter_chunk:" + std::to_string(slot);
+  // the filter matrix is captured by value: the graph key carries the radius it was built for
+  char key[64];
+  std::snprintf(key, sizeof(key), "filter_chunk:%d:%.17g", slot, filterR[slot]);
+  const FilterKe<T>& kf = filter_ke_of<T>(slot);
   while (launched < M.S.maxIT) {
     const int n = std::min(CH, M.S.maxIT - launched);
     auto body = [&]() {
       for (int c = 0; c < n; ++c) {
-        launch_filter_ku<T>(st, KU_P_UPDATE, g, slot, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
+        launch_filter_ku<T>(st, KU_P_UPDATE, g, kf, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
         launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1);
       }
     };
@@ -591,6 +611,7 @@ int Engine::filter(int slot, const double* d_src, double* d_out) {
 // test entry points
 // ---------------------------------------------------------------------------
 void Engine::apply_K(const double* h_u, double* h_y) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   DevBuf<double> cu, du, dy;
   cu.upload(h_u, size_t(Nn) * 3);
   du.alloc(size_t(G[0].stride) * 3);
@@ -603,6 +624,7 @@ void Engine::apply_K(const double* h_u, double* h_y) {
 }
 
 void Engine::apply_vcycle(const double* h_r, double* h_z) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   DevBuf<double> cu;
   cu.upload(h_r, size_t(Nn) * 3);
   PcgScalars z{};
@@ -699,6 +721,7 @@ void Engine::sec_harvest() {
 }
 
 void Engine::set_moduli_host(const double* h_E) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_E, sizeof(double) * Ne, cudaMemcpyHostToDevice));
   launch_scatter_elems_t<double>(st, tmpA.p, eleMapBack0.p, Ne, E64.p);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
@@ -713,6 +736,7 @@ int Engine::pcg_host(int lc, double* h_u) {
 
 int Engine::filter_host(double rmin, const double* h_src, double* h_out) {
   setup_filter(0, rmin);
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_src, sizeof(double) * Ne, cudaMemcpyHostToDevice));
   const int its = filter(0, tmpA.p, tmpB.p);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
@@ -752,6 +776,7 @@ void Engine::get_diag(int level, double* h_d) const {
 // optimisation loop
 // ---------------------------------------------------------------------------
 void Engine::begin(int consType, double V0, int nLoop, double rMin, double rHat) {
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
   consType_ = consType;
   V0_ = V0;
   nLoop_ = nLoop;

@@ -19,6 +19,13 @@
 
 namespace topx {
 
+// Device bytes held by the DevBufs this thread allocated (a job's footprint, measured by the
+// thread that builds its engine).
+inline int64_t& devbuf_bytes() {
+  thread_local int64_t b = 0;
+  return b;
+}
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -43,9 +50,10 @@ struct DevBuf {
   ~DevBuf() { release(); }
   void alloc(size_t count, bool zero = true) {
     release();
-    n = count;
     if (count) {
       TOPX_CUDA_OK(cudaMalloc(&p, sizeof(T) * count));
+      n = count;
+      devbuf_bytes() += int64_t(sizeof(T) * count);
       if (zero) TOPX_CUDA_OK(cudaMemset(p, 0, sizeof(T) * count));
     }
   }
@@ -54,7 +62,10 @@ struct DevBuf {
     if (count) TOPX_CUDA_OK(cudaMemcpy(p, h, sizeof(T) * count, cudaMemcpyHostToDevice));
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      devbuf_bytes() -= int64_t(sizeof(T) * n);
+    }
     p = nullptr;
     n = 0;
   }
@@ -95,7 +106,7 @@ struct FWork {
 
 class Engine {
  public:
-  Engine(Model& model, int precision, int device);
+  Engine(Model& model, int precision, int device, bool coarse_coop = true);
   ~Engine();
 
   // ---- design state -----------------------------------------------------
@@ -167,6 +178,8 @@ class Engine {
   int pcg(const double* b, double* y, bool warm, double tol, int maxIT);
   template <typename TF>
   int filter_t(FWork<TF>& f, int slot, const double* d_src, double* d_out);
+  template <typename TF>
+  const FilterKe<TF>& filter_ke_of(int slot) const;
   void step_local(IterRecord& rec, const ObjState& os);
   void factor_coarsest();
   void assemble_launches();
@@ -190,7 +203,7 @@ class Engine {
   DevBuf<double> slabBS, slabW, slabV, slabXS;  // slab-ordered vectors of one coarse solve
   DevBuf<CoopBarrier> coopBar;  // barrier of the cooperative coarse solve
   int coopCtas = 0;             // its CTA count; 0: multi-launch coarse solve
-  void check_coop_barrier();    // throws after a barrier wait gave up (and re-arms the barrier)
+  void check_coop_barrier();    // waits for the stream; throws if a barrier wait gave up (re-arming it)
   // workspaces
   KrylovWork kw;
   VWork<double> v64;
@@ -213,6 +226,8 @@ class Engine {
   DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;
   DevBuf<uint8_t> passive;
   std::array<double, 2> filterR{{0, 0}};
+  std::array<FilterKe<double>, 2> filterKe64{};  // filter element matrix per slot
+  std::array<FilterKe<float>, 2> filterKe32{};
   // run state
   int consType_ = 0, nLoop_ = 0, loop_ = 0, loopbeta_ = 0;
   int64_t nActive_ = 0;

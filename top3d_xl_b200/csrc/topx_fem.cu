@@ -2,6 +2,7 @@
 // Jacobi diagonal, PCG vector algebra, trilinear multigrid transfers, SIMP,
 // unit compliance.  FP64 (plain path) and FP32 (mixed path) instantiations.
 #include <cmath>
+#include <mutex>
 #include <stdexcept>
 #include <type_traits>
 
@@ -322,11 +323,18 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
 }
 
 static int g_num_sms = 148;
+// once per device and process: engines on several host threads share the attributes
 void prepare_fem_kernels() {
-  int dev = 0, n = 0;
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
   TOPX_CUDA_OK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return;
+  int n = 0;
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
   if (n > 0) g_num_sms = n;
+  if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
 // z-chunk length of the K*u launch: fewest (waves x halo-inclusive planes) for three CTAs per SM

@@ -35,7 +35,6 @@ enum KuMode { KU_PLAIN = 0, KU_P_UPDATE = 2 };
 
 // element matrices in constant memory
 void upload_ke(const double* Ke576);
-void upload_filter_kernel(const double* KF64, int slot);
 
 // --- level-1 elasticity --------------------------------------------------
 template <typename T>

@@ -15,26 +15,16 @@ static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
   return unsigned(b);
 }
 
-__constant__ double c_KF64[2][64];
-__constant__ float c_KF32[2][64];
-
+// The filter kernel matrix travels as a launch parameter (no process-wide constant memory),
+// so engines with different filter radii can run side by side.
 template <typename T>
-__device__ __forceinline__ T kf(int slot, int i);
-template <>
-__device__ __forceinline__ double kf<double>(int slot, int i) {
-  return c_KF64[slot][i];
+FilterKe<T> filter_ke(const double* KF64) {
+  FilterKe<T> k;
+  for (int i = 0; i < 64; ++i) k.v[i] = T(KF64[i]);
+  return k;
 }
-template <>
-__device__ __forceinline__ float kf<float>(int slot, int i) {
-  return c_KF32[slot][i];
-}
-
-void upload_filter_kernel(const double* KF64, int slot) {
-  float f[64];
-  for (int i = 0; i < 64; ++i) f[i] = float(KF64[i]);
-  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_KF64, KF64, sizeof(double) * 64, sizeof(double) * 64 * slot));
-  TOPX_CUDA_OK(cudaMemcpyToSymbol(c_KF32, f, sizeof(float) * 64, sizeof(float) * 64 * slot));
-}
+template FilterKe<double> filter_ke<double>(const double*);
+template FilterKe<float> filter_ke<float>(const double*);
 
 // element -> node: node = sum over its hexes (local-node order) of src_e*(1/8)  (TOP3D_XL.m:880-886)
 template <typename T>
@@ -61,7 +51,7 @@ void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node) {
 
 // Jacobi preconditioner 1/diag (TOP3D_XL.m:855-867); 0 on absent nodes
 template <typename T>
-__global__ void k_filter_diag(Grid g, const uint8_t* __restrict__ solid, int slot, T* __restrict__ dp) {
+__global__ void k_filter_diag(Grid g, const uint8_t* __restrict__ solid, const FilterKe<double> kf, T* __restrict__ dp) {
   const int64_t N = g.nnodes();
   const int nny = g.ny + 1, nnx = g.nx + 1;
   for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
@@ -70,14 +60,14 @@ __global__ void k_filter_diag(Grid g, const uint8_t* __restrict__ solid, int slo
     for (int a = 0; a < 8; ++a) {
       const int ey = gy - hex_ly(a), ex = gx - hex_lx(a), ez = gz - hex_lz(a);
       if (ey < 0 || ey >= g.ny || ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
-      if (solid[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)]) s += c_KF64[slot][a * 9];
+      if (solid[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)]) s += kf.v[a * 9];
     }
     dp[n] = s > 0.0 ? T(1.0 / s) : T(0);
   }
 }
 template <typename T>
-void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, int slot, T* dp) {
-  (k_filter_diag<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, solid, slot, dp), topx::count_launch());
+void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, const FilterKe<double>& kf, T* dp) {
+  (k_filter_diag<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, solid, kf, dp), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -86,7 +76,7 @@ void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, int slot,
 constexpr int FTY = 32, FTX = 4, FTZ = 2, FNT = FTY * FTX * FTZ;
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int slot, const T* __restrict__ in,
+__global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, const FilterKe<T> kf, const T* __restrict__ in,
                                                     const T* __restrict__ zin, T* __restrict__ out,
                                                     const uint8_t* __restrict__ solid, PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
@@ -139,7 +129,7 @@ __global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int slot, const T* __
             const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
             if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
             const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
-            acc[e] = fma(kf<T>(slot, a * 8 + b), u, acc[e]);
+            acc[e] = fma(kf.v[a * 8 + b], u, acc[e]);
           }
         }
     T y = T(0);
@@ -160,15 +150,15 @@ __global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int slot, const T* __
 }
 
 template <typename T>
-void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, int slot, const T* in, const T* z, T* pout, T* out,
+void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& kf, const T* in, const T* z, T* pout, T* out,
                       const uint8_t* solid, PcgScalars* sc, RedScratch rs) {
   (void)pout;
   dim3 blk(FTY, FTX, FTZ);
   dim3 grd((g.nny() + FTY - 1) / FTY, (g.nnx() + FTX - 1) / FTX, (g.nnz() + FTZ - 1) / FTZ);
   if (mode == KU_PLAIN)
-    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, kf, in, z, out, solid, sc, rs), topx::count_launch());
   else
-    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, slot, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, kf, in, z, out, solid, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -415,11 +405,11 @@ void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* dc, c
 
 template void launch_filter_e2n<double>(cudaStream_t, Grid, const double*, double*);
 template void launch_filter_e2n<float>(cudaStream_t, Grid, const float*, float*);
-template void launch_filter_diag<double>(cudaStream_t, Grid, const uint8_t*, int, double*);
-template void launch_filter_diag<float>(cudaStream_t, Grid, const uint8_t*, int, float*);
-template void launch_filter_ku<double>(cudaStream_t, KuMode, Grid, int, const double*, const double*, double*, double*,
+template void launch_filter_diag<double>(cudaStream_t, Grid, const uint8_t*, const FilterKe<double>&, double*);
+template void launch_filter_diag<float>(cudaStream_t, Grid, const uint8_t*, const FilterKe<double>&, float*);
+template void launch_filter_ku<double>(cudaStream_t, KuMode, Grid, const FilterKe<double>&, const double*, const double*, double*, double*,
                                        const uint8_t*, PcgScalars*, RedScratch);
-template void launch_filter_ku<float>(cudaStream_t, KuMode, Grid, int, const float*, const float*, float*, float*,
+template void launch_filter_ku<float>(cudaStream_t, KuMode, Grid, const FilterKe<float>&, const float*, const float*, float*, float*,
                                       const uint8_t*, PcgScalars*, RedScratch);
 template void launch_filter_residual_init<double>(cudaStream_t, Grid, const double*, const double*, double*, double*,
                                                   double*, PcgScalars*, RedScratch, double, int);

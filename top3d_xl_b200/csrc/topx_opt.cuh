@@ -20,13 +20,20 @@ struct OcState {
 enum EwOp { EW_COPY = 0, EW_MUL = 1, EW_DIV_MAXX = 2 };
 
 // --- PDE filter ------------------------------------------------------------
+// 8x8 element matrix of the Helmholtz filter (TOP3D_XL.m:845-853), passed by value to kernels
+template <typename T>
+struct FilterKe {
+  T v[64];
+};
+template <typename T>
+FilterKe<T> filter_ke(const double* KF64);
 template <typename T>
 void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node);
 template <typename T>
-void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, int slot, T* dp);
+void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, const FilterKe<double>& kf, T* dp);
 template <typename T>
-void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, int slot, const T* in, const T* z, T* pout, T* out,
-                      const uint8_t* solid, PcgScalars* sc, RedScratch rs);
+void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& kf, const T* in, const T* z, T* pout,
+                      T* out, const uint8_t* solid, PcgScalars* sc, RedScratch rs);
 template <typename T>
 void launch_filter_residual_init(cudaStream_t st, Grid g, const T* b, const T* dp, T* r, T* z, T* y, PcgScalars* sc,
                                  RedScratch rs, double tol, int maxIT);

@@ -306,3 +306,99 @@ def TOP3D_XL(inputModel, consType, V0, nLoop, rMin, *varargin, precision="fp64",
     finally:
         ctx.close()
         log.close()
+
+
+class Server:
+    """Continuous-batching job server (topx_server_* in include/topx.h).
+
+    Jobs are solid cuboids (or voxel masks) run through the same optimisation loop as
+    ``TOP3D_XL``; up to ``slots`` of them are on the GPU at once, admitted by device-memory
+    footprint against ``hbm_budget_bytes``.
+    """
+
+    def __init__(self, slots=6, precision="fp64", hbm_budget_bytes=0.0, device=0):
+        self.lib = L.load()
+        p = L.ServerParams()
+        self.lib.topx_server_default_params(C.byref(p))
+        p.slots = int(slots)
+        p.precision = {"fp64": 0, "mixed": 1}[precision]
+        p.hbm_budget_bytes = float(hbm_budget_bytes)
+        p.device = int(device)
+        self._h = C.c_void_p()
+        st = self.lib.topx_server_create(C.byref(self._h), C.byref(p))
+        if st != 0:
+            raise TopxError(st, "topx_server_create failed")
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            self.lib.topx_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, shape=None, consType="GLOBAL", V0=0.12, nLoop=50, rMin=np.sqrt(3), rHat=0.0, voxels=None,
+               keep_density=False):
+        """Enqueue one job; returns its id at once."""
+        j = L.Job()
+        if voxels is not None:
+            v = np.asfortranarray(np.asarray(voxels, dtype=np.uint8))
+            j.nely, j.nelx, j.nelz = v.shape
+            buf = np.ascontiguousarray(v.ravel(order="F"))
+            j.voxels = buf.ctypes.data_as(C.POINTER(C.c_uint8))
+        else:
+            j.nely, j.nelx, j.nelz = shape
+            j.voxels = None
+        j.consType = {"GLOBAL": 0, "LOCAL": 1}.get(consType, -1)  # the C side rejects anything else
+        j.V0, j.nLoop, j.rMin, j.rHat = float(V0), int(nLoop), float(rMin), float(rHat)
+        j.keep_density = 1 if keep_density else 0
+        jid = C.c_int64()
+        st = self.lib.topx_server_submit(self._h, C.byref(j), C.byref(jid))
+        if st != 0:
+            raise TopxError(st, "topx_server_submit failed")
+        return int(jid.value)
+
+    @staticmethod
+    def _res(r):
+        return {k: getattr(r, k) for k, _ in L.JobResult._fields_}
+
+    def poll(self, jid):
+        r = L.JobResult()
+        st = self.lib.topx_server_poll(self._h, jid, C.byref(r))
+        return None if st == 1 else self._res(r)
+
+    def wait(self, jid):
+        r = L.JobResult()
+        st = self.lib.topx_server_wait(self._h, jid, C.byref(r))
+        if st != 0:
+            raise TopxError(st, "topx_server_wait failed")
+        return self._res(r)
+
+    def history(self, jid):
+        n = C.c_int()
+        self.lib.topx_server_get_history(self._h, jid, None, 0, C.byref(n))
+        arr = (L.Iter * max(1, n.value))()
+        st = self.lib.topx_server_get_history(self._h, jid, arr, n.value, C.byref(n))
+        if st != 0:
+            raise TopxError(st, "topx_server_get_history failed")
+        return [dict(loop=it.loop, c=it.c, vol=it.vol, sharp=it.sharp, cons=it.cons, change=it.change,
+                     its=it.its[0]) for it in arr[:n.value]]
+
+    def density(self, jid, numElements):
+        out = np.empty(int(numElements))
+        st = self.lib.topx_server_get_density(self._h, jid, _dptr(out), out.size)
+        if st != 0:
+            raise TopxError(st, "topx_server_get_density failed")
+        return out
+
+    def stats(self):
+        s = L.ServerStats()
+        self.lib.topx_server_get_stats(self._h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in L.ServerStats._fields_}
+
+    def last_error(self):
+        return self.lib.topx_server_last_error(self._h).decode()
