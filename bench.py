@@ -37,8 +37,35 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "cuboid128": dict(shape=(128, 256, 128), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
     "cuboid50": dict(shape=(50, 100, 50), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
+    "cuboid50_local": dict(shape=(50, 100, 50), cons="LOCAL", V0=0.5, rMin=math.sqrt(3), rHat=6.0, nLoop=300),
     "cuboid25": dict(shape=(25, 50, 25), cons="GLOBAL", V0=0.12, rMin=math.sqrt(3), rHat=0.0, nLoop=50),
+    # generated irregular domain (top3d_xl_b200/workloads.py, seed 8) read from a .TopVoxel file
+    "irregular4": dict(topvoxel="IRREGULAR_FULL", cons="LOCAL", V0=0.5, rMin=math.sqrt(3), rHat=6.0, nLoop=300),
 }
+_TOPVOXEL = {}
+
+
+def workload_source(wl):
+    """A voxel array (cuboids) or the path of the generated .TopVoxel file (written once)."""
+    if "topvoxel" not in wl:
+        return np.ones(wl["shape"], bool)
+    key = wl["topvoxel"]
+    if key not in _TOPVOXEL:
+        import tempfile
+
+        from top3d_xl_b200 import workloads as W
+        path = os.path.join(tempfile.mkdtemp(prefix="topx_"), key + ".TopVoxel")
+        W.write_topvoxel(path, *W.irregular_domain(**getattr(W, key)))
+        _TOPVOXEL[key] = path
+    return _TOPVOXEL[key]
+
+
+def load_workload(ctx, wl):
+    src = workload_source(wl)
+    if isinstance(src, str):
+        ctx.load_topvoxel(src)
+    else:
+        ctx.load_voxels(src)
 METRIC = "OC iterations/s (GLOBAL, FP64; mixed precision beside it)"
 # DRAM bytes (read + write) per grid node of one K*u launch in PCG mode, from an ncu capture of
 # the 128x256x128 cuboid (dram__bytes_read.sum + dram__bytes_write.sum = 259.68 MB + 86.09 MB
@@ -117,8 +144,7 @@ def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False
     event timing (direct launches instead of CUDA graphs, outside the timed region)."""
     from top3d_xl_b200 import Context
     ctx = Context(precision, device=device)
-    vox = np.ones(wl["shape"], bool)
-    ctx.load_voxels(vox)
+    load_workload(ctx, wl)
     ctx.begin(wl["cons"], wl["V0"], wl["nLoop"], wl["rMin"], wl["rHat"])
     hist = []
     for _ in range(warmup):
@@ -154,7 +180,7 @@ def run_e2e(wl, precision, steps, warmup, device):
     goes to the device, one iteration runs, and the new density comes back."""
     from top3d_xl_b200 import Context
     ctx = Context(precision, device=device)
-    ctx.load_voxels(np.ones(wl["shape"], bool))
+    load_workload(ctx, wl)
     ctx.begin(wl["cons"], wl["V0"], wl["nLoop"], wl["rMin"], wl["rHat"])
     x = ctx.density()
     for _ in range(warmup):
@@ -178,8 +204,7 @@ def cpu_sample(wl, its_per_oc, filter_its_per_oc, budget_s=30.0):
     import threadpoolctl  # noqa: F401
     from oracle import top3dxl_oracle as O
     cores = os.cpu_count() or 1
-    vox = np.ones(wl["shape"], bool)
-    m = O.build_model(vox)
+    m = O.build_model(workload_source(wl))
     sol = O.Solver(m)
     Ne = m.levels[0].numElements
     S = m.S
@@ -203,10 +228,11 @@ def cpu_sample(wl, its_per_oc, filter_its_per_oc, budget_s=30.0):
     O.unit_compliance(m, U)
     t_ce = time.perf_counter() - t
     t_oc = t_asm + its_per_oc * t_it + filter_its_per_oc * t_fit + t_ce
-    sample = ("oracle FP64 on the same %dx%dx%d cuboid: 1 stencil assembly (%.1fs), 1 PCG iteration "
-              "(K*u + V-cycle, %.2fs), 1 filter matvec (%.2fs), 1 compliance (%.2fs); OC iteration = "
-              "assembly + %.1f PCG its + %.1f filter its + compliance (counts from the GPU run)"
-              % (*wl["shape"], t_asm, t_it, t_fit, t_ce, its_per_oc, filter_its_per_oc))
+    what = ("%dx%dx%d cuboid" % wl["shape"]) if "shape" in wl else ("generated %s domain" % wl["topvoxel"])
+    sample = ("oracle FP64 (numpy/scipy, BLAS on all cores, elementwise passes on one) on the same %s: "
+              "1 stencil assembly (%.1fs), 1 PCG iteration (K*u + V-cycle, %.2fs), 1 filter matvec (%.2fs), "
+              "1 compliance (%.2fs); OC iteration = assembly + %.1f PCG its + %.1f filter its + compliance "
+              "(counts from the GPU run)" % (what, t_asm, t_it, t_fit, t_ce, its_per_oc, filter_its_per_oc))
     return dict(value=1.0 / t_oc, unit="OC iterations/s", cores=cores, kind="port", sample=sample,
                 sec_per_oc=t_oc)
 
@@ -300,9 +326,14 @@ def main(argv=None):
     a = ap.parse_args(argv)
     wl = WORKLOADS[a.workload]
     ws, rank, local, dist, torch = dist_setup()
-    cfg = {"workload": "%s GLOBAL V0=%.2f rMin=sqrt(3): TOP3D_XL(true(%d,%d,%d),'GLOBAL',0.12,50,sqrt(3))"
-                       % (a.workload, wl["V0"], *wl["shape"]),
-           "elements": int(np.prod(wl["shape"])), "consType": wl["cons"],
+    if "shape" in wl:
+        call = "TOP3D_XL(true(%d,%d,%d),'%s',%g,%d,sqrt(3)%s)" % (*wl["shape"], wl["cons"], wl["V0"], wl["nLoop"],
+                                                             ",%g" % wl["rHat"] if wl["cons"] == "LOCAL" else "")
+    else:
+        call = "TOP3D_XL('<generated %s>.TopVoxel','%s',%g,%d,sqrt(3),%g)" % (wl["topvoxel"], wl["cons"], wl["V0"],
+                                                                           wl["nLoop"], wl["rHat"])
+    cfg = {"workload": "%s %s V0=%g rMin=sqrt(3): %s" % (a.workload, wl["cons"], wl["V0"], call),
+           "elements": int(np.prod(wl["shape"])) if "shape" in wl else None, "consType": wl["cons"],
            "l2": "inputs larger than L2 (state > 126 MB per job)", "parallelism": "replicas only"}
 
     if a.impl == "reference":

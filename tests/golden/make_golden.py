@@ -9,12 +9,14 @@ compare against the same numbers.
 """
 import os
 import sys
+import tempfile
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from oracle import top3dxl_oracle as O  # noqa: E402
+from top3d_xl_b200.workloads import IRREGULAR_SMALL, irregular_domain, write_topvoxel  # noqa: E402
 
 
 def noise_envelope(run, ref, seeds=(1, 2, 3, 4, 5, 6), eps=(1e-15, 1e-12)):
@@ -77,6 +79,14 @@ def main():
     env = noise_envelope(run, h)
     env["vox"] = vox
     save("irregular_global_6.npz", h, env)
+    # LOCAL on a small generated irregular domain read from a .TopVoxel file (random surface
+    # loads, fixed lowest layer): the irregular-workload generator at reduced size
+    path = os.path.join(tempfile.mkdtemp(), "irregular_small.TopVoxel")
+    write_topvoxel(path, *irregular_domain(**IRREGULAR_SMALL))
+    run = lambda: O.run_local(path, 0.5, 300, np.sqrt(3), 6.0, max_loops=4)  # noqa: E731
+    h = run()
+    h["c"] = np.array(h["c"])
+    save("irregular_topvoxel_local_4.npz", h, noise_envelope(run, h))
 
 
 if __name__ == "__main__":
