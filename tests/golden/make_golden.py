@@ -25,10 +25,13 @@ def noise_envelope(run, ref, seeds=(1, 2, 3, 4, 5, 6), eps=(1e-15, 1e-12)):
     exact factorisations of the coarsest matrix (condition ~1e4) differ in FP64.  This is
     the rounding sensitivity of the reference algorithm, which bounds how closely any
     re-implementation can track it; past the first iterations it saturates near 1e-6 on
-    irregular domains, whatever the noise level."""
+    irregular domains, whatever the noise level.  `its_var` is the largest change of each PCG
+    iteration count under the same noise (a count can move once the design has)."""
     orig = O.Solver.coarse_solve
     env_c = np.zeros(len(ref["c"]))
     env_x = 0.0
+    ref_its = np.asarray(ref["its"])
+    its_var = np.zeros(ref_its.size, dtype=np.int32)
     try:
         for sd, ep in [(s, e) for e in eps for s in seeds]:
             rng = np.random.default_rng(sd)
@@ -42,9 +45,12 @@ def noise_envelope(run, ref, seeds=(1, 2, 3, 4, 5, 6), eps=(1e-15, 1e-12)):
             n = min(len(h["c"]), len(ref["c"]))
             env_c[:n] = np.maximum(env_c[:n], np.abs(np.array(h["c"][:n]) - ref["c"][:n]) / np.abs(ref["c"][:n]))
             env_x = max(env_x, float(np.max(np.abs(h["xPhys"] - ref["xPhys"]))))
+            its = np.asarray(h["its"])
+            k = min(its.size, ref_its.size)
+            its_var[:k] = np.maximum(its_var[:k], np.abs(its[:k] - ref_its[:k]))
     finally:
         O.Solver.coarse_solve = orig
-    return dict(env_c=env_c, env_x=env_x)
+    return dict(env_c=env_c, env_x=env_x, its_var=its_var)
 
 
 def save(name, hist, extra=None):

@@ -1,7 +1,8 @@
 """End-to-end FP64 parity of the optimisation loop against the golden oracle
 histories (tests/golden/make_golden.py), through the C ABI.
 
-Bar: identical PCG iteration counts; per-iteration compliance within 1e-9
+Bar: identical PCG iteration counts (or within the oracle's own count spread under rounding
+noise, `its_var`, where it has one); per-iteration compliance within 1e-9
 relative while the reference algorithm's own rounding sensitivity allows it
 (the golden files hold `env_c`, the spread of the oracle against itself with
 1e-15 and 1e-12 relative noise in its coarse solve), and within 10x that envelope after;
@@ -38,7 +39,9 @@ def _check(g, cs, hist, x):
     c = np.array([h["c"] for h in hist])
     its = np.array([k for h in hist for k in h["its"]])
     assert len(c) == len(g["c"])
-    assert np.array_equal(its, g["its"]), (its, g["its"])
+    # counts agree exactly, except where the oracle's own counts move under rounding noise
+    var = g["its_var"] if "its_var" in g else np.zeros(len(g["its"]), np.int32)
+    assert np.all(np.abs(its - g["its"]) <= var), (its, g["its"], var)
     rel = np.abs(c - g["c"]) / np.abs(g["c"])
     env = g["env_c"]
     bar = np.where(env < 1e-10, 1e-9, np.maximum(1e-9, 10 * env))

@@ -215,7 +215,9 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     gjP.alloc(4 * (64 * 64 + size_t(128) * si.m));
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
-    coopCtas = coarse_coop ? slab_solve_coop_ctas(si.m) : 0;
+    // one cooperative launch pays off once the slab blocks are large; below that the chain of
+    // small launches is quicker (measured crossover between m = 507 and m = 867)
+    coopCtas = (coarse_coop && si.m > 600) ? slab_solve_coop_ctas(si.m) : 0;
   }
   // ---- workspaces ------------------------------------------------------------
   {
