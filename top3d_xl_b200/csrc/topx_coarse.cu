@@ -379,7 +379,7 @@ __global__ void k_form(SlabInfo si, FormOp op0, FormOp op1) {
 // ---------------------------------------------------------------------------
 constexpr int GJB = 64;  // pivot block width (= update tile)
 constexpr int GJ_PIVOT_THREADS = 128;
-constexpr size_t GJ_UPDATE_SMEM = 2 * GJB * GJB * sizeof(double);
+constexpr size_t GJ_UPDATE_SMEM = 2 * GJB * (GJB + 8) * sizeof(double);
 
 struct GJSet {
   double* A[2];
@@ -589,20 +589,34 @@ enum GJTiles { GJ_ALL = 0, GJ_CRIT = 1, GJ_REST = 2 };
 // rank-kb exchange update of one 64x64 tile per CTA (4x4 outputs per thread); both rank-64
 // operands (Ct rows of this tile, R or Pinv columns) come in with one round of loads, and the
 // old tile is fetched into registers before the product.
-// One TS x TS tile (TS = 64, or a 32 x 32 quarter) with origin (i0, j0): (TS/16)^2 outputs
-// per thread.  Tiles in the pivot row block take the new row panel (or Pinv); tiles in the
-// pivot column block take C_i Pinv; all others add C_i R_j.
+// FP64 tensor-core product step D += A B on an 8x8x4 fragment (mma.sync m8n8k4): lane l holds
+// A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + i].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int GJ_PAD = 8;  // row padding of the staged operands: a fragment load takes two wavefronts
+
+// One TS x TS tile (TS = 64, or a 32 x 32 quarter) with origin (i0, j0) on the FP64 tensor
+// cores: the 8 warps split it 2 x 4 (TS = 64) or 4 x 2 (TS = 32) and each warp runs 8x8x4
+// fragment products over the rank-64 operands staged in shared memory.  Tiles in the pivot
+// row block take the new row panel (or Pinv); tiles in the pivot column block take C_i Pinv;
+// all others add C_i R_j.
 template <int TS>
 __device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSet& set, int z, int i0, int j0,
                                                double* gj_smem) {
-  constexpr int PT = TS / 16;
-  double(*sC)[TS] = reinterpret_cast<double(*)[TS]>(gj_smem);            // [kt][row]
-  double(*sR)[TS] = reinterpret_cast<double(*)[TS]>(gj_smem + GJB * TS);  // [kt][col]
+  constexpr int LD = TS + GJ_PAD;
+  constexpr int WR = TS == 64 ? 2 : 4, WC = 8 / WR;  // warp grid over the tile
+  constexpr int FR = TS / WR / 8, FC = TS / WC / 8;  // 8x8 fragments per warp
+  double(*sC)[LD] = reinterpret_cast<double(*)[LD]>(gj_smem);            // [kt][row]
+  double(*sR)[LD] = reinterpret_cast<double(*)[LD]>(gj_smem + GJB * LD);  // [kt][col]
   double* __restrict__ A = z ? set.A[1] : set.A[0];
   const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
   const double* __restrict__ R = z ? set.R[1] : set.R[0];
   const double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int tid = threadIdx.x;
   const bool iK = (i0 >= k0 && i0 < k0 + GJB), jK = (j0 >= k0 && j0 < k0 + GJB);
   if (iK) {  // rows of the pivot block: new row panel / Pinv
     for (int i = tid; i < TS * TS; i += 256) {
@@ -628,47 +642,48 @@ __device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSe
     if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + (j - k0)] : R[int64_t(kt) * m + j];
     sR[kt][cc] = v;
   }
-  double acc[PT][PT];
+  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
+  const int rb = (warp / WC) * (TS / WR), cb = (warp % WC) * (TS / WC);
+  double acc[FR][FC][2];
 #pragma unroll
-  for (int q = 0; q < PT; ++q)
+  for (int fr = 0; fr < FR; ++fr)
 #pragma unroll
-    for (int w = 0; w < PT; ++w) {
-      const int ii = i0 + PT * ty + q, j = j0 + PT * tx + w;
-      acc[q][w] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
-    }
+    for (int fc = 0; fc < FC; ++fc)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int ii = i0 + rb + 8 * fr + g, j = j0 + cb + 8 * fc + 2 * q + h;
+        acc[fr][fc][h] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
+      }
   __syncthreads();
-#pragma unroll 8
-  for (int k = 0; k < GJB; ++k) {
-    double cv[PT], rv[PT];
+#pragma unroll 4
+  for (int k4 = 0; k4 < GJB / 4; ++k4) {
+    const int kk = 4 * k4 + q;
+    double a[FR], b[FC];
 #pragma unroll
-    for (int h = 0; h < PT; h += 2) {
-      const double2 c = *reinterpret_cast<const double2*>(&sC[k][PT * ty + h]);
-      const double2 r = *reinterpret_cast<const double2*>(&sR[k][PT * tx + h]);
-      cv[h] = c.x;
-      cv[h + 1] = c.y;
-      rv[h] = r.x;
-      rv[h + 1] = r.y;
-    }
+    for (int fr = 0; fr < FR; ++fr) a[fr] = sC[kk][rb + 8 * fr + g];
 #pragma unroll
-    for (int q = 0; q < PT; ++q)
+    for (int fc = 0; fc < FC; ++fc) b[fc] = sR[kk][cb + 8 * fc + g];
 #pragma unroll
-      for (int w = 0; w < PT; ++w) acc[q][w] = fma(cv[q], rv[w], acc[q][w]);
+    for (int fr = 0; fr < FR; ++fr)
+#pragma unroll
+      for (int fc = 0; fc < FC; ++fc) dmma884(acc[fr][fc][0], acc[fr][fc][1], a[fr], b[fc]);
   }
 #pragma unroll
-  for (int q = 0; q < PT; ++q) {
-    const int ii = i0 + PT * ty + q;
+  for (int fr = 0; fr < FR; ++fr) {
+    const int ii = i0 + rb + 8 * fr + g;
     if (ii >= m) continue;
-    const int jb = j0 + PT * tx;
     double* Ar = A + int64_t(ii) * m;
-    // 16-byte stores only where the absolute address is 16-byte aligned (matrix bases
-    // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
-    if (jb + PT - 1 < m && (reinterpret_cast<uintptr_t>(Ar + jb) & 15) == 0) {
 #pragma unroll
-      for (int w = 0; w < PT; w += 2) *reinterpret_cast<double2*>(Ar + jb + w) = make_double2(acc[q][w], acc[q][w + 1]);
-    } else {
-#pragma unroll
-      for (int w = 0; w < PT; ++w)
-        if (jb + w < m) Ar[jb + w] = acc[q][w];
+    for (int fc = 0; fc < FC; ++fc) {
+      const int j = j0 + cb + 8 * fc + 2 * q;
+      // 16-byte stores only where the absolute address is 16-byte aligned (matrix bases
+      // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
+      if (j + 1 < m && (reinterpret_cast<uintptr_t>(Ar + j) & 15) == 0) {
+        *reinterpret_cast<double2*>(Ar + j) = make_double2(acc[fr][fc][0], acc[fr][fc][1]);
+      } else {
+        if (j < m) Ar[j] = acc[fr][fc][0];
+        if (j + 1 < m) Ar[j + 1] = acc[fr][fc][1];
+      }
     }
   }
 }
