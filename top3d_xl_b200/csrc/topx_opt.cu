@@ -6,6 +6,8 @@
 #include "topx_kernels.cuh"
 #include "topx_opt.cuh"
 
+#include <algorithm>
+
 namespace topx {
 
 static inline unsigned grid1d(int64_t n, int threads, int cap = 148 * 16) {
@@ -72,76 +74,95 @@ void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, const Fil
 }
 
 // Filter operator y = sum_e KF u_e over solid hexes (MatTimesVec_matrixFree_B, TOP3D_XL.m:904-917),
-// node-centric with a shared-memory tile, fused PCG direction update and p'q.
-constexpr int FTY = 32, FTX = 4, FTZ = 2, FNT = FTY * FTX * FTZ;
+// node-centric: a CTA of 32x8 nodes marches FKZ node planes along z with a ring of three node
+// planes and two planes of solid flags in shared memory; fused PCG direction update and p'q.
+// The z-chunk zc is picked per grid so that small grids still give every SM a few CTAs.
+constexpr int FKY = 32, FKX = 8, FNT = FKY * FKX;
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, const FilterKe<T> kf, const T* __restrict__ in,
+__global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int zc, const FilterKe<T> kf, const T* __restrict__ in,
                                                     const T* __restrict__ zin, T* __restrict__ out,
                                                     const uint8_t* __restrict__ solid, PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
-  __shared__ T su[FTZ + 2][FTX + 2][FTY + 2];
-  __shared__ T ss[FTZ + 1][FTX + 1][FTY + 1];
+  __shared__ T su[3][FKX + 2][FKY + 2];
+  __shared__ T ss[2][FKX + 1][FKY + 1];
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
-  const int y0 = blockIdx.x * FTY, x0 = blockIdx.y * FTX, z0 = blockIdx.z * FTZ;
-  const int tid = threadIdx.x + FTY * (threadIdx.y + FTX * threadIdx.z);
+  const int y0 = blockIdx.x * FKY, x0 = blockIdx.y * FKX, zc0 = blockIdx.z * zc;
+  const int ty = threadIdx.x, tx = threadIdx.y;
+  const int tid = ty + FKY * tx;
   const bool first = (MODE != KU_PLAIN) && sc->first;
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
-  for (int i = tid; i < (FTZ + 2) * (FTX + 2) * (FTY + 2); i += FNT) {
-    const int sy = i % (FTY + 2), r = i / (FTY + 2), sx = r % (FTX + 2), sz = r / (FTX + 2);
-    const int gy = y0 - 1 + sy, gx = x0 - 1 + sx, gz = z0 - 1 + sz;
-    T v = T(0);
-    if (gy >= 0 && gy < nny && gx >= 0 && gx < nnx && gz >= 0 && gz < nnz) {
-      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
-      if (MODE == KU_PLAIN)
-        v = in[n];
-      else
-        v = first ? zin[n] : zin[n] + beta * in[n];
+  auto load_nodes = [&](int zp, int slot) {
+    for (int i = tid; i < (FKX + 2) * (FKY + 2); i += FNT) {
+      const int sy = i % (FKY + 2), sx = i / (FKY + 2);
+      const int gy = y0 - 1 + sy, gx = x0 - 1 + sx;
+      T v = T(0);
+      if (zp >= 0 && zp < nnz && gy >= 0 && gy < nny && gx >= 0 && gx < nnx) {
+        const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * zp);
+        if (MODE == KU_PLAIN)
+          v = in[n];
+        else
+          v = first ? zin[n] : zin[n] + beta * in[n];
+      }
+      su[slot][sx][sy] = v;
     }
-    su[sz][sx][sy] = v;
-  }
-  for (int i = tid; i < (FTZ + 1) * (FTX + 1) * (FTY + 1); i += FNT) {
-    const int sy = i % (FTY + 1), r = i / (FTY + 1), sx = r % (FTX + 1), sz = r / (FTX + 1);
-    const int ey = y0 - 1 + sy, ex = x0 - 1 + sx, ez = z0 - 1 + sz;
-    T v = T(0);
-    if (ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz)
-      v = solid[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)] ? T(1) : T(0);
-    ss[sz][sx][sy] = v;
-  }
-  __syncthreads();
-  const int ty = threadIdx.x, tx = threadIdx.y, tz = threadIdx.z;
-  const int gy = y0 + ty, gx = x0 + tx, gz = z0 + tz;
+  };
+  auto load_solid = [&](int ez, int slot) {
+    for (int i = tid; i < (FKX + 1) * (FKY + 1); i += FNT) {
+      const int sy = i % (FKY + 1), sx = i / (FKY + 1);
+      const int ey = y0 - 1 + sy, ex = x0 - 1 + sx;
+      T v = T(0);
+      if (ez >= 0 && ez < g.nz && ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx)
+        v = solid[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)] ? T(1) : T(0);
+      ss[slot][sx][sy] = v;
+    }
+  };
+  load_nodes(zc0 - 1, 0);
+  load_nodes(zc0, 1);
+  load_solid(zc0 - 1, 0);
+  const int gy = y0 + ty, gx = x0 + tx;
+  const bool own = gy < nny && gx < nnx;
   double dot = 0.0;
-  if (gy < nny && gx < nnx && gz < nnz) {
-    T acc[8];
+  for (int k = 0; k < zc; ++k) {
+    const int z = zc0 + k;
+    if (z >= nnz) break;
+    load_nodes(z + 1, (k + 2) % 3);
+    load_solid(z, (k + 1) % 2);
+    __syncthreads();
+    if (own) {
+      const T(*const pl[3])[FKY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
+      const T(*const el[2])[FKY + 1] = {ss[k % 2], ss[(k + 1) % 2]};
+      T acc[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) acc[e] = T(0);
+      for (int e = 0; e < 8; ++e) acc[e] = T(0);
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+      for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx)
+        for (int dx = -1; dx <= 1; ++dx)
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const T u = su[tz + 1 + dz][tx + 1 + dx][ty + 1 + dy];
+          for (int dy = -1; dy <= 1; ++dy) {
+            const T u = pl[dz + 1][tx + 1 + dx][ty + 1 + dy];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
-            const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
-            if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
-            const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
-            acc[e] = fma(kf.v[a * 8 + b], u, acc[e]);
+            for (int e = 0; e < 8; ++e) {
+              const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1, oz = (e & 4) ? 0 : -1;
+              const int ly = dy - oy, lx = dx - ox, lz = dz - oz;
+              if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
+              const int a = hex_local(-oy, -ox, -oz), b = hex_local(ly, lx, lz);
+              acc[e] = fma(kf.v[a * 8 + b], u, acc[e]);
+            }
           }
-        }
-    T y = T(0);
+      T y = T(0);
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
-      const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
-      y = fma(ss[tz + 1 + oz][tx + 1 + ox][ty + 1 + oy], acc[e], y);
+      for (int a = 0; a < 8; ++a) {
+        const int oy = -hex_ly(a), ox = -hex_lx(a), oz = -hex_lz(a);
+        const int e = (oy + 1) + 2 * (ox + 1) + 4 * (oz + 1);
+        y = fma(el[oz + 1][tx + 1 + ox][ty + 1 + oy], acc[e], y);
+      }
+      const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * z);
+      out[n] = y;
+      if (MODE != KU_PLAIN) dot += double(pl[1][tx + 1][ty + 1]) * double(y);
     }
-    const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
-    out[n] = y;
-    if (MODE != KU_PLAIN) dot = double(su[tz + 1][tx + 1][ty + 1]) * double(y);
+    __syncthreads();
   }
   if (MODE != KU_PLAIN) {
     double v[1] = {dot}, tot[1];
@@ -153,12 +174,15 @@ template <typename T>
 void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& kf, const T* in, const T* z, T* pout, T* out,
                       const uint8_t* solid, PcgScalars* sc, RedScratch rs) {
   (void)pout;
-  dim3 blk(FTY, FTX, FTZ);
-  dim3 grd((g.nny() + FTY - 1) / FTY, (g.nnx() + FTX - 1) / FTX, (g.nnz() + FTZ - 1) / FTZ);
+  const int tiles = ((g.nny() + FKY - 1) / FKY) * ((g.nnx() + FKX - 1) / FKX);
+  const int chunks = (148 * 4 + tiles - 1) / tiles;  // aim at four CTAs per SM
+  const int zc = std::max(2, std::min(16, (g.nnz() + chunks - 1) / chunks));
+  dim3 blk(FKY, FKX, 1);
+  dim3 grd((g.nny() + FKY - 1) / FKY, (g.nnx() + FKX - 1) / FKX, (g.nnz() + zc - 1) / zc);
   if (mode == KU_PLAIN)
-    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, kf, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, kf, in, z, out, solid, sc, rs), topx::count_launch());
   else
-    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, kf, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, kf, in, z, out, solid, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
