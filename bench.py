@@ -291,6 +291,22 @@ def run_sequential(jobs, precision, device):
     return dict(jobs=len(jobs), oc_its=its, busy_s=busy, oc_its_per_s=its / busy if busy > 0 else None)
 
 
+def max_over_ranks(ms_local, dist, torch, device):
+    """The job's time: the slowest rank's device time (one all-reduce of a scalar), then a
+    barrier so no rank leaves the timed phase early.  Identity without a process group."""
+    if not dist:
+        return ms_local
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def replicas_value(world_size, steps, ms_max):
+    """Whole-job throughput of N independent replicas: all ranks' OC iterations / slowest time."""
+    return world_size * steps / (ms_max / 1000.0)
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -392,19 +408,13 @@ def main(argv=None):
     with Clocks(device) as clk:
         fp64 = run_native(wl, "fp64", a.steps, a.warmup, device, profile_steps=2)
     ms_local = fp64["ms"]
-    if dist:
-        t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        dist.barrier()
-    else:
-        ms_max = ms_local
+    ms_max = max_over_ranks(ms_local, dist, torch, "cuda")
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return 0
     mixed = run_native(wl, "mixed", a.steps, a.warmup, device)
-    value = ws * a.steps / (ms_max / 1000.0)
+    value = replicas_value(ws, a.steps, ms_max)
     cm = np.array([h["c"] for h in mixed["hist"]])
     cd = np.array([h["c"] for h in fp64["hist"]])
     n = min(len(cm), len(cd))

@@ -176,3 +176,13 @@ def test_ke_value_classes_header_is_current_and_matches_ke():
         first.setdefault(c, Ke[idx] * np.sign(code))
         assert abs(Ke[idx] - np.sign(code) * first[c]) <= 1e-15 * abs(first[c])
     assert n == 10
+
+
+def test_mex_gateway_compiles_against_the_c_abi():
+    """top3d_xl_b200/matlab/topx_mex.c is compile-checked (no mex.h here: a declaration stub)."""
+    import subprocess
+    src = os.path.join(ROOT, "top3d_xl_b200", "matlab", "topx_mex.c")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "tests", "mex_stub"), "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
