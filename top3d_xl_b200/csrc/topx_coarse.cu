@@ -759,8 +759,11 @@ static void spd_inverse_batched(cudaStream_t st, const GJStreams& gs, int m, int
     if (k + 1 < nt) {
       TOPX_CUDA_OK(cudaEventRecord(gs.panel[k % 2], st));
       TOPX_CUDA_OK(cudaStreamWaitEvent(gs.side, gs.panel[k % 2], 0));
-      const unsigned nrest = std::min((nt - 1) * (nt - 1), unsigned(GJ_REST_CTAS / nset));
-      (k_gj_update<<<dim3(nrest, 1, nset), 256, GJ_REST_SMEM, gs.side>>>(m, k0, kb, set, GJ_REST, int(k + 1)),
+      // engines sharing the GPU keep ordinary CTAs here: reserving SMs would starve their neighbours
+      const unsigned nrest = gs.reserve_sms ? std::min((nt - 1) * (nt - 1), unsigned(GJ_REST_CTAS / nset))
+                                            : (nt - 1) * (nt - 1);
+      (k_gj_update<<<dim3(nrest, 1, nset), 256, gs.reserve_sms ? GJ_REST_SMEM : GJ_UPDATE_SMEM, gs.side>>>(
+           m, k0, kb, set, GJ_REST, int(k + 1)),
        topx::count_launch());
       TOPX_CUDA_OK(cudaEventRecord(gs.rest[k % 2], gs.side));
       if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));

@@ -22,6 +22,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   // graph captures; every host-side copy below waits for this stream first
   TOPX_CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   TOPX_CUDA_OK(cudaStreamCreateWithFlags(&gjs.side, cudaStreamNonBlocking));
+  gjs.reserve_sms = coarse_coop;  // engines alone on the GPU
   for (cudaEvent_t* e : {&gjs.panel[0], &gjs.panel[1], &gjs.rest[0], &gjs.rest[1]})
     TOPX_CUDA_OK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   prepare_coarse_kernels();

@@ -105,6 +105,7 @@ struct GJStreams {
   cudaStream_t side;
   cudaEvent_t panel[2];
   cudaEvent_t rest[2];
+  bool reserve_sms;  // side-stream CTAs take whole SMs (an engine alone on the GPU)
 };
 void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const double* A, const double* Bup,
                         double* Inv, double* X, double* XT, double* gj_scratch);

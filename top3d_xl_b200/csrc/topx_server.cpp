@@ -4,8 +4,9 @@
 // model, estimates its device footprint from the model's grid sizes and waits until that
 // footprint fits the HBM budget; then it creates the job's engine (own stream, own graphs,
 // own scratch), runs the optimisation loop and frees everything.  Jobs on different workers
-// overlap on the device.  Engines here use the multi-launch coarsest solve: a cooperative
-// launch wants every SM at once, which jobs sharing the GPU cannot promise.
+// overlap on the device.  Engines here use the multi-launch coarsest solve and ordinary CTAs
+// for the factorisation's side-stream update: a cooperative launch wants every SM at once and
+// SM-reserving CTAs would starve the neighbouring jobs.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -191,6 +192,9 @@ topx_status topx_server_create(topx_server** out, const topx_server_params* p) {
     topx_server_default_params(&s->params);
   if (s->params.slots < 1 || s->params.slots > 64) return TOPX_ERR_ARG;
   if (s->params.precision != TOPX_FP64 && s->params.precision != TOPX_MIXED) return TOPX_ERR_ARG;
+  // worker threads wait on their streams a lot: yield the core instead of spinning on it
+  // (takes effect only if this process has not touched the device yet)
+  if (cudaSetDeviceFlags(cudaDeviceScheduleYield) != cudaSuccess) cudaGetLastError();
   s->budget = s->params.hbm_budget_bytes;
   if (s->budget <= 0) {
     size_t fr = 0, tot = 0;
