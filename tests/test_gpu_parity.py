@@ -130,3 +130,27 @@ def test_filter_preserves_constants(setup):
     m, ctx = setup["m"], setup["ctx"]
     out, _ = ctx.filter(np.sqrt(3), np.ones(m.levels[0].numElements))
     assert np.max(np.abs(out - 1.0)) < 1e-3
+
+
+@pytest.mark.parametrize("shape", [(64, 96, 64), (112, 136, 112)])
+def test_vcycle_with_large_coarsest_slabs(shape):
+    # coarsest slabs of m = 243 (4 pivot blocks, the last one 51 wide) and m = 675 (11 blocks,
+    # the last one 35 wide): the Gauss-Jordan inverses run many tile tasks, both chains at once
+    from top3d_xl_b200 import Context
+    vox = np.ones(shape, bool)
+    m = O.build_model(vox)
+    x = np.random.default_rng(4).uniform(0.3, 1.0, m.levels[0].numElements)
+    S = m.S
+    E = S.modulusMin + x ** S.SIMPpenalty * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    with Context("fp64") as ctx:
+        ctx.load_voxels(vox)
+        ctx.set_moduli(E)
+        ctx.assemble()
+        for seed in (3, 5):  # two solves with the same factors
+            r = np.random.default_rng(seed).standard_normal(m.levels[0].numDOFs)
+            assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
+        ctx.assemble()  # a second factorisation through the same scratch and control words
+        r = np.random.default_rng(6).standard_normal(m.levels[0].numDOFs)
+        assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10

@@ -366,457 +366,39 @@ __global__ void k_form(SlabInfo si, FormOp op0, FormOp op1) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// SPD inverse in place by blocked Gauss-Jordan exchange (pivot blocks of 64),
-// batched over up to two matrices (grid z).  One exchange step on pivot block K:
-//   [P B; C D] -> [P^-1, -P^-1 B; C P^-1, D - C P^-1 B]
-// After all blocks the matrix holds its inverse.  No pivoting is needed for SPD.
-// Three launches per step:
-//   k_gj_pivot   CTA 0: P^-1 (register-blocked exchange on the 64x64 block);
-//                CTAs 1..: Ct = (old column panel A[:, K])^T, through a shared transpose
-//   k_gj_panel   R = -P^-1 A[K, :]
-//   k_gj_update  A[i, j] += C_i R_j,  A[i, K] = C_i P^-1,  A[K, :] = R (P^-1 on the diagonal)
-// ---------------------------------------------------------------------------
-constexpr int GJB = 64;  // pivot block width (= update tile)
-constexpr int GJ_PIVOT_THREADS = 128;
-constexpr size_t GJ_UPDATE_SMEM = 2 * GJB * (GJB + 8) * sizeof(double);
-
-struct GJSet {
-  double* A[2];
-  double* Pinv[2];
-  double* R[2];   // 64 x m
-  double* Ct[2];  // 64 x m
-};
-
-// 1/v by Newton-Raphson iteration x <- x (2 - v x) from a single-precision seed
-// (two steps: 24 -> ~48 -> full double accuracy), avoiding the long-latency
-// IEEE division on the pivot chain.
-__device__ __forceinline__ double recip_newton(double v) {
-  double x = double(1.0f / float(v));
-  x = x * (2.0 - v * x);
-  x = x * (2.0 - v * x);
-  return x;
-}
-
-// CTA 0: P = A[K,K] -> Pinv.  Thread (ri, ci) = (tid / 16, tid % 16) holds rows 8ri..8ri+7 and
-// columns 4ci..4ci+3 of the block in registers.  Each exchange step eliminates a 2x2 pivot
-// block (owned by one thread, which publishes its inverse) with the two pivot rows and columns
-// published through double-buffered shared arrays: one barrier per two pivots; every element
-// then takes two FMAs and the owners of the pivot rows and columns overwrite theirs.
-// Rows and columns >= kb hold the identity, which the exchange leaves unchanged.
-// CTAs 1..: 64 rows each of the old column panel, transposed into Ct.
-__global__ void __launch_bounds__(GJ_PIVOT_THREADS) k_gj_pivot(int m, int k0, int kb, GJSet set) {
-  const int z = blockIdx.z;
-  const double* __restrict__ A = z ? set.A[1] : set.A[0];
-  const int tid = threadIdx.x;
-  if (blockIdx.x > 0) {
-    __shared__ double tile[GJB][GJB + 1];
-    double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
-    const int i0 = (blockIdx.x - 1) * GJB;
-#pragma unroll 8
-    for (int e = tid; e < GJB * GJB; e += GJ_PIVOT_THREADS) {
-      const int rr = e / GJB, t = e % GJB;
-      const int ii = i0 + rr;
-      tile[rr][t] = (ii < m && t < kb) ? A[int64_t(ii) * m + k0 + t] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int e = tid; e < GJB * GJB; e += GJ_PIVOT_THREADS) {
-      const int t = e / GJB, rr = e % GJB;
-      const int ii = i0 + rr;
-      if (ii < m && t < kb) Ct[int64_t(t) * m + ii] = tile[rr][t];
-    }
-    return;
-  }
-  double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
-  __shared__ __align__(16) double rowb[2][2][GJB];
-  __shared__ __align__(16) double colb[2][2][GJB];
-  __shared__ double qb[2][4];
-  const int ci = tid & 15, ri = tid >> 4;
-  double a[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = 8 * ri + i, c = 4 * ci + q;
-      a[i][q] = (r < kb && c < kb) ? A[int64_t(k0 + r) * m + k0 + c] : (r == c ? 1.0 : 0.0);
-    }
-  // exchange steps on 2x2 pivot blocks {t, t+1}, Q = P^-1:
-  //   A_TT <- Q,  A_Tc <- -Q A_Tc,  A_rT <- A_rT Q = w_r,  A_rc <- A_rc - w_r A_Tc
-  // (a pivot at or past kb is an identity row and column, which the exchange leaves alone)
-  for (int tb = 0; tb < GJB / 8; ++tb) {
-    if (8 * tb >= kb) break;
-#pragma unroll
-    for (int qq = 0; qq < 8; qq += 2) {
-      const int t = 8 * tb + qq;
-      if (t >= kb) break;
-      const int buf = (qq >> 1) & 1;  // = (t / 2) & 1
-      const int cq = qq & 3;          // local column of pivot t in its owners (0 or 2)
-      const bool rowOwner = (ri == tb);
-      const bool colOwner = (ci == 2 * tb + (qq >> 2));
-      if (rowOwner) {
-        *reinterpret_cast<double2*>(&rowb[buf][0][4 * ci]) = make_double2(a[qq][0], a[qq][1]);
-        *reinterpret_cast<double2*>(&rowb[buf][0][4 * ci + 2]) = make_double2(a[qq][2], a[qq][3]);
-        *reinterpret_cast<double2*>(&rowb[buf][1][4 * ci]) = make_double2(a[qq + 1][0], a[qq + 1][1]);
-        *reinterpret_cast<double2*>(&rowb[buf][1][4 * ci + 2]) = make_double2(a[qq + 1][2], a[qq + 1][3]);
-        if (colOwner) {
-          const double p00 = a[qq][cq], p01 = a[qq][cq + 1], p10 = a[qq + 1][cq], p11 = a[qq + 1][cq + 1];
-          const double rd = recip_newton(p00 * p11 - p01 * p10);
-          qb[buf][0] = p11 * rd;
-          qb[buf][1] = -p01 * rd;
-          qb[buf][2] = -p10 * rd;
-          qb[buf][3] = p00 * rd;
-        }
-      }
-      if (colOwner) {
-#pragma unroll
-        for (int i = 0; i < 8; i += 2) {
-          *reinterpret_cast<double2*>(&colb[buf][0][8 * ri + i]) = make_double2(a[i][cq], a[i + 1][cq]);
-          *reinterpret_cast<double2*>(&colb[buf][1][8 * ri + i]) = make_double2(a[i][cq + 1], a[i + 1][cq + 1]);
-        }
-      }
-      __syncthreads();
-      const double q00 = qb[buf][0], q01 = qb[buf][1], q10 = qb[buf][2], q11 = qb[buf][3];
-      double r0[4], r1[4];
-      {
-        const double2 x01 = *reinterpret_cast<const double2*>(&rowb[buf][0][4 * ci]);
-        const double2 x23 = *reinterpret_cast<const double2*>(&rowb[buf][0][4 * ci + 2]);
-        const double2 y01 = *reinterpret_cast<const double2*>(&rowb[buf][1][4 * ci]);
-        const double2 y23 = *reinterpret_cast<const double2*>(&rowb[buf][1][4 * ci + 2]);
-        r0[0] = x01.x;
-        r0[1] = x01.y;
-        r0[2] = x23.x;
-        r0[3] = x23.y;
-        r1[0] = y01.x;
-        r1[1] = y01.y;
-        r1[2] = y23.x;
-        r1[3] = y23.y;
-      }
-      double w0[8], w1[8];
-#pragma unroll
-      for (int i = 0; i < 8; i += 2) {
-        const double2 c0 = *reinterpret_cast<const double2*>(&colb[buf][0][8 * ri + i]);
-        const double2 c1 = *reinterpret_cast<const double2*>(&colb[buf][1][8 * ri + i]);
-        w0[i] = fma(c0.x, q00, c1.x * q10);
-        w1[i] = fma(c0.x, q01, c1.x * q11);
-        w0[i + 1] = fma(c0.y, q00, c1.y * q10);
-        w1[i + 1] = fma(c0.y, q01, c1.y * q11);
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a[i][q] = fma(-w1[i], r1[q], fma(-w0[i], r0[q], a[i][q]));
-      if (rowOwner) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          a[qq][q] = -fma(q00, r0[q], q01 * r1[q]);
-          a[qq + 1][q] = -fma(q10, r0[q], q11 * r1[q]);
-        }
-      }
-      if (colOwner) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          a[i][cq] = w0[i];
-          a[i][cq + 1] = w1[i];
-        }
-        if (rowOwner) {
-          a[qq][cq] = q00;
-          a[qq][cq + 1] = q01;
-          a[qq + 1][cq] = q10;
-          a[qq + 1][cq + 1] = q11;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    double* dst = Pinv + (8 * ri + i) * GJB + 4 * ci;
-    *reinterpret_cast<double2*>(dst) = make_double2(a[i][0], a[i][1]);
-    *reinterpret_cast<double2*>(dst + 2) = make_double2(a[i][2], a[i][3]);
-  }
-}
-
-// row panel R[kt][j] = -sum_t Pinv[kt][t] A[k0 + t][j] for the columns outside the pivot block.
-// CTA (x: 64 columns, y: 16 of the 64 pivot rows); thread: one row, four columns.
-__global__ void __launch_bounds__(256) k_gj_panel(int m, int k0, int kb, GJSet set) {
-  const int z = blockIdx.z;
-  const int j0 = blockIdx.x * GJB, r0 = blockIdx.y * 16;
-  if (j0 == k0 || r0 >= kb) return;
-  const double* __restrict__ A = z ? set.A[1] : set.A[0];
-  const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
-  double* __restrict__ R = z ? set.R[1] : set.R[0];
-  __shared__ double sP[16][GJB + 1];
-  __shared__ __align__(16) double sA[GJB][GJB + 4];
-  const int tid = threadIdx.x;
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const int i = tid + 256 * e;
-    sP[i / GJB][i % GJB] = Pinv[(r0 + i / GJB) * GJB + i % GJB];
-  }
-#pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    const int i = tid + 256 * e;
-    const int t = i / GJB, cc = i % GJB;
-    const int j = j0 + cc;
-    sA[t][cc] = (t < kb && j < m) ? A[int64_t(k0 + t) * m + j] : 0.0;
-  }
-  __syncthreads();
-  const int rr = tid >> 4, cx = (tid & 15) * 4;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 16
-  for (int t = 0; t < GJB; ++t) {
-    const double p = sP[rr][t];
-    const double2 a01 = *reinterpret_cast<const double2*>(&sA[t][cx]);
-    const double2 a23 = *reinterpret_cast<const double2*>(&sA[t][cx + 2]);
-    acc[0] = fma(p, a01.x, acc[0]);
-    acc[1] = fma(p, a01.y, acc[1]);
-    acc[2] = fma(p, a23.x, acc[2]);
-    acc[3] = fma(p, a23.y, acc[3]);
-  }
-  if (r0 + rr < kb) {
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-      const int j = j0 + cx + w;
-      if (j < m) R[int64_t(r0 + rr) * m + j] = -acc[w];
-    }
-  }
-}
-
-// Tiles of one exchange update: all of them (GJ_ALL), only those in row or column block kc
-// (GJ_CRIT: what the next pivot and panel read), or all the others (GJ_REST).
-enum GJTiles { GJ_ALL = 0, GJ_CRIT = 1, GJ_REST = 2 };
-
-// rank-kb exchange update of one 64x64 tile per CTA (4x4 outputs per thread); both rank-64
-// operands (Ct rows of this tile, R or Pinv columns) come in with one round of loads, and the
-// old tile is fetched into registers before the product.
-// FP64 tensor-core product step D += A B on an 8x8x4 fragment (mma.sync m8n8k4): lane l holds
-// A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + i].
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-constexpr int GJ_PAD = 8;  // row padding of the staged operands: a fragment load takes two wavefronts
-
-// One TS x TS tile (TS = 64, or a 32 x 32 quarter) with origin (i0, j0) on the FP64 tensor
-// cores: the 8 warps split it 2 x 4 (TS = 64) or 4 x 2 (TS = 32) and each warp runs 8x8x4
-// fragment products over the rank-64 operands staged in shared memory.  Tiles in the pivot
-// row block take the new row panel (or Pinv); tiles in the pivot column block take C_i Pinv;
-// all others add C_i R_j.
-template <int TS>
-__device__ __forceinline__ void gj_update_tile(int m, int k0, int kb, const GJSet& set, int z, int i0, int j0,
-                                               double* gj_smem) {
-  constexpr int LD = TS + GJ_PAD;
-  constexpr int WR = TS == 64 ? 2 : 4, WC = 8 / WR;  // warp grid over the tile
-  constexpr int FR = TS / WR / 8, FC = TS / WC / 8;  // 8x8 fragments per warp
-  double(*sC)[LD] = reinterpret_cast<double(*)[LD]>(gj_smem);            // [kt][row]
-  double(*sR)[LD] = reinterpret_cast<double(*)[LD]>(gj_smem + GJB * LD);  // [kt][col]
-  double* __restrict__ A = z ? set.A[1] : set.A[0];
-  const double* __restrict__ Pinv = z ? set.Pinv[1] : set.Pinv[0];
-  const double* __restrict__ R = z ? set.R[1] : set.R[0];
-  const double* __restrict__ Ct = z ? set.Ct[1] : set.Ct[0];
-  const int tid = threadIdx.x;
-  const bool iK = (i0 >= k0 && i0 < k0 + GJB), jK = (j0 >= k0 && j0 < k0 + GJB);
-  if (iK) {  // rows of the pivot block: new row panel / Pinv
-    for (int i = tid; i < TS * TS; i += 256) {
-      const int ii = i0 + i / TS, j = j0 + i % TS;
-      const int pr = ii - k0;
-      if (pr < kb && j < m) A[int64_t(ii) * m + j] = jK ? Pinv[pr * GJB + (j - k0)] : R[int64_t(pr) * m + j];
-    }
-    return;
-  }
-#pragma unroll
-  for (int e = 0; e < TS / 4; ++e) {
-    const int i = tid + 256 * e;
-    const int kt = i / TS, rr = i % TS;
-    const int ii = i0 + rr;
-    sC[kt][rr] = (kt < kb && ii < m) ? Ct[int64_t(kt) * m + ii] : 0.0;
-  }
-#pragma unroll
-  for (int e = 0; e < TS / 4; ++e) {
-    const int i = tid + 256 * e;
-    const int kt = i / TS, cc = i % TS;
-    const int j = j0 + cc;
-    double v = 0.0;
-    if (kt < kb && j < m) v = jK ? Pinv[kt * GJB + (j - k0)] : R[int64_t(kt) * m + j];
-    sR[kt][cc] = v;
-  }
-  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
-  const int rb = (warp / WC) * (TS / WR), cb = (warp % WC) * (TS / WC);
-  double acc[FR][FC][2];
-#pragma unroll
-  for (int fr = 0; fr < FR; ++fr)
-#pragma unroll
-    for (int fc = 0; fc < FC; ++fc)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int ii = i0 + rb + 8 * fr + g, j = j0 + cb + 8 * fc + 2 * q + h;
-        acc[fr][fc][h] = (!jK && ii < m && j < m) ? A[int64_t(ii) * m + j] : 0.0;
-      }
-  __syncthreads();
-#pragma unroll 4
-  for (int k4 = 0; k4 < GJB / 4; ++k4) {
-    const int kk = 4 * k4 + q;
-    double a[FR], b[FC];
-#pragma unroll
-    for (int fr = 0; fr < FR; ++fr) a[fr] = sC[kk][rb + 8 * fr + g];
-#pragma unroll
-    for (int fc = 0; fc < FC; ++fc) b[fc] = sR[kk][cb + 8 * fc + g];
-#pragma unroll
-    for (int fr = 0; fr < FR; ++fr)
-#pragma unroll
-      for (int fc = 0; fc < FC; ++fc) dmma884(acc[fr][fc][0], acc[fr][fc][1], a[fr], b[fc]);
-  }
-#pragma unroll
-  for (int fr = 0; fr < FR; ++fr) {
-    const int ii = i0 + rb + 8 * fr + g;
-    if (ii >= m) continue;
-    double* Ar = A + int64_t(ii) * m;
-#pragma unroll
-    for (int fc = 0; fc < FC; ++fc) {
-      const int j = j0 + cb + 8 * fc + 2 * q;
-      // 16-byte stores only where the absolute address is 16-byte aligned (matrix bases
-      // Inv + s*m*m are odd multiples of 8 bytes when m is odd)
-      if (j + 1 < m && (reinterpret_cast<uintptr_t>(Ar + j) & 15) == 0) {
-        *reinterpret_cast<double2*>(Ar + j) = make_double2(acc[fr][fc][0], acc[fr][fc][1]);
-      } else {
-        if (j < m) Ar[j] = acc[fr][fc][0];
-        if (j + 1 < m) Ar[j + 1] = acc[fr][fc][1];
-      }
-    }
-  }
-}
-
-// the kernel: tiles selected by `tiles` (see GJTiles), taken in a CTA-stride loop
-__global__ void __launch_bounds__(256, 3) k_gj_update(int m, int k0, int kb, GJSet set, int tiles, int kc) {
-  extern __shared__ __align__(16) double gj_smem[];
-  const int nt = (m + GJB - 1) / GJB;
-  // the critical tiles go in 32 x 32 quarters: four times the CTAs, a quarter of the latency
-  const int ntiles = tiles == GJ_ALL ? nt * nt : tiles == GJ_CRIT ? 4 * (2 * nt - 1) : (nt - 1) * (nt - 1);
-  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
-    int ib, jb;
-    if (tiles == GJ_ALL) {
-      ib = b / nt;
-      jb = b - ib * nt;
-    } else if (tiles == GJ_CRIT) {
-      const int tb = b >> 2;
-      if (tb < nt) {
-        ib = kc;
-        jb = tb;
-      } else {
-        ib = tb - nt;
-        ib += ib >= kc;
-        jb = kc;
-      }
-    } else {
-      ib = b / (nt - 1);
-      jb = b - ib * (nt - 1);
-      ib += ib >= kc;
-      jb += jb >= kc;
-    }
-    if (tiles == GJ_CRIT)
-      gj_update_tile<32>(m, k0, kb, set, int(blockIdx.z), ib * GJB + 32 * ((b >> 1) & 1), jb * GJB + 32 * (b & 1),
-                         gj_smem);
-    else
-      gj_update_tile<64>(m, k0, kb, set, int(blockIdx.z), ib * GJB, jb * GJB, gj_smem);
-    __syncthreads();
-  }
-}
-
-// The side-stream update runs on GJ_REST_CTAS CTAs that each reserve a whole SM (their shared
-// memory request leaves no room for another CTA), so the latency-bound pivot and panel of the
-// next step get SMs of their own instead of sharing FP64 pipes with update tiles.
-constexpr int GJ_REST_CTAS = 96;
-constexpr size_t GJ_REST_SMEM = 200 * 1024;
-
 // once per device and process: engines on several host threads share the attributes
-void prepare_coarse_kernels() {
-  static std::mutex mu;
-  static bool done[64] = {};
-  int dev = 0;
-  TOPX_CUDA_OK(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(mu);
-  if (dev >= 0 && dev < 64 && done[dev]) return;
+void prepare_coarse_kernels() { prepare_gj_flow(); }
 
-  TOPX_CUDA_OK(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(GJ_REST_SMEM)));
-  if (dev >= 0 && dev < 64) done[dev] = true;
-}
-
-// Exchange steps with one step of lookahead: after the panel of step k, the tiles that step
-// k+1's pivot and panel read (row and column block k+1) are updated on the main stream while
-// all other tiles are updated on the side stream, overlapping step k+1's pivot and panel.
-// Steps alternate between two scratch sets, since the side stream still reads step k's
-// (Pinv, R, Ct) while step k+1 writes its own.
-static void spd_inverse_batched(cudaStream_t st, const GJStreams& gs, int m, int nset, const GJSet (&sets)[2]) {
-  const unsigned nt = (m + GJB - 1) / GJB;
-  for (unsigned k = 0; k < nt; ++k) {
-    const GJSet& set = sets[k % 2];
-    const int k0 = int(k) * GJB;
-    const int kb = (m - k0) < GJB ? (m - k0) : GJB;
-    (k_gj_pivot<<<dim3(1 + nt, 1, nset), GJ_PIVOT_THREADS, 0, st>>>(m, k0, kb, set), topx::count_launch());
-    (k_gj_panel<<<dim3(nt, 4, nset), 256, 0, st>>>(m, k0, kb, set), topx::count_launch());
-    if (k + 1 < nt) {
-      TOPX_CUDA_OK(cudaEventRecord(gs.panel[k % 2], st));
-      TOPX_CUDA_OK(cudaStreamWaitEvent(gs.side, gs.panel[k % 2], 0));
-      // engines sharing the GPU keep ordinary CTAs here: reserving SMs would starve their neighbours
-      const unsigned nrest = gs.reserve_sms ? std::min((nt - 1) * (nt - 1), unsigned(GJ_REST_CTAS / nset))
-                                            : (nt - 1) * (nt - 1);
-      (k_gj_update<<<dim3(nrest, 1, nset), 256, gs.reserve_sms ? GJ_REST_SMEM : GJ_UPDATE_SMEM, gs.side>>>(
-           m, k0, kb, set, GJ_REST, int(k + 1)),
-       topx::count_launch());
-      TOPX_CUDA_OK(cudaEventRecord(gs.rest[k % 2], gs.side));
-      if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
-      (k_gj_update<<<dim3(4 * (2 * nt - 1), 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_CRIT,
-                                                                                int(k + 1)),
-       topx::count_launch());
-    } else {
-      if (k > 0) TOPX_CUDA_OK(cudaStreamWaitEvent(st, gs.rest[(k - 1) % 2], 0));
-      (k_gj_update<<<dim3(nt * nt, 1, nset), 256, GJ_UPDATE_SMEM, st>>>(m, k0, kb, set, GJ_ALL, 0),
-       topx::count_launch());
-    }
-  }
-  TOPX_CUDA_OK(cudaGetLastError());
-}
-
-void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const double* A, const double* Bup,
-                        double* Sinv, double* X, double* XT, double* gj_scratch) {
+// Every Schur complement is inverted in place by the dataflow Gauss-Jordan kernel
+// (topx_gjflow.cu), the top and bottom chains' matrices in the same launch.
+void launch_slab_factor(cudaStream_t st, const GJFlow& gf, SlabInfo si, const double* A, const double* Bup,
+                        double* Sinv, double* X, double* XT) {
   const int m = si.m, ns = si.ns, mid = ns / 2;
   const int64_t mm = int64_t(m) * m;
   const int64_t bs = int64_t(si.nu) * si.nv * 81;
   const unsigned nbm = grid1d(mm, 256);
-  // scratch per (step parity, chain): Pinv 64x64, R 64xm, Ct 64xm
-  const int64_t gjs = 64 * 64 + 2 * 64 * int64_t(m);
-  GJSet sets[2] = {};
-  for (int p = 0; p < 2; ++p)
-    for (int c = 0; c < 2; ++c) {
-      sets[p].Pinv[c] = gj_scratch + (2 * p + c) * gjs;
-      sets[p].R[c] = sets[p].Pinv[c] + 64 * 64;
-      sets[p].Ct[c] = sets[p].R[c] + 64 * int64_t(m);
-    }
-  GJSet& set = sets[0];
+  auto invert = [&](int nset, double* A0, double* A1) {
+    launch_gj_flow(st, m, nset, A0, A1, gf.tasks[nset - 1], gf.ntasks[nset - 1], gf.scratch, gf.ctrl, gf.nctas);
+  };
   const int ntop = mid, nbot = ns - 1 - mid;
   for (int k = 0; k < std::max(ntop, nbot); ++k) {
     SchurOp so[2] = {};
     FormOp fo[2] = {};
+    double* inv[2] = {nullptr, nullptr};
     int nset = 0, nform = 0;
     if (k < ntop) {  // top slab k
       const int s = k;
       so[nset] = SchurOp{A + s * mm, Sinv + s * mm, s ? X + (s - 1) * mm : nullptr, s ? Bup + (s - 1) * bs : nullptr,
                          nullptr, nullptr};
-      set.A[nset] = Sinv + s * mm;
-      ++nset;
+      inv[nset++] = Sinv + s * mm;
     }
     if (k < nbot) {  // bottom slab ns-1-k
       const int s = ns - 1 - k;
       so[nset] = SchurOp{A + s * mm, Sinv + s * mm, nullptr, nullptr, k ? X + s * mm : nullptr, k ? Bup + s * bs : nullptr};
-      set.A[nset] = Sinv + s * mm;
-      ++nset;
+      inv[nset++] = Sinv + s * mm;
     }
-    sets[1].A[0] = set.A[0];
-    sets[1].A[1] = set.A[1];
     (k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]), topx::count_launch());
-    spd_inverse_batched(st, gs, m, nset, sets);
+    invert(nset, inv[0], inv[1]);
     if (k < ntop) {  // L_k = B_k^T S_k^{-1}
       fo[nform++] = FormOp{Bup + k * bs, Sinv + k * mm, X + k * mm, XT + k * mm, 0};
     }
@@ -831,8 +413,7 @@ void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const
              mid > 0 ? Bup + (mid - 1) * bs : nullptr, mid < ns - 1 ? X + mid * mm : nullptr,
              mid < ns - 1 ? Bup + mid * bs : nullptr};
   (k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm), topx::count_launch());
-  set.A[0] = sets[1].A[0] = Sinv + mid * mm;
-  spd_inverse_batched(st, gs, m, 1, sets);
+  invert(1, Sinv + mid * mm, nullptr);
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

@@ -1,5 +1,6 @@
 // Device engine of the TOP3D_XL B200 path (see topx_engine.hpp).
 #include "topx_engine.hpp"
+#include "topx_gjflow.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -21,10 +22,6 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   // other host threads (and their synchronous set-up copies) never stall or break this one's
   // graph captures; every host-side copy below waits for this stream first
   TOPX_CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  TOPX_CUDA_OK(cudaStreamCreateWithFlags(&gjs.side, cudaStreamNonBlocking));
-  gjs.reserve_sms = coarse_coop;  // engines alone on the GPU
-  for (cudaEvent_t* e : {&gjs.panel[0], &gjs.panel[1], &gjs.rest[0], &gjs.rest[1]})
-    TOPX_CUDA_OK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   prepare_coarse_kernels();
   prepare_fem_kernels();
   nl = M.numLevels;
@@ -213,7 +210,19 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
       slabLT32.alloc(mm * nsm1);
     }
     slabBup.alloc(size_t(si.nu) * si.nv * 81 * nsm1);
-    gjP.alloc(4 * (64 * 64 + size_t(128) * si.m));
+    for (int nset = 1; nset <= 2; ++nset) {
+      const std::vector<uint32_t> plan = gf_plan(si.m, nset);
+      gf_check_plan(plan, si.m, nset);
+      gfTasks[nset - 1].upload(plan.data(), plan.size());
+      gf.tasks[nset - 1] = gfTasks[nset - 1].p;
+      gf.ntasks[nset - 1] = unsigned(plan.size());
+    }
+    gfScr.alloc(gf_scratch_doubles(si.m), false);
+    gfCtrl.alloc(gf_ctrl_words(si.m));
+    gf.scratch = gfScr.p;
+    gf.ctrl = gfCtrl.p;
+    // an engine alone on the GPU fills it; engines sharing it leave room for their neighbours
+    gf.nctas = gj_flow_ctas(coarse_coop);
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
     // one cooperative launch pays off once the slab blocks are large; below that the chain of
@@ -248,6 +257,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   dscal.alloc(16);
   TOPX_CUDA_OK(cudaMallocHost(&h_sc, sizeof(PcgScalars)));
   TOPX_CUDA_OK(cudaMallocHost(&h_bar, sizeof(CoopBarrier)));
+  TOPX_CUDA_OK(cudaMallocHost(&h_gferr, sizeof(int)));
+  *h_gferr = 0;
   // ---- optimiser state -------------------------------------------------------
   for (DevBuf<double>* b : {&x, &xPhys, &dc, &ce, &tmpA, &tmpB, &xTilde, &xhat, &dfdx, &dxv, &volMax})
     b->alloc(size_t(Ne));
@@ -287,7 +298,6 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
 Engine::~Engine() {
   // no work of this engine may still be in flight when its buffers and graphs go
   if (st) cudaStreamSynchronize(st);
-  if (gjs.side) cudaStreamSynchronize(gjs.side);
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
   for (auto e : ev) cudaEventDestroy(e);
   for (auto e : sev) cudaEventDestroy(e);
@@ -296,9 +306,7 @@ Engine::~Engine() {
     if (e) cudaEventDestroy(e);
   if (h_sc) cudaFreeHost(h_sc);
   if (h_bar) cudaFreeHost(h_bar);
-  for (auto e : {gjs.panel[0], gjs.panel[1], gjs.rest[0], gjs.rest[1]})
-    if (e) cudaEventDestroy(e);
-  if (gjs.side) cudaStreamDestroy(gjs.side);
+  if (h_gferr) cudaFreeHost(h_gferr);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -334,20 +342,31 @@ void Engine::alloc_fwork(FWork<TF>& f) {
 void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
   TOPX_CUDA_OK(cudaMemcpyAsync(h_sc, d, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
   if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+  if (gf.ctrl) TOPX_CUDA_OK(cudaMemcpyAsync(h_gferr, gf.ctrl, sizeof(int), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   h = *h_sc;
-  if (coopCtas && h_bar->err) {
-    TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
-    throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
-  }
+  check_device_waits();
 }
 
 void Engine::check_coop_barrier() {
   if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+  if (gf.ctrl) TOPX_CUDA_OK(cudaMemcpyAsync(h_gferr, gf.ctrl, sizeof(int), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  check_device_waits();
+}
+
+// The bounded waits of the device code set an error word instead of spinning on; the words
+// were copied into pinned memory before the caller's stream sync.  A word that is set is
+// cleared (so the engine stays usable) and reported.
+void Engine::check_device_waits() const {
   if (coopCtas && h_bar->err) {
     TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
     throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
+  }
+  if (gf.ctrl && *h_gferr) {
+    *h_gferr = 0;
+    TOPX_CUDA_OK(cudaMemset(gf.ctrl, 0, sizeof(int)));
+    throw std::runtime_error("coarse factorisation: a dependency wait of the Gauss-Jordan inverse gave up");
   }
 }
 
@@ -425,7 +444,7 @@ void Engine::factor_coarsest() {
   launch_slab_assemble(st, G[nl - 1], si, Ks[nl - 1].p, present[nl - 1].p, slabA.p, slabBup.p);
   sec_end();
   sec_begin(SEC_INVERSE);
-  launch_slab_factor(st, gjs, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p, gjP.p);
+  launch_slab_factor(st, gf, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p);
   sec_end();
   if (prec == PREC_MIXED) {
     launch_convert<double, float>(st, slabSinv.p, slabSinv32.p, int64_t(slabSinv.n));

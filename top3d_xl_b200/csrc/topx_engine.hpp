@@ -162,7 +162,7 @@ class Engine {
   Model& M;
   int prec;
   cudaStream_t st = nullptr;
-  GJStreams gjs{};  // side stream + events of the coarse factorisation
+  GJFlow gf{};  // dataflow inverse of the coarse factorisation: plans, scratch, control words
   int nl = 0;
   std::vector<Grid> G;  // per level
   int64_t Ne = 0, Nn = 0;
@@ -198,12 +198,15 @@ class Engine {
   DevBuf<double> fl_F;
   int nflag = 0;
   SlabInfo si;
-  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gjP, gjR, gjC;
+  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gfScr;
+  DevBuf<uint32_t> gfTasks[2];  // inverse task plans for one and two matrices
+  DevBuf<unsigned> gfCtrl;      // control words of the inverse (word 0: error flag)
   DevBuf<float> slabSinv32, slabL32, slabLT32;  // FP32 copies applied by the mixed-precision V-cycle
   DevBuf<double> slabBS, slabW, slabV, slabXS;  // slab-ordered vectors of one coarse solve
   DevBuf<CoopBarrier> coopBar;  // barrier of the cooperative coarse solve
   int coopCtas = 0;             // its CTA count; 0: multi-launch coarse solve
   void check_coop_barrier();    // waits for the stream; throws if a barrier wait gave up (re-arming it)
+  void check_device_waits() const;  // after a stream sync: throws if a bounded device wait gave up
   // workspaces
   KrylovWork kw;
   VWork<double> v64;
@@ -221,6 +224,7 @@ class Engine {
   DevBuf<double> dscal;
   PcgScalars* h_sc = nullptr;  // pinned
   CoopBarrier* h_bar = nullptr;  // pinned
+  int* h_gferr = nullptr;        // pinned copy of gfCtrl[0]
   // optimiser state (compact, FP64)
   DevBuf<double> x, xPhys, dc, ce, tmpA, tmpB, xTilde, xhat, dfdx, dxv, volMax;
   DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;

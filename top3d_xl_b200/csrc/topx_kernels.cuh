@@ -97,18 +97,27 @@ void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks
 void prepare_coarse_kernels();
 // caches the SM count used to shape the K*u launch (call once per device, outside capture)
 void prepare_fem_kernels();
-// twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
-// Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes);
-// gj_scratch holds 4 * (64*64 + 128*m) doubles
-// side stream and events of the factorisation's lookahead (the side stream joins graph captures)
-struct GJStreams {
-  cudaStream_t side;
-  cudaEvent_t panel[2];
-  cudaEvent_t rest[2];
-  bool reserve_sms;  // side-stream CTAs take whole SMs (an engine alone on the GPU)
+// Dataflow Gauss-Jordan inverse (topx_gjflow.cu): ticket-ordered task tables for one and two
+// matrices (gf_plan), ring scratch (gf_scratch_doubles) and control words (gf_ctrl_words; word
+// 0 is the error flag, set when a wait gave up, read and cleared by the host).
+struct GJFlow {
+  const uint32_t* tasks[2];
+  unsigned ntasks[2];
+  double* scratch;
+  unsigned* ctrl;
+  int nctas;
 };
-void launch_slab_factor(cudaStream_t st, const GJStreams& gs, SlabInfo si, const double* A, const double* Bup,
-                        double* Inv, double* X, double* XT, double* gj_scratch);
+// one-time per-device kernel attributes (call outside stream capture)
+void prepare_gj_flow();
+// CTAs of one inverse launch: two per SM for an engine alone on the GPU, else half the SMs
+int gj_flow_ctas(bool whole_gpu);
+// in-place inverse of the SPD m x m matrices A0 (and A1 when nset == 2)
+void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,
+                    unsigned ntasks, double* scratch, unsigned* ctrl, int nctas);
+// twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
+// Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes)
+void launch_slab_factor(cudaStream_t st, const GJFlow& gf, SlabInfo si, const double* A, const double* Bup,
+                        double* Inv, double* X, double* XT);
 // x = K_coarsest^{-1} b; bs, W, V, xs are ns*m FP64 scratch vectors in slab order
 template <typename T, typename TM>
 void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT, const T* b,

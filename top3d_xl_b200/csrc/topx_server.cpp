@@ -21,6 +21,7 @@
 
 #include "topx.h"
 #include "topx_engine.hpp"
+#include "topx_gjflow.hpp"
 
 namespace {
 
@@ -46,8 +47,12 @@ int64_t footprint_estimate(const topx_info& in, int precision) {
   std::sort(d, d + 3);
   const int64_t ns = d[2], m = 3 * d[0] * d[1];
   const int64_t slab = (2 * ns + 2 * (ns - 1)) * m * m * 8 + (precision == TOPX_MIXED ? 3 * ns * m * m * 4 : 0);
+  // the Gauss-Jordan inverse's ring scratch, control words and task plans (~nt^3 tasks each)
+  const int64_t nt = topx::gf_tiles(int(m));
+  const int64_t inverse = int64_t(topx::gf_scratch_doubles(int(m))) * 8 + int64_t(topx::gf_ctrl_words(int(m))) * 4 +
+                          3 * nt * (nt * nt + 2 * nt + 1) * 4;
   const int64_t per_node = precision == TOPX_MIXED ? 560 : 520, per_elem = 200;
-  return per_node * nodes + per_elem * elems + slab + (int64_t(48) << 20);
+  return per_node * nodes + per_elem * elems + slab + inverse + (int64_t(48) << 20);
 }
 
 }  // namespace
