@@ -590,15 +590,20 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
 }
 
 // ---------------------------------------------------------------------------
-// The same coarse solve as one cooperative launch: one CTA per SM, the chain steps
-// separated by a grid-wide barrier instead of kernel boundaries.  Each warp takes one
-// matrix row per step (dot against the step's input vectors, staged in shared memory)
-// and prefetches the rows of its next step into L2 before it waits at the barrier.
+// The same coarse solve as one cooperative launch, one CTA per SM.  After the gather there is
+// one grid-wide barrier; from then on every vector of the solve (W, V and x in slab order)
+// starts out "absent" (a signalling-NaN bit pattern, which no arithmetic result can equal) and
+// each chain step polls the entries it reads until their producers' values replace it.  A step
+// so waits only for its own inputs, at the cost of one L2 round trip, instead of a grid
+// barrier followed by a reload; each warp loads its matrix row into registers before it polls.
 // ---------------------------------------------------------------------------
 constexpr int COOP_THREADS = 512;
 constexpr int COOP_WARPS = COOP_THREADS / 32;
-// polls of the barrier word before a CTA gives up (well under a second in all)
+// polls of the barrier word, and of a solve vector (each after a ~64 ns sleep), before a CTA
+// gives up (well under a second in all)
 constexpr unsigned kCoopSpinLimit = 1u << 20;
+constexpr unsigned kFlowSpinLimit = 1u << 20;
+constexpr unsigned long long kAbsent = 0x7FF4DEADBEEF0001ull;
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
@@ -606,6 +611,17 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 __device__ __forceinline__ int ld_volatile_int(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ bool coop_has(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v)) != kAbsent;
+}
 
 // Grid-wide barrier with a bounded wait.  bar->count only grows within a launch: barrier
 // number i (1, 2, ...) is passed once it reaches i * gridDim.x, so an arrival is one
@@ -650,6 +666,41 @@ __device__ void coop_exit(CoopBarrier* bar) {
   }
 }
 
+// su[j] = g0[j] (j < m) and g1[j - m] (m <= j < n) once every one of them is present; called
+// by the whole CTA.  False (in every thread) once this CTA or another one gave up.
+__device__ bool coop_wait_vector(double* su, const double* g0, const double* g1, int m, int n, CoopBarrier* bar) {
+  for (unsigned it = 0;; ++it) {
+    bool ok = true;
+    for (int j = threadIdx.x; j < n; j += COOP_THREADS) {
+      if (it == 0 || !coop_has(su[j])) {
+        const double v = ld_relaxed_f64(j < m ? g0 + j : g1 + (j - m));
+        su[j] = v;
+        ok = ok && coop_has(v);
+      }
+    }
+    if (__syncthreads_and(ok)) return true;
+    const int bad = threadIdx.x == 0 && (it >= kFlowSpinLimit || ld_volatile_int(&bar->err));
+    if (__syncthreads_or(bad)) {
+      if (threadIdx.x == 0) atomicExch(&bar->err, 1);
+      return false;
+    }
+    __nanosleep(64);
+  }
+}
+
+// one entry, polled by one thread (0.0 once the wait gave up; the error word is then set)
+__device__ double coop_wait_value(const double* p, CoopBarrier* bar) {
+  for (unsigned it = 0;; ++it) {
+    const double v = ld_relaxed_f64(p);
+    if (coop_has(v)) return v;
+    if (it >= kFlowSpinLimit || ld_volatile_int(&bar->err)) {
+      atomicExch(&bar->err, 1);
+      return 0.0;
+    }
+    __nanosleep(64);
+  }
+}
+
 // Dot of one matrix row with a shared-memory vector by one warp.  The row is read in
 // pieces of 32 x 32 elements whose loads are all issued before the first use, so a row
 // of up to 1024 entries costs one memory round trip.
@@ -675,14 +726,7 @@ __device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const 
   return warp_sum(a0 + a1);
 }
 
-template <typename TM>
-__device__ __forceinline__ void warp_prefetch_row(const TM* Mr, int m, int lane) {
-  const char* p = reinterpret_cast<const char*>(Mr);
-  const int bytes = m * int(sizeof(TM));
-  for (int off = lane * 128; off < bytes; off += 32 * 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
-}
-
-// One chain step: up to two independent row blocks y = a - M u (M: m x m), both staged.
+// One chain step: up to two independent row blocks y = a - M u (M: m x m).
 struct ChainOp {
   const void* M;
   const double* u;
@@ -690,21 +734,14 @@ struct ChainOp {
   double* y;
 };
 
+// The warp's first row (up to 1024 entries) is loaded into registers before the step's input
+// vectors are polled into su, so the two memory round trips overlap; results are stored as
+// strong (relaxed) writes, which the next step's pollers observe.  a_polled: the a vector
+// is itself produced during the launch (V in the backward chains).
 // (op[0] / op[1] picked by value so the descriptors stay in registers)
 template <typename TM>
-__device__ __forceinline__ void chain_prefetch(const ChainOp (&op)[2], int nop, int m, int gw, int nw, int lane) {
-  for (int r = gw; r < nop * m; r += nw) {
-    const int o = r >= m ? 1 : 0, rr = r - o * m;
-    const ChainOp c = o ? op[1] : op[0];
-    warp_prefetch_row(static_cast<const TM*>(c.M) + int64_t(rr) * m, m, lane);
-  }
-}
-
-template <typename TM>
-__device__ __forceinline__ void chain_step(const ChainOp (&op)[2], int nop, int m, double* su, int gw, int nw,
-                                           int lane) {
-  // the warp's first row (up to 1024 entries) is requested before the input vectors are
-  // staged, so the two memory round trips overlap
+__device__ __forceinline__ bool chain_step(const ChainOp (&op)[2], int nop, int m, double* su, int gw, int nw,
+                                           int lane, bool a_polled, CoopBarrier* bar) {
   constexpr int PIECE = 32;
   TM v[PIECE];
   const int r0 = gw;
@@ -717,8 +754,19 @@ __device__ __forceinline__ void chain_step(const ChainOp (&op)[2], int nop, int 
     const int j = lane + 32 * i;
     v[i] = (have && j < m) ? __ldg(M0 + j) : TM(0);
   }
-  for (int j = threadIdx.x; j < nop * m; j += COOP_THREADS) su[j] = __ldcg((j >= m ? op[1].u - m : op[0].u) + j);
-  __syncthreads();
+  // the first row's a entry too: it does not depend on this step's inputs
+  double a_first = 0.0;
+  if (have && lane == 0) {
+    const double* pa = c0.a + (r0 - o0 * m);
+    a_first = a_polled ? coop_wait_value(pa, bar) : __ldcg(pa);
+  }
+  if (!coop_wait_vector(su, op[0].u, nop > 1 ? op[1].u : op[0].u, m, nop * m, bar)) return false;
+  auto finish = [&](const ChainOp& c, int rr, double d) {
+    if (lane == 0) {
+      const double a = a_polled ? coop_wait_value(c.a + rr, bar) : __ldcg(c.a + rr);
+      st_relaxed_f64(c.y + rr, a - d);
+    }
+  };
   if (have) {
     const double* u = su + o0 * m;
     double a0 = 0.0, a1 = 0.0;
@@ -733,14 +781,14 @@ __device__ __forceinline__ void chain_step(const ChainOp (&op)[2], int nop, int 
       if (j < m) a0 = fma(double(__ldg(M0 + j)), u[j], a0);
     }
     const double d = warp_sum(a0 + a1);
-    if (lane == 0) c0.y[r0 - o0 * m] = __ldcg(c0.a + (r0 - o0 * m)) - d;
+    if (lane == 0) st_relaxed_f64(c0.y + (r0 - o0 * m), a_first - d);
   }
   for (int r = gw + nw; r < nop * m; r += nw) {
     const int o = r >= m ? 1 : 0, rr = r - o * m;
     const ChainOp c = o ? op[1] : op[0];
-    const double d = warp_row_dot(static_cast<const TM*>(c.M) + int64_t(rr) * m, su + o * m, m, lane);
-    if (lane == 0) c.y[rr] = __ldcg(c.a + rr) - d;
+    finish(c, rr, warp_row_dot(static_cast<const TM*>(c.M) + int64_t(rr) * m, su + o * m, m, lane));
   }
+  return true;
 }
 
 // forward step k: top W_{k+1} = bs_{k+1} - L_k W_k; bottom W_s = bs_s - U_s W_{s+1}, s = ns-2-k
@@ -796,7 +844,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
                       const TM* __restrict__ XT, const T* __restrict__ b, double* bs, double* W, double* V,
                       double* xs, T* __restrict__ x, const PcgScalars* sc, CoopBarrier* bar) {
   if (sc && sc->done) return;
-  extern __shared__ double su[];  // 2 m doubles
+  extern __shared__ double su_all[];  // two buffers of 2 m doubles, alternating by step
   const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
   const int nsteps = max(ntop, nbot);
   const int64_t mm = int64_t(m) * m, N = int64_t(ns) * m;
@@ -804,11 +852,18 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * COOP_WARPS + warp, nw = gridDim.x * COOP_WARPS;
   const int64_t tid = int64_t(blockIdx.x) * COOP_THREADS + threadIdx.x, nth = int64_t(gridDim.x) * COOP_THREADS;
+  const double absent = __longlong_as_double(static_cast<long long>(kAbsent));
+  int sbuf = 0;
+  auto next_su = [&]() {
+    double* p = su_all + sbuf * 2 * m;
+    sbuf ^= 1;
+    return p;
+  };
   ChainOp op[2];
-  int nop;
   unsigned epoch = 0;
 
-  // gather into slab order; chain heads (and a lone middle slab) take b directly
+  // gather into slab order (chain heads and a lone middle slab take b directly); every other
+  // entry of the solve vectors starts absent
   for (int64_t t = tid; t < N; t += nth) {
     const int s = int(t / m), row = int(t - int64_t(s) * m);
     const int c = row / 3, k = row - 3 * c;
@@ -816,10 +871,11 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
     const double v = double(b[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride]);
     bs[t] = v;
-    if ((s == 0 && ntop > 0) || (s == ns - 1 && nbot > 0) || (ntop == 0 && nbot == 0)) W[t] = v;
+    const bool head = (s == 0 && ntop > 0) || (s == ns - 1 && nbot > 0) || (ntop == 0 && nbot == 0);
+    W[t] = head ? v : absent;
+    V[t] = absent;
+    xs[t] = absent;
   }
-  nop = forward_ops(0, si, X, bs, W, op);
-  chain_prefetch<TM>(op, nop, m, gw, nw, lane);
   if (!coop_barrier(bar, epoch)) {
     coop_exit(bar);
     return;
@@ -827,34 +883,29 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
 
   // forward chains toward the middle
   for (int k = 0; k + 1 < nsteps; ++k) {
-    nop = forward_ops(k, si, X, bs, W, op);
-    chain_step<TM>(op, nop, m, su, gw, nw, lane);
-    ChainOp nx[2];
-    const int nn = forward_ops(k + 1, si, X, bs, W, nx);
-    chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
-    if (!coop_barrier(bar, epoch)) {
-    coop_exit(bar);
-    return;
-  }
+    const int nop = forward_ops(k, si, X, bs, W, op);
+    if (!chain_step<TM>(op, nop, m, next_su(), gw, nw, lane, false, bar)) {
+      coop_exit(bar);
+      return;
+    }
   }
   // middle slab: W_mid = b_mid - L_{mid-1} W_{mid-1} - U_mid W_{mid+1}
   if (ntop > 0 || nbot > 0) {
     const ChainOp up{X + (mid - 1) * mm, W + int64_t(mid - 1) * m, nullptr, nullptr};
     const ChainOp dn{X + mid * mm, W + int64_t(mid + 1) * m, nullptr, nullptr};
-    nop = (ntop > 0) + (nbot > 0);
+    const int nop = (ntop > 0) + (nbot > 0);
     op[0] = ntop > 0 ? up : dn;
     op[1] = dn;
-    for (int j = threadIdx.x; j < nop * m; j += COOP_THREADS) su[j] = __ldcg((j >= m ? op[1].u - m : op[0].u) + j);
-    __syncthreads();
+    double* su = next_su();
+    if (!coop_wait_vector(su, op[0].u, op[1].u, m, nop * m, bar)) {
+      coop_exit(bar);
+      return;
+    }
     for (int r = gw; r < m; r += nw) {
       double d = warp_row_dot(static_cast<const TM*>(op[0].M) + int64_t(r) * m, su, m, lane);
       if (nop > 1) d += warp_row_dot(static_cast<const TM*>(op[1].M) + int64_t(r) * m, su + m, m, lane);
-      if (lane == 0) W[int64_t(mid) * m + r] = __ldcg(bs + int64_t(mid) * m + r) - d;
+      if (lane == 0) st_relaxed_f64(W + int64_t(mid) * m + r, __ldcg(bs + int64_t(mid) * m + r) - d);
     }
-    if (!coop_barrier(bar, epoch)) {
-    coop_exit(bar);
-    return;
-  }
   }
   // V_s = Inv_s W_s for all slabs, each CTA over a contiguous row range; x_mid = V_mid
   {
@@ -862,39 +913,29 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     for (int64_t rs = r0; rs < r1;) {
       const int s = int(rs / m);
       const int64_t re = min(r1, int64_t(s + 1) * m);
-      for (int j = threadIdx.x; j < m; j += COOP_THREADS) su[j] = __ldcg(W + int64_t(s) * m + j);
-      __syncthreads();
+      double* su = next_su();
+      if (!coop_wait_vector(su, W + int64_t(s) * m, W + int64_t(s) * m, m, m, bar)) {
+        coop_exit(bar);
+        return;
+      }
       for (int64_t r = rs + warp; r < re; r += COOP_WARPS) {
         const int rr = int(r - int64_t(s) * m);
         const double d = warp_row_dot(Inv + s * mm + int64_t(rr) * m, su, m, lane);
         if (lane == 0) {
-          V[r] = d;
-          if (s == mid) xs[r] = d;
+          st_relaxed_f64(V + r, d);
+          if (s == mid) st_relaxed_f64(xs + r, d);
         }
       }
-      __syncthreads();
       rs = re;
     }
   }
-  nop = backward_ops(0, si, XT, V, xs, op);
-  chain_prefetch<TM>(op, nop, m, gw, nw, lane);
-  if (!coop_barrier(bar, epoch)) {
-    coop_exit(bar);
-    return;
-  }
   // backward chains outward from the middle
   for (int k = 0; k < nsteps; ++k) {
-    nop = backward_ops(k, si, XT, V, xs, op);
-    chain_step<TM>(op, nop, m, su, gw, nw, lane);
-    if (k + 1 < nsteps) {
-      ChainOp nx[2];
-      const int nn = backward_ops(k + 1, si, XT, V, xs, nx);
-      chain_prefetch<TM>(nx, nn, m, gw, nw, lane);
+    const int nop = backward_ops(k, si, XT, V, xs, op);
+    if (!chain_step<TM>(op, nop, m, next_su(), gw, nw, lane, true, bar)) {
+      coop_exit(bar);
+      return;
     }
-    if (!coop_barrier(bar, epoch)) {
-    coop_exit(bar);
-    return;
-  }
   }
   // scatter to the grid
   for (int64_t t = tid; t < N; t += nth) {
@@ -902,7 +943,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     const int c = row / 3, k = row - 3 * c;
     int gy, gx, gz;
     slab_node(g, si, s, c % si.nu, c / si.nu, gy, gx, gz);
-    x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(__ldcg(xs + t));
+    x[gy + int64_t(nny) * (gx + int64_t(nnx) * gz) + k * g.stride] = T(coop_wait_value(xs + t, bar));
   }
   coop_exit(bar);
 }
@@ -913,7 +954,7 @@ int slab_solve_coop_ctas(int m) {
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   if (!coop) return 0;
-  const size_t smem = size_t(2) * m * sizeof(double);
+  const size_t smem = size_t(4) * m * sizeof(double);
   if (smem > size_t(200) * 1024) return 0;
   const void* kernels[2] = {reinterpret_cast<const void*>(&k_slab_solve_coop<double, double>),
                             reinterpret_cast<const void*>(&k_slab_solve_coop<float, float>)};
@@ -933,7 +974,7 @@ void launch_slab_solve_coop(cudaStream_t st, int nctas, Grid g, SlabInfo si, con
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(nctas));
   cfg.blockDim = dim3(COOP_THREADS);
-  cfg.dynamicSmemBytes = size_t(2) * si.m * sizeof(double);
+  cfg.dynamicSmemBytes = size_t(4) * si.m * sizeof(double);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
