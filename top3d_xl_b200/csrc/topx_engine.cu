@@ -225,9 +225,10 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     gf.nctas = gj_flow_ctas(coarse_coop);
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
-    // one cooperative launch pays off once the slab blocks are large; below that the chain of
-    // small launches is quicker (measured crossover between m = 507 and m = 867)
-    coopCtas = (coarse_coop && si.m > 600) ? slab_solve_coop_ctas(si.m) : 0;
+    // the cooperative solve beats the chain of small launches at every slab size measured
+    // (m = 75 .. 1875); below m = 600 a grid of 64 CTAs polls faster than one of every SM
+    coopCtas = coarse_coop ? slab_solve_coop_ctas(si.m) : 0;
+    if (coopCtas && si.m < 600) coopCtas = std::min(coopCtas, 64);
   }
   // ---- workspaces ------------------------------------------------------------
   {
