@@ -666,17 +666,17 @@ __device__ void coop_exit(CoopBarrier* bar) {
   }
 }
 
-// su[j] = g0[j] (j < m) and g1[j - m] (m <= j < n) once every one of them is present; called
-// by the whole CTA.  False (in every thread) once this CTA or another one gave up.
-__device__ bool coop_wait_vector(double* su, const double* g0, const double* g1, int m, int n, CoopBarrier* bar) {
+// su[j] = g0[j] (j < m) and g1[j - m] (m <= j < n), in the factors' type, once every one of them
+// is present; called by the whole CTA.  False (in every thread) once this CTA or another one
+// gave up.
+template <typename TS>
+__device__ bool coop_wait_vector(TS* su, const double* g0, const double* g1, int m, int n, CoopBarrier* bar) {
   for (unsigned it = 0;; ++it) {
     bool ok = true;
     for (int j = threadIdx.x; j < n; j += COOP_THREADS) {
-      if (it == 0 || !coop_has(su[j])) {
-        const double v = ld_relaxed_f64(j < m ? g0 + j : g1 + (j - m));
-        su[j] = v;
-        ok = ok && coop_has(v);
-      }
+      const double v = ld_relaxed_f64(j < m ? g0 + j : g1 + (j - m));
+      su[j] = TS(v);
+      ok = ok && coop_has(v);
     }
     if (__syncthreads_and(ok)) return true;
     const int bad = threadIdx.x == 0 && (it >= kFlowSpinLimit || ld_volatile_int(&bar->err));
@@ -703,12 +703,12 @@ __device__ double coop_wait_value(const double* p, CoopBarrier* bar) {
 
 // Dot of one matrix row with a shared-memory vector by one warp.  The row is read in
 // pieces of 32 x 32 elements whose loads are all issued before the first use, so a row
-// of up to 1024 entries costs one memory round trip.
+// of up to 1024 entries costs one memory round trip.  Each lane accumulates its ~m/32 terms
+// in the factors' type (FP32 factors: FP32 products, no conversions); the warp sum is FP64.
 template <typename TM>
-__device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const double* __restrict__ u, int m,
-                                               int lane) {
+__device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const TM* __restrict__ u, int m, int lane) {
   constexpr int PIECE = 32;
-  double a0 = 0.0, a1 = 0.0;
+  TM a0 = TM(0), a1 = TM(0);
   for (int base = 0; base < m; base += 32 * PIECE) {
     TM v[PIECE];
 #pragma unroll
@@ -719,11 +719,11 @@ __device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const 
 #pragma unroll
     for (int i = 0; i < PIECE; i += 2) {
       const int j = base + lane + 32 * i;
-      if (j < m) a0 = fma(double(v[i]), u[j], a0);
-      if (j + 32 < m) a1 = fma(double(v[i + 1]), u[j + 32], a1);
+      if (j < m) a0 = fma(v[i], u[j], a0);
+      if (j + 32 < m) a1 = fma(v[i + 1], u[j + 32], a1);
     }
   }
-  return warp_sum(a0 + a1);
+  return warp_sum(double(a0) + double(a1));
 }
 
 // One chain step: up to two independent row blocks y = a - M u (M: m x m).
@@ -740,7 +740,7 @@ struct ChainOp {
 // is itself produced during the launch (V in the backward chains).
 // (op[0] / op[1] picked by value so the descriptors stay in registers)
 template <typename TM>
-__device__ __forceinline__ bool chain_step(const ChainOp (&op)[2], int nop, int m, double* su, int gw, int nw,
+__device__ __forceinline__ bool chain_step(const ChainOp (&op)[2], int nop, int m, TM* su, int gw, int nw,
                                            int lane, bool a_polled, CoopBarrier* bar) {
   constexpr int PIECE = 32;
   TM v[PIECE];
@@ -768,19 +768,19 @@ __device__ __forceinline__ bool chain_step(const ChainOp (&op)[2], int nop, int 
     }
   };
   if (have) {
-    const double* u = su + o0 * m;
-    double a0 = 0.0, a1 = 0.0;
+    const TM* u = su + o0 * m;
+    TM a0 = TM(0), a1 = TM(0);
 #pragma unroll
     for (int i = 0; i < PIECE; i += 2) {
       const int j = lane + 32 * i;
-      if (j < m) a0 = fma(double(v[i]), u[j], a0);
-      if (j + 32 < m) a1 = fma(double(v[i + 1]), u[j + 32], a1);
+      if (j < m) a0 = fma(v[i], u[j], a0);
+      if (j + 32 < m) a1 = fma(v[i + 1], u[j + 32], a1);
     }
     for (int base = 32 * PIECE; base < m; base += 32) {
       const int j = base + lane;
-      if (j < m) a0 = fma(double(__ldg(M0 + j)), u[j], a0);
+      if (j < m) a0 = fma(__ldg(M0 + j), u[j], a0);
     }
-    const double d = warp_sum(a0 + a1);
+    const double d = warp_sum(double(a0) + double(a1));
     if (lane == 0) st_relaxed_f64(c0.y + (r0 - o0 * m), a_first - d);
   }
   for (int r = gw + nw; r < nop * m; r += nw) {
@@ -844,7 +844,8 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
                       const TM* __restrict__ XT, const T* __restrict__ b, double* bs, double* W, double* V,
                       double* xs, T* __restrict__ x, const PcgScalars* sc, CoopBarrier* bar) {
   if (sc && sc->done) return;
-  extern __shared__ double su_all[];  // two buffers of 2 m doubles, alternating by step
+  extern __shared__ double su_dyn[];  // two buffers of 2 m entries, alternating by step
+  TM* const su_all = reinterpret_cast<TM*>(su_dyn);
   const int m = si.m, ns = si.ns, mid = ns / 2, ntop = mid, nbot = ns - 1 - mid;
   const int nsteps = max(ntop, nbot);
   const int64_t mm = int64_t(m) * m, N = int64_t(ns) * m;
@@ -855,7 +856,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
   const double absent = __longlong_as_double(static_cast<long long>(kAbsent));
   int sbuf = 0;
   auto next_su = [&]() {
-    double* p = su_all + sbuf * 2 * m;
+    TM* p = su_all + sbuf * 2 * m;
     sbuf ^= 1;
     return p;
   };
@@ -896,7 +897,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     const int nop = (ntop > 0) + (nbot > 0);
     op[0] = ntop > 0 ? up : dn;
     op[1] = dn;
-    double* su = next_su();
+    TM* su = next_su();
     if (!coop_wait_vector(su, op[0].u, op[1].u, m, nop * m, bar)) {
       coop_exit(bar);
       return;
@@ -913,7 +914,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     for (int64_t rs = r0; rs < r1;) {
       const int s = int(rs / m);
       const int64_t re = min(r1, int64_t(s + 1) * m);
-      double* su = next_su();
+      TM* su = next_su();
       if (!coop_wait_vector(su, W + int64_t(s) * m, W + int64_t(s) * m, m, m, bar)) {
         coop_exit(bar);
         return;
