@@ -283,86 +283,102 @@ void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks
 // formed explicitly (blocked Gauss-Jordan exchange, FP64), so a solve is a
 // short chain of dense GEMVs on all SMs.
 // ---------------------------------------------------------------------------
-struct SchurOp {
-  const double* A;
-  double* S;
-  const double* Lt;  // L_{s-1} (top term), or null
-  const double* Bt;  // Bup_{s-1}
-  const double* Ub;  // U_s (bottom term), or null
-  const double* Bb;  // Bup_s
+// Y[r][:] = sum_t coef_t(r) src[idx_t(r)][:] over the 27-point coupling stencil B of the slab
+// pair, for the rows r of one CTA: the rows' (coefficient, source row) lists are built once in
+// shared memory and the columns are swept with coalesced loads.  Two stencil kinds:
+//   kind 0: r = DOF (c, k) of the upper slab, terms a in the lower slab around c:
+//           coef = B[a][(du+1) + 3 (dv+1)][i][k], source row 3a + i   ((du, dv) = c - a)
+//   kind 1: r = DOF (c, k) of the lower slab, terms n in the upper slab around c:
+//           coef = B[c][(du+1) + 3 (dv+1)][k][q], source row 3n + q   ((du, dv) = n - c)
+// An op takes up to two terms (the middle slab's Schur complement), summed in one FMA chain in
+// the order (dv, du, i) of each term, first term first.
+struct RowCombOp {
+  const double* src[2];  // m x m row-major sources (src[1] optional)
+  const double* B[2];    // their stencils
+  int kind[2];
+  double* Y;
 };
+constexpr int RC_ROWS = 4, RC_THREADS = 256, RC_TERMS = 54;
 
-__global__ void k_schur(SlabInfo si, SchurOp op0, SchurOp op1) {
-  const SchurOp op = blockIdx.y == 0 ? op0 : op1;
-  const int64_t m = si.m;
-  const int64_t N = m * m;
-  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t row = t / m, col = t % m;
-    const int b = int(col / 3), jc = int(col % 3);
-    const int ub = b % si.nu, vb = b / si.nu;
-    double s = 0.0;
-    if (op.Lt) {  // (L_{s-1} B_{s-1})[row][col]: col is DOF (b, jc) of slab s, neighbours a in slab s-1
-      for (int dv = -1; dv <= 1; ++dv)
-        for (int du = -1; du <= 1; ++du) {
-          const int ua = ub - du, va = vb - dv;
-          if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
-          const int a = ua + si.nu * va;
-          const double* Bb = op.Bt + int64_t(a) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
-          for (int i = 0; i < 3; ++i) s = fma(op.Lt[row * m + 3 * a + i], Bb[i * 3 + jc], s);
+__device__ int rc_terms(const SlabInfo& si, int kind, const double* B, const double* src, int r, double* coef,
+                        const double** row) {
+  const int m = si.m, c = r / 3, k = r - 3 * c, uc = c % si.nu, vc = c / si.nu;
+  int n = 0;
+  for (int dv = -1; dv <= 1; ++dv)
+    for (int du = -1; du <= 1; ++du) {
+      if (kind == 0) {
+        const int ua = uc - du, va = vc - dv;
+        if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
+        const int aa = ua + si.nu * va;
+        const double* Bb = B + int64_t(aa) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
+        for (int i = 0; i < 3; ++i) {
+          coef[n] = Bb[i * 3 + k];
+          row[n++] = src + (3 * int64_t(aa) + i) * m;
         }
-    }
-    if (op.Ub) {  // (U_s B_s^T)[row][col]: col is DOF (b, jc) of slab s, neighbours c in slab s+1
-      const double* Bc = op.Bb + int64_t(b) * 81;
-      for (int dv = -1; dv <= 1; ++dv)
-        for (int du = -1; du <= 1; ++du) {
-          const int uc = ub + du, vc = vb + dv;
-          if (uc < 0 || uc >= si.nu || vc < 0 || vc >= si.nv) continue;
-          const int c = uc + si.nu * vc;
-          const double* Bn = Bc + ((du + 1) + 3 * (dv + 1)) * 9;
-          for (int k = 0; k < 3; ++k) s = fma(op.Ub[row * m + 3 * c + k], Bn[jc * 3 + k], s);
-        }
-    }
-    op.S[t] = op.A[t] - s;
-  }
-}
-
-struct FormOp {
-  const double* Bp;    // Bup_s
-  const double* Inv;   // S_s^{-1} (kind 0) or T_{s+1}^{-1} (kind 1)
-  double* X;           // L_s (kind 0) or U_s (kind 1)
-  double* XT;          // transpose
-  int kind;
-};
-
-// kind 0: L_s = B_s^T S_s^{-1}   (rows: DOFs of slab s+1, cols: slab s)
-// kind 1: U_s = B_s T_{s+1}^{-1} (rows: DOFs of slab s,   cols: slab s+1)
-__global__ void k_form(SlabInfo si, FormOp op0, FormOp op1) {
-  const FormOp op = blockIdx.y == 0 ? op0 : op1;
-  const int64_t m = si.m;
-  const int64_t N = m * m;
-  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < N; t += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t row = t / m, col = t % m;
-    const int c = int(row / 3), k = int(row % 3);
-    const int uc = c % si.nu, vc = c / si.nu;
-    double s = 0.0;
-    for (int dv = -1; dv <= 1; ++dv)
-      for (int du = -1; du <= 1; ++du) {
-        if (op.kind == 0) {
-          const int ua = uc - du, va = vc - dv;
-          if (ua < 0 || ua >= si.nu || va < 0 || va >= si.nv) continue;
-          const int a = ua + si.nu * va;
-          const double* Bb = op.Bp + int64_t(a) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
-          for (int i = 0; i < 3; ++i) s = fma(Bb[i * 3 + k], op.Inv[(3 * int64_t(a) + i) * m + col], s);
-        } else {
-          const int un = uc + du, vn = vc + dv;
-          if (un < 0 || un >= si.nu || vn < 0 || vn >= si.nv) continue;
-          const int n = un + si.nu * vn;
-          const double* Bn = op.Bp + int64_t(c) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
-          for (int q = 0; q < 3; ++q) s = fma(Bn[k * 3 + q], op.Inv[(3 * int64_t(n) + q) * m + col], s);
+      } else {
+        const int un = uc + du, vn = vc + dv;
+        if (un < 0 || un >= si.nu || vn < 0 || vn >= si.nv) continue;
+        const int nn = un + si.nu * vn;
+        const double* Bn = B + int64_t(c) * 81 + ((du + 1) + 3 * (dv + 1)) * 9;
+        for (int q = 0; q < 3; ++q) {
+          coef[n] = Bn[k * 3 + q];
+          row[n++] = src + (3 * int64_t(nn) + q) * m;
         }
       }
-    op.X[t] = s;
-    op.XT[col * m + row] = s;
+    }
+  return n;
+}
+
+__global__ void __launch_bounds__(RC_THREADS) k_rowcomb(SlabInfo si, RowCombOp op0, RowCombOp op1) {
+  const RowCombOp op = blockIdx.y == 0 ? op0 : op1;
+  const int m = si.m, r0 = blockIdx.x * RC_ROWS;
+  __shared__ double scoef[RC_ROWS][RC_TERMS];
+  __shared__ const double* srow[RC_ROWS][RC_TERMS];
+  __shared__ int scnt[RC_ROWS];
+  if (threadIdx.x < RC_ROWS) {
+    const int r = r0 + threadIdx.x;
+    int n = 0;
+    if (r < m)
+      for (int t = 0; t < 2; ++t)
+        if (op.src[t]) n += rc_terms(si, op.kind[t], op.B[t], op.src[t], r, &scoef[threadIdx.x][n], &srow[threadIdx.x][n]);
+    scnt[threadIdx.x] = n;
+  }
+  __syncthreads();
+  for (int col = threadIdx.x; col < m; col += RC_THREADS)
+    for (int rr = 0; rr < RC_ROWS; ++rr) {
+      const int r = r0 + rr;
+      if (r >= m) break;
+      double acc = 0.0;
+      const int n = scnt[rr];
+      for (int t = 0; t < n; ++t) acc = fma(scoef[rr][t], srow[rr][t][col], acc);
+      op.Y[int64_t(r) * m + col] = acc;
+    }
+}
+
+// D[r][c] = (A ? A[r][c] : 0) - / + Y[c][r] over 32 x 32 tiles staged in shared memory
+// (sub: D = A - Y^T for a Schur complement, Y null -> D = A; copy: D = Y^T)
+struct TransOp {
+  const double* A;
+  const double* Y;
+  double* D;
+};
+__global__ void __launch_bounds__(256) k_transpose_tiles(int m, TransOp op0, TransOp op1, int sub) {
+  const TransOp op = blockIdx.z == 0 ? op0 : op1;
+  __shared__ double t[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (op.Y)
+    for (int j = ty; j < 32; j += 8) {
+      const int r = by + j, c = bx + tx;  // Y[r][c], r: rows of Y = columns of D
+      t[j][tx] = (r < m && c < m) ? op.Y[int64_t(r) * m + c] : 0.0;
+    }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int r = bx + j, c = by + tx;  // D[r][c] = ... Y[c][r] = t[tx][j]
+    if (r >= m || c >= m) continue;
+    const int64_t k = int64_t(r) * m + c;
+    const double y = op.Y ? t[tx][j] : 0.0;
+    op.D[k] = sub ? op.A[k] - y : y;
   }
 }
 
@@ -376,43 +392,77 @@ void launch_slab_factor(cudaStream_t st, const GJFlow& gf, SlabInfo si, const do
   const int m = si.m, ns = si.ns, mid = ns / 2;
   const int64_t mm = int64_t(m) * m;
   const int64_t bs = int64_t(si.nu) * si.nv * 81;
-  const unsigned nbm = grid1d(mm, 256);
+  const unsigned nrc = unsigned((m + RC_ROWS - 1) / RC_ROWS), nt32 = unsigned((m + 31) / 32);
   auto invert = [&](int nset, double* A0, double* A1) {
     launch_gj_flow(st, m, nset, A0, A1, gf.tasks[nset - 1], gf.ntasks[nset - 1], gf.scratch, gf.ctrl, gf.nctas);
   };
+  // S = A - Y^T with Y = (sum of the coupling terms)^T by rows (ops without a term copy A)
+  auto schur = [&](int nset, const RowCombOp (&ro)[2], const TransOp (&to)[2]) {
+    int nrow = 0;
+    RowCombOp rc[2] = {};
+    for (int i = 0; i < nset; ++i)
+      if (ro[i].src[0]) rc[nrow++] = ro[i];
+    if (nrow) (k_rowcomb<<<dim3(nrc, nrow), RC_THREADS, 0, st>>>(si, rc[0], rc[1]), topx::count_launch());
+    (k_transpose_tiles<<<dim3(nt32, nt32, nset), 256, 0, st>>>(m, to[0], to[1], 1), topx::count_launch());
+  };
   const int ntop = mid, nbot = ns - 1 - mid;
   for (int k = 0; k < std::max(ntop, nbot); ++k) {
-    SchurOp so[2] = {};
-    FormOp fo[2] = {};
+    RowCombOp ro[2] = {}, fo[2] = {};
+    TransOp to[2] = {}, ft[2] = {};
     double* inv[2] = {nullptr, nullptr};
     int nset = 0, nform = 0;
-    if (k < ntop) {  // top slab k
+    if (k < ntop) {  // top slab k: S_k = A_k - L_{k-1} B_{k-1}
       const int s = k;
-      so[nset] = SchurOp{A + s * mm, Sinv + s * mm, s ? X + (s - 1) * mm : nullptr, s ? Bup + (s - 1) * bs : nullptr,
-                         nullptr, nullptr};
+      double* Y = gf.ytmp + nset * mm;
+      if (s) ro[nset] = RowCombOp{{XT + (s - 1) * mm, nullptr}, {Bup + (s - 1) * bs, nullptr}, {0, 0}, Y};
+      to[nset] = TransOp{A + s * mm, s ? Y : nullptr, Sinv + s * mm};
       inv[nset++] = Sinv + s * mm;
     }
-    if (k < nbot) {  // bottom slab ns-1-k
+    if (k < nbot) {  // bottom slab s = ns-1-k: T_s = A_s - U_s B_s^T
       const int s = ns - 1 - k;
-      so[nset] = SchurOp{A + s * mm, Sinv + s * mm, nullptr, nullptr, k ? X + s * mm : nullptr, k ? Bup + s * bs : nullptr};
+      double* Y = gf.ytmp + nset * mm;
+      if (k) ro[nset] = RowCombOp{{XT + s * mm, nullptr}, {Bup + s * bs, nullptr}, {1, 0}, Y};
+      to[nset] = TransOp{A + s * mm, k ? Y : nullptr, Sinv + s * mm};
       inv[nset++] = Sinv + s * mm;
     }
-    (k_schur<<<dim3(nbm, nset), 256, 0, st>>>(si, so[0], so[1]), topx::count_launch());
+    schur(nset, ro, to);
     invert(nset, inv[0], inv[1]);
     if (k < ntop) {  // L_k = B_k^T S_k^{-1}
-      fo[nform++] = FormOp{Bup + k * bs, Sinv + k * mm, X + k * mm, XT + k * mm, 0};
+      fo[nform] = RowCombOp{{Sinv + k * mm, nullptr}, {Bup + k * bs, nullptr}, {0, 0}, X + k * mm};
+      ft[nform++] = TransOp{nullptr, X + k * mm, XT + k * mm};
     }
     if (k < nbot) {  // U_{s-1} = B_{s-1} T_s^{-1}, s = ns-1-k
       const int s = ns - 1 - k;
-      fo[nform++] = FormOp{Bup + (s - 1) * bs, Sinv + s * mm, X + (s - 1) * mm, XT + (s - 1) * mm, 1};
+      fo[nform] = RowCombOp{{Sinv + s * mm, nullptr}, {Bup + (s - 1) * bs, nullptr}, {1, 0}, X + (s - 1) * mm};
+      ft[nform++] = TransOp{nullptr, X + (s - 1) * mm, XT + (s - 1) * mm};
     }
-    if (nform) (k_form<<<dim3(nbm, nform), 256, 0, st>>>(si, fo[0], fo[1]), topx::count_launch());
+    if (nform) {
+      (k_rowcomb<<<dim3(nrc, nform), RC_THREADS, 0, st>>>(si, fo[0], fo[1]), topx::count_launch());
+      (k_transpose_tiles<<<dim3(nt32, nt32, nform), 256, 0, st>>>(m, ft[0], ft[1], 0), topx::count_launch());
+    }
   }
-  // middle slab
-  SchurOp sm{A + mid * mm, Sinv + mid * mm, mid > 0 ? X + (mid - 1) * mm : nullptr,
-             mid > 0 ? Bup + (mid - 1) * bs : nullptr, mid < ns - 1 ? X + mid * mm : nullptr,
-             mid < ns - 1 ? Bup + mid * bs : nullptr};
-  (k_schur<<<dim3(nbm, 1), 256, 0, st>>>(si, sm, sm), topx::count_launch());
+  // middle slab: M = A_mid - L_{mid-1} B_{mid-1} - U_mid B_mid^T (top term first)
+  {
+    RowCombOp ro[2] = {};
+    TransOp to[2] = {};
+    const bool up = mid > 0, dn = mid < ns - 1;
+    if (up || dn) {
+      ro[0].Y = gf.ytmp;
+      int t = 0;
+      if (up) {
+        ro[0].src[t] = XT + (mid - 1) * mm;
+        ro[0].B[t] = Bup + (mid - 1) * bs;
+        ro[0].kind[t++] = 0;
+      }
+      if (dn) {
+        ro[0].src[t] = XT + mid * mm;
+        ro[0].B[t] = Bup + mid * bs;
+        ro[0].kind[t++] = 1;
+      }
+    }
+    to[0] = TransOp{A + mid * mm, (up || dn) ? gf.ytmp : nullptr, Sinv + mid * mm};
+    schur(1, ro, to);
+  }
   invert(1, Sinv + mid * mm, nullptr);
   TOPX_CUDA_OK(cudaGetLastError());
 }

@@ -219,8 +219,10 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     }
     gfScr.alloc(gf_scratch_doubles(si.m), false);
     gfCtrl.alloc(gf_ctrl_words(si.m));
+    gfY.alloc(2 * mm, false);
     gf.scratch = gfScr.p;
     gf.ctrl = gfCtrl.p;
+    gf.ytmp = gfY.p;
     // an engine alone on the GPU fills it; engines sharing it leave room for their neighbours
     gf.nctas = gj_flow_ctas(coarse_coop);
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);

@@ -198,7 +198,7 @@ class Engine {
   DevBuf<double> fl_F;
   int nflag = 0;
   SlabInfo si;
-  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gfScr;
+  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gfScr, gfY;
   DevBuf<uint32_t> gfTasks[2];  // inverse task plans for one and two matrices
   DevBuf<unsigned> gfCtrl;      // control words of the inverse (word 0: error flag)
   DevBuf<float> slabSinv32, slabL32, slabLT32;  // FP32 copies applied by the mixed-precision V-cycle

@@ -106,6 +106,7 @@ struct GJFlow {
   double* scratch;
   unsigned* ctrl;
   int nctas;
+  double* ytmp;  // 2 m x m: the coupling terms of the Schur complements, by rows, before transposition
 };
 // one-time per-device kernel attributes (call outside stream capture)
 void prepare_gj_flow();

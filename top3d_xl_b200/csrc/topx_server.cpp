@@ -46,7 +46,7 @@ int64_t footprint_estimate(const topx_info& in, int precision) {
   int64_t d[3] = {in.resY[L] + 1, in.resX[L] + 1, in.resZ[L] + 1};
   std::sort(d, d + 3);
   const int64_t ns = d[2], m = 3 * d[0] * d[1];
-  const int64_t slab = (2 * ns + 2 * (ns - 1)) * m * m * 8 + (precision == TOPX_MIXED ? 3 * ns * m * m * 4 : 0);
+  const int64_t slab = (2 * ns + 2 * (ns - 1) + 2) * m * m * 8 + (precision == TOPX_MIXED ? 3 * ns * m * m * 4 : 0);
   // the Gauss-Jordan inverse's ring scratch, control words and task plans (~nt^3 tasks each)
   const int64_t nt = topx::gf_tiles(int(m));
   const int64_t inverse = int64_t(topx::gf_scratch_doubles(int(m))) * 8 + int64_t(topx::gf_ctrl_words(int(m))) * 4 +
