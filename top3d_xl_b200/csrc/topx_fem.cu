@@ -120,10 +120,11 @@ __device__ __forceinline__ void ku_fetch(const T* __restrict__ in, const T* __re
 
 // Accumulate, for the four hexes on one side of the node plane (upper: oz = 0,
 // lower: oz = -1), the node's 3 rows of Ke times the hex's 24 DOFs, then add
-// E_e * acc to y in the reference's local-node order.
-template <typename T, int OZ>
-__device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], const T (*const el[2])[KY + 1],
-                                        int tx, int ty, T (&y)[3]) {
+// E_e * acc to y in the reference's local-node order.  PL(dz, c, dx, dy) is the (masked)
+// value of component c of the neighbour at offset (dy, dx, dz); EL(oz, ox, oy) the modulus of
+// the hex whose lowest corner is at offset (oy, ox, oz).
+template <typename T, int OZ, typename FPL, typename FEL>
+__device__ __forceinline__ void ku_half(FPL&& PL, FEL&& EL, T (&y)[3]) {
   T acc[4][3];
 #pragma unroll
   for (int e = 0; e < 4; ++e) acc[e][0] = acc[e][1] = acc[e][2] = T(0);
@@ -133,9 +134,9 @@ __device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], 
     for (int dx = -1; dx <= 1; ++dx)
 #pragma unroll
       for (int dy = -1; dy <= 1; ++dy) {
-        const T u0 = pl[dz + 1][0][tx + 1 + dx][ty + 1 + dy];
-        const T u1 = pl[dz + 1][1][tx + 1 + dx][ty + 1 + dy];
-        const T u2 = pl[dz + 1][2][tx + 1 + dx][ty + 1 + dy];
+        const T u0 = PL(dz, 0, dx, dy);
+        const T u1 = PL(dz, 1, dx, dy);
+        const T u2 = PL(dz, 2, dx, dy);
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int oy = (e & 1) ? 0 : -1, ox = (e & 2) ? 0 : -1;
@@ -156,7 +157,7 @@ __device__ __forceinline__ void ku_half(const T (*const pl[3])[KX + 2][KY + 2], 
   for (int a = (OZ == 0 ? 0 : 4); a < (OZ == 0 ? 4 : 8); ++a) {
     const int oy = -hex_ly(a), ox = -hex_lx(a);
     const int e = (oy + 1) + 2 * (ox + 1);
-    const T Ee = el[OZ + 1][tx + 1 + ox][ty + 1 + oy];
+    const T Ee = EL(OZ, ox, oy);
 #pragma unroll
     for (int i = 0; i < 3; ++i) y[i] = fma(Ee, acc[e][i], y[i]);
   }
@@ -287,8 +288,10 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
       const T(*const pl[3])[KX + 2][KY + 2] = {su[k % 3], su[(k + 1) % 3], su[(k + 2) % 3]};
       const T(*const el[2])[KY + 1] = {se[k % 3], se[(k + 1) % 3]};
       T y[3] = {T(0), T(0), T(0)};
-      ku_half<T, 0>(pl, el, tx, ty, y);   // hexes above the node: local nodes 1-4
-      ku_half<T, -1>(pl, el, tx, ty, y);  // hexes below the node: local nodes 5-8
+      auto PL = [&](int dz, int c, int dx, int dy) { return pl[dz + 1][c][tx + 1 + dx][ty + 1 + dy]; };
+      auto EL = [&](int oz, int ox, int oy) { return el[oz + 1][tx + 1 + ox][ty + 1 + oy]; };
+      ku_half<T, 0>(PL, EL, y);   // hexes above the node: local nodes 1-4
+      ku_half<T, -1>(PL, EL, y);  // hexes below the node: local nodes 5-8
       // the node's own value: masked copy in the ring for free DOFs, unmasked for fixed ones
       T p[3] = {pl[1][0][tx + 1][ty + 1], pl[1][1][tx + 1][ty + 1], pl[1][2][tx + 1][ty + 1]};
       if (fbo) {
@@ -319,6 +322,93 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   if (MODE != KU_PLAIN) {
     double v[1] = {dot}, tot[1];
     if (reduce_publish<1>(v, rs, tot) && tid == 0) sc->pq = tot[0];
+  }
+}
+
+// The last node row y = ny of the grid, one thread per (x, z) node, when the tile kernel's
+// y-tiles end exactly at it: with ny a multiple of the tile height the tile kernel would
+// otherwise run whole tiles for this one row (node counts here are 2^k + 1).  Same operator,
+// same FMA order per node, neighbour values and moduli read directly; the p'q partial sum is
+// added to the tile kernel's.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_ku_l1_lastrow(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
+                                                       T* __restrict__ out, const T* __restrict__ E,
+                                                       const uint8_t* __restrict__ fixbits,
+                                                       const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs) {
+  if (MODE != KU_PLAIN && sc->done) return;
+  const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
+  const int64_t S = g.stride;
+  const bool first = (MODE != KU_PLAIN) && sc->first;
+  const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
+  const int Y = nny - 1;
+  double dot = 0.0;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < int64_t(nnx) * nnz;
+       t += int64_t(gridDim.x) * blockDim.x) {
+    const int x = int(t % nnx), z = int(t / nnx);
+    T nb[3][3][3][3];  // [dz+1][c][dx+1][dy+1], masked by the free bits, zero outside the grid
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int gy = Y + dy, gx = x + dx, gz = z + dz;
+          const bool ok = gy < nny && gx >= 0 && gx < nnx && gz >= 0 && gz < nnz;  // gy >= Y-1 >= 0
+          T v0 = T(0), v1 = T(0), v2 = T(0);
+          uint8_t fb = 0;
+          if (ok) {
+            const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
+            ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
+            fb = fixbits[n];
+          }
+          nb[dz + 1][0][dx + 1][dy + 1] = (fb & 1) ? T(0) : v0;
+          nb[dz + 1][1][dx + 1][dy + 1] = (fb & 2) ? T(0) : v1;
+          nb[dz + 1][2][dx + 1][dy + 1] = (fb & 4) ? T(0) : v2;
+        }
+    T em[2][2][2];  // [oz+1][ox+1][oy+1]: hexes around the node, zero outside the grid
+#pragma unroll
+    for (int oz = -1; oz <= 0; ++oz)
+#pragma unroll
+      for (int ox = -1; ox <= 0; ++ox)
+#pragma unroll
+        for (int oy = -1; oy <= 0; ++oy) {
+          const int ey = Y + oy, ex = x + ox, ez = z + oz;
+          const bool ok = ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz;
+          em[oz + 1][ox + 1][oy + 1] = ok ? E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)] : T(0);
+        }
+    T y[3] = {T(0), T(0), T(0)};
+    auto PL = [&](int dz, int c, int dx, int dy) { return nb[dz + 1][c][dx + 1][dy + 1]; };
+    auto EL = [&](int oz, int ox, int oy) { return em[oz + 1][ox + 1][oy + 1]; };
+    ku_half<T, 0>(PL, EL, y);
+    ku_half<T, -1>(PL, EL, y);
+    const int64_t n = Y + int64_t(nny) * (x + int64_t(nnx) * z);
+    const uint8_t fbo = fixbits[n];
+    T p[3] = {nb[1][0][1][1], nb[1][1][1][1], nb[1][2][1][1]};
+    if (fbo) {
+      T p0, p1, p2;
+      ku_fetch<T, MODE>(in, zin, n, S, first, beta, p0, p1, p2);
+      const T cf = cfix[n];
+      if (fbo & 1) {
+        p[0] = p0;
+        y[0] = cf * p0;
+      }
+      if (fbo & 2) {
+        p[1] = p1;
+        y[1] = cf * p1;
+      }
+      if (fbo & 4) {
+        p[2] = p2;
+        y[2] = cf * p2;
+      }
+    }
+    out[n] = y[0];
+    out[n + S] = y[1];
+    out[n + 2 * S] = y[2];
+    if (MODE != KU_PLAIN) dot += double(p[0]) * double(y[0]) + double(p[1]) * double(y[1]) + double(p[2]) * double(y[2]);
+  }
+  if (MODE != KU_PLAIN) {
+    double v[1] = {dot}, tot[1];
+    if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) sc->pq += tot[0];
   }
 }
 
@@ -358,13 +448,25 @@ template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
   (void)pout;
-  const int zc = ku_z_chunk(g.nny(), g.nnx(), g.nnz());
+  // y-tiles of the tile kernel; a last node row that would fill a tile on its own goes to
+  // k_ku_l1_lastrow instead
+  const bool lastrow = g.ny >= KY && g.ny % KY == 0;
+  const int rows = lastrow ? g.ny : g.nny();
+  const int zc = ku_z_chunk(rows, g.nnx(), g.nnz());
   dim3 blk(KY, KX, 1);
-  dim3 grd((g.nny() + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + zc - 1) / zc);
+  dim3 grd((rows + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + zc - 1) / zc);
   if (mode == KU_PLAIN)
     (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   else
     (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+  if (lastrow) {
+    const unsigned nb = unsigned((int64_t(g.nnx()) * g.nnz() + 255) / 256);
+    if (mode == KU_PLAIN)
+      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, 256, 0, st>>>(g, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    else
+      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, 256, 0, st>>>(g, in, z, out, E, fixbits, cfix, sc, rs),
+       topx::count_launch());
+  }
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
