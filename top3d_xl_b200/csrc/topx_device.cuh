@@ -169,6 +169,30 @@ __device__ __forceinline__ bool reduce_publish_max(double v, RedScratch rs, doub
   return true;
 }
 
+// Division of 32-bit unsigned integers by an invariant divisor d >= 1 through a multiply-high
+// and shifts (Granlund and Montgomery, "Division by invariant integers using multiplication",
+// 1994): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+//   q = (t + ((n - t) >> 1)) >> (l - 1),  t = mulhi(m, n)    (l >= 1; d = 1 returns n)
+// exact for every n < 2^32.
+struct FastDiv {
+  uint32_t d = 1, m = 0;
+  int l = 0;
+  FastDiv() = default;
+  explicit FastDiv(uint32_t dd) : d(dd) {
+    while ((uint64_t(1) << l) < d) ++l;
+    m = l == 0 ? 0u : uint32_t(((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1);
+  }
+  __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+    if (l == 0) return n;
+#ifdef __CUDA_ARCH__
+    const uint32_t t = __umulhi(m, n);
+#else
+    const uint32_t t = uint32_t((uint64_t(m) * n) >> 32);
+#endif
+    return (t + ((n - t) >> 1)) >> (l - 1);
+  }
+};
+
 // Local node index (0..7) of the node at corner (ly, lx, lz) of a hex, using
 // the reference's local numbering (TOP3D_XL.m:1697): node 1 = (y+1, x, z),
 // node 2 = (y+1, x+1, z), node 3 = (y, x+1, z), node 4 = (y, x, z), 5-8 = z+1.

@@ -613,14 +613,16 @@ void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, c
 // ---------------------------------------------------------------------------
 template <typename TI, typename T, int S, int AXIS>
 __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny, int inx, int inz,
-                                T* __restrict__ out, int64_t ostr, int ony, int onx, int onz) {
-  const int64_t N = int64_t(ony) * onx * onz;
-  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
-    const int oy = int(n % ony), ox = int((n / ony) % onx), oz = int(n / (int64_t(ony) * onx));
+                                T* __restrict__ out, int64_t ostr, int ony, int onx, int onz, FastDiv fdy,
+                                FastDiv fdx) {
+  const uint32_t N = uint32_t(ony) * onx * onz;
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    const uint32_t q = fdy.div(n), oz = fdx.div(q);
+    const int oy = int(n - q * uint32_t(ony)), ox = int(q - oz * uint32_t(onx));
     T acc[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int d = -(S - 1); d <= S - 1; ++d) {
-      int iy = oy, ix = ox, iz = oz;
+      int iy = oy, ix = ox, iz = int(oz);
       int lim;
       if (AXIS == 0) {
         iy = S * oy + d;
@@ -629,7 +631,7 @@ __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny
         ix = S * ox + d;
         lim = inx;
       } else {
-        iz = S * oz + d;
+        iz = S * int(oz) + d;
         lim = inz;
       }
       const int ia = AXIS == 0 ? iy : (AXIS == 1 ? ix : iz);
@@ -649,16 +651,18 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
   const int fy = gf.nny(), fx = gf.nnx(), fz = gf.nnz();
   const int cy = gc.nny(), cx = gc.nnx(), cz = gc.nnz();
   const int64_t s1 = int64_t(cy) * fx * fz, s2 = int64_t(cy) * cx * fz;
+  if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
+  const FastDiv dcy{uint32_t(cy)}, dfx{uint32_t(fx)}, dcx{uint32_t(cx)};
   if (span == 4) {
-    (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz), topx::count_launch());
-    (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz), topx::count_launch());
+    (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx), topx::count_launch());
+    (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx), topx::count_launch());
     (k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz), topx::count_launch());
+                                                                             cx, cz, dcy, dcx), topx::count_launch());
   } else {
-    (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz), topx::count_launch());
-    (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz), topx::count_launch());
+    (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx), topx::count_launch());
+    (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx), topx::count_launch());
     (k_restrict_axis<T, T, 2, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz), topx::count_launch());
+                                                                             cx, cz, dcy, dcx), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
