@@ -418,7 +418,8 @@ def main(argv=None):
     cm = np.array([h["c"] for h in mixed["hist"]])
     cd = np.array([h["c"] for h in fp64["hist"]])
     n = min(len(cm), len(cd))
-    relerr = float(np.max(np.abs(cm[:n] - cd[:n]) / np.abs(cd[:n])))
+    relerrs = np.abs(cm[:n] - cd[:n]) / np.abs(cd[:n])
+    relerr = float(np.max(relerrs))
     # roofline of the dominant kernel: level-1 K*u in PCG mode (FP64 in both arms).
     # Per launch it reads p_old and z and writes q (3 doubles per node each), reads the
     # moduli (1 double per element) and the free-DOF bits (1 byte per node): 73 B/node +
@@ -447,7 +448,8 @@ def main(argv=None):
                       "dtype": "f64 Krylov iteration, operator, dots, compliance, OC; f32 multigrid "
                                "preconditioner and filter",
                       "pcg_its_per_step": float(np.mean(its_mixed)),
-                      "max_rel_compliance_err_vs_fp64": relerr, "iterations_compared": n},
+                      "max_rel_compliance_err_vs_fp64": relerr, "iterations_compared": n,
+                      "rel_compliance_err_per_iteration": [float("%.3g" % e) for e in relerrs]},
             "pcg_its_per_step": float(np.mean(its64)), "filter_its_per_step": float(np.mean(fits)),
             "phases_ms": {"fp64": phases(fp64), "mixed": phases(mixed)},
             "sections_ms_per_step": {k: round(v[0] / prof["steps"], 3) for k, v in prof["sections"].items()},

@@ -751,14 +751,41 @@ __device__ double coop_wait_value(const double* p, CoopBarrier* bar) {
   }
 }
 
+// Per-lane partial dot products (two accumulators).  FP64 factors accumulate in FP64.  FP32
+// factors multiply and add in FP32 over runs of a few terms, each run then added in FP64: no
+// per-term widening, and the FP32 rounding stays that of short sums whatever m is.
+template <typename TM>
+struct LaneDot;
+template <>
+struct LaneDot<double> {
+  double a0 = 0.0, a1 = 0.0;
+  __device__ __forceinline__ void add0(double v, double u) { a0 = fma(v, u, a0); }
+  __device__ __forceinline__ void add1(double v, double u) { a1 = fma(v, u, a1); }
+  __device__ __forceinline__ void flush() {}
+  __device__ __forceinline__ double total() const { return a0 + a1; }
+};
+template <>
+struct LaneDot<float> {
+  float f0 = 0.f, f1 = 0.f;
+  double a0 = 0.0, a1 = 0.0;
+  __device__ __forceinline__ void add0(float v, float u) { f0 = fmaf(v, u, f0); }
+  __device__ __forceinline__ void add1(float v, float u) { f1 = fmaf(v, u, f1); }
+  __device__ __forceinline__ void flush() {
+    a0 += double(f0);
+    a1 += double(f1);
+    f0 = f1 = 0.f;
+  }
+  __device__ __forceinline__ double total() const { return (a0 + double(f0)) + (a1 + double(f1)); }
+};
+constexpr int kDotRun = 4;  // FP32 terms per accumulator between FP64 flushes
+
 // Dot of one matrix row with a shared-memory vector by one warp.  The row is read in
 // pieces of 32 x 32 elements whose loads are all issued before the first use, so a row
-// of up to 1024 entries costs one memory round trip.  Each lane accumulates its ~m/32 terms
-// in the factors' type (FP32 factors: FP32 products, no conversions); the warp sum is FP64.
+// of up to 1024 entries costs one memory round trip.  The warp sum is FP64.
 template <typename TM>
 __device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const TM* __restrict__ u, int m, int lane) {
   constexpr int PIECE = 32;
-  TM a0 = TM(0), a1 = TM(0);
+  LaneDot<TM> acc;
   for (int base = 0; base < m; base += 32 * PIECE) {
     TM v[PIECE];
 #pragma unroll
@@ -769,11 +796,12 @@ __device__ __forceinline__ double warp_row_dot(const TM* __restrict__ Mr, const 
 #pragma unroll
     for (int i = 0; i < PIECE; i += 2) {
       const int j = base + lane + 32 * i;
-      if (j < m) a0 = fma(v[i], u[j], a0);
-      if (j + 32 < m) a1 = fma(v[i + 1], u[j + 32], a1);
+      if (j < m) acc.add0(v[i], u[j]);
+      if (j + 32 < m) acc.add1(v[i + 1], u[j + 32]);
+      if ((i / 2) % kDotRun == kDotRun - 1) acc.flush();
     }
   }
-  return warp_sum(double(a0) + double(a1));
+  return warp_sum(acc.total());
 }
 
 // One chain step: up to two independent row blocks y = a - M u (M: m x m).
@@ -819,18 +847,24 @@ __device__ __forceinline__ bool chain_step(const ChainOp (&op)[2], int nop, int 
   };
   if (have) {
     const TM* u = su + o0 * m;
-    TM a0 = TM(0), a1 = TM(0);
+    LaneDot<TM> acc;
 #pragma unroll
     for (int i = 0; i < PIECE; i += 2) {
       const int j = lane + 32 * i;
-      if (j < m) a0 = fma(v[i], u[j], a0);
-      if (j + 32 < m) a1 = fma(v[i + 1], u[j + 32], a1);
+      if (j < m) acc.add0(v[i], u[j]);
+      if (j + 32 < m) acc.add1(v[i + 1], u[j + 32]);
+      if ((i / 2) % kDotRun == kDotRun - 1) acc.flush();
     }
+    int run = 0;
     for (int base = 32 * PIECE; base < m; base += 32) {
       const int j = base + lane;
-      if (j < m) a0 = fma(__ldg(M0 + j), u[j], a0);
+      if (j < m) acc.add0(__ldg(M0 + j), u[j]);
+      if (++run == kDotRun) {
+        acc.flush();
+        run = 0;
+      }
     }
-    const double d = warp_sum(double(a0) + double(a1));
+    const double d = warp_sum(acc.total());
     if (lane == 0) st_relaxed_f64(c0.y + (r0 - o0 * m), a_first - d);
   }
   for (int r = gw + nw; r < nop * m; r += nw) {

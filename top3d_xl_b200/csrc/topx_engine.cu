@@ -224,7 +224,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     gf.ctrl = gfCtrl.p;
     gf.ytmp = gfY.p;
     // an engine alone on the GPU fills it; engines sharing it leave room for their neighbours
-    gf.nctas = gj_flow_ctas(coarse_coop);
+    gf.nctas = gj_flow_ctas(coarse_coop, si.m);
     for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
     coopBar.alloc(1);
     // the cooperative solve beats the chain of small launches at every slab size measured

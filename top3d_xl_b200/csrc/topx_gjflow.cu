@@ -479,13 +479,17 @@ void prepare_gj_flow() {
   if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
-int gj_flow_ctas(bool whole_gpu) {
+int gj_flow_ctas(bool whole_gpu, int m) {
   int dev = 0, nsm = 0, per = 0;
   TOPX_CUDA_OK(cudaGetDevice(&dev));
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gj_flow, GF_THREADS, GF_SMEM));
   per = std::max(1, std::min(per, 2));
-  return whole_gpu ? nsm * per : std::max(1, nsm / 2);
+  if (whole_gpu) return nsm * per;
+  // an engine sharing the GPU: enough CTAs for one step's tile tasks, at most a quarter of the
+  // SMs (each CTA holds its SM's shared memory while it waits for its next task)
+  const int nt = gf_tiles(m);
+  return std::max(2, std::min(nsm / 4, nt * nt));
 }
 
 void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,

@@ -110,8 +110,8 @@ struct GJFlow {
 };
 // one-time per-device kernel attributes (call outside stream capture)
 void prepare_gj_flow();
-// CTAs of one inverse launch: two per SM for an engine alone on the GPU, else half the SMs
-int gj_flow_ctas(bool whole_gpu);
+// CTAs of one inverse launch of order m: every SM for an engine alone on the GPU, else a few
+int gj_flow_ctas(bool whole_gpu, int m);
 // in-place inverse of the SPD m x m matrices A0 (and A1 when nset == 2)
 void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,
                     unsigned ntasks, double* scratch, unsigned* ctrl, int nctas);
