@@ -210,8 +210,13 @@ class Context:
         """Kernels launched by the library in this process so far (graph replays included)."""
         return int(self.lib.topx_launch_count())
 
-    def density(self):
-        out = np.empty(self.numElements)
+    def density(self, out=None):
+        """The physical density (compact element order).  out: an optional contiguous float64
+        array of numElements entries to write into (e.g. page-locked host memory)."""
+        if out is None:
+            out = np.empty(self.numElements)
+        elif out.dtype != np.float64 or out.size != self.numElements or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array of numElements entries")
         self._check(self.lib.topx_get_density(self._h, _dptr(out), out.size))
         return out
 
