@@ -874,13 +874,14 @@ bool Engine::step(IterRecord& rec) {
     TOPX_CUDA_OK(cudaMemcpyAsync(ocS.p, &oc, sizeof(oc), cudaMemcpyHostToDevice, st));
     sec_begin(SEC_OC);
     const uint8_t* pas = passive.p;
+    launch_oc_prep(st, Ne, x.p, dc.p, tmpA.p);  // tmpA is free once the filter has run
     for (int chunk = 0; chunk < 8; ++chunk) {
-      for (int k = 0; k < 32; ++k) launch_oc_step(st, Ne, x.p, dc.p, pas, ocS.p, rs1, 0.2);
+      for (int k = 0; k < 32; ++k) launch_oc_step(st, Ne, x.p, tmpA.p, pas, ocS.p, rs1, 0.2);
       TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
       TOPX_CUDA_OK(cudaStreamSynchronize(st));
       if (oc.converged) break;
     }
-    launch_oc_final(st, Ne, x.p, dc.p, pas, xPhys.p, ocS.p, rs1, rs2, 0.2);
+    launch_oc_final(st, Ne, x.p, tmpA.p, pas, xPhys.p, ocS.p, rs1, rs2, 0.2);
     sec_end();
     TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
     TOPX_CUDA_OK(cudaEventRecord(ev[5], st));

@@ -368,19 +368,33 @@ void launch_ewise(cudaStream_t st, int op, int64_t n, const double* a, const dou
 // launch evaluates one bisection step as a grid reduction; once the interval
 // test fails the remaining launches return at once.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double oc_xnew(double x, double dc, double lmid, double move) {
-  const double cand = x * sqrt(-dc / lmid);
-  return fmax(0.0, fmax(x - move, fmin(1.0, fmin(x + move, cand))));
+// x sqrt(-dc / lmid) evaluated as w * r with w = x sqrt(-dc) formed once per OC iteration
+// (k_oc_prep) and r = 1 / sqrt(lmid) once per bisection step: the bisection then streams x and w
+// with two multiplications per element instead of a division and a square root (the result
+// differs from the reference's evaluation order by a few ulps).
+__device__ __forceinline__ double oc_xnew(double x, double w, double r, double move) {
+  return fmax(0.0, fmax(x - move, fmin(1.0, fmin(x + move, w * r))));
 }
 
-__global__ void k_oc_step(int64_t Ne, const double* __restrict__ x, const double* __restrict__ dc,
+__global__ void k_oc_prep(int64_t Ne, const double* __restrict__ x, const double* __restrict__ dc,
+                          double* __restrict__ w) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x)
+    w[e] = x[e] * sqrt(-dc[e]);
+}
+void launch_oc_prep(cudaStream_t st, int64_t Ne, const double* x, const double* dc, double* w) {
+  (k_oc_prep<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, w), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+__global__ void k_oc_step(int64_t Ne, const double* __restrict__ x, const double* __restrict__ w,
                           const uint8_t* __restrict__ passive, OcState* os, RedScratch rs, double move) {
   if (os->converged) return;
   const double lmid = 0.5 * (os->l2 + os->l1);
+  const double r = 1.0 / sqrt(lmid);
   double s = 0.0;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
     const double xv = x[e];
-    const double xn = (passive && passive[e]) ? 1.0 : oc_xnew(xv, dc[e], lmid, move);
+    const double xn = (passive && passive[e]) ? 1.0 : oc_xnew(xv, w[e], r, move);
     s += xn - xv;
   }
   double v[1] = {s}, tot[1];
@@ -395,22 +409,23 @@ __global__ void k_oc_step(int64_t Ne, const double* __restrict__ x, const double
     if (!((os->l2 - os->l1) / (os->l1 + os->l2) > 1e-6)) os->converged = 1;
   }
 }
-void launch_oc_step(cudaStream_t st, int64_t Ne, const double* x, const double* dc, const uint8_t* passive,
+void launch_oc_step(cudaStream_t st, int64_t Ne, const double* x, const double* w, const uint8_t* passive,
                     OcState* os, RedScratch rs, double move) {
-  (k_oc_step<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, os, rs, move), topx::count_launch());
+  (k_oc_step<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, w, passive, os, rs, move), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
 // x = xnew(lmid); xPhys = x (passive = 1); change = max|xnew - x|; sharpness
-__global__ void k_oc_final(int64_t Ne, double* __restrict__ x, const double* __restrict__ dc,
+__global__ void k_oc_final(int64_t Ne, double* __restrict__ x, const double* __restrict__ w,
                            const uint8_t* __restrict__ passive, double* __restrict__ xPhys, OcState* os,
                            RedScratch rs, RedScratch rs2, double move) {
   const double lmid = os->lmid;
+  const double r = 1.0 / sqrt(lmid);
   double ch = 0.0, sh = 0.0;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
     const double xv = x[e];
     const bool pas = passive && passive[e];
-    const double xn = pas ? 1.0 : oc_xnew(xv, dc[e], lmid, move);
+    const double xn = pas ? 1.0 : oc_xnew(xv, w[e], r, move);
     ch = fmax(ch, fabs(xn - xv));
     x[e] = xn;
     xPhys[e] = xn;
@@ -421,9 +436,9 @@ __global__ void k_oc_final(int64_t Ne, double* __restrict__ x, const double* __r
   double mx;
   if (reduce_publish_max(ch, rs2, mx) && threadIdx.x == 0) os->change = mx;
 }
-void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* dc, const uint8_t* passive, double* xPhys,
+void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* w, const uint8_t* passive, double* xPhys,
                      OcState* os, RedScratch rs, RedScratch rs2, double move) {
-  (k_oc_final<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, dc, passive, xPhys, os, rs, rs2, move), topx::count_launch());
+  (k_oc_final<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, w, passive, xPhys, os, rs, rs2, move), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
