@@ -235,7 +235,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   // ---- workspaces ------------------------------------------------------------
   {
     const size_t S1 = size_t(G[0].stride) * 3;
-    for (DevBuf<double>* b : {&kw.r, &kw.z, &kw.p, &kw.q}) b->alloc(S1);
+    for (DevBuf<double>* b : {&kw.r, &kw.z, &kw.p, &kw.q, &kw.p2}) b->alloc(S1);
     E64.alloc(size_t(G[0].nelems()));
     cfix64.upload(cf.data(), cf.size());
     if (prec == PREC_FP64) {
@@ -521,10 +521,11 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
     const int first = launched;
     if (!prof_ && use_graphs && launched + CH <= maxIT) {
       run_graph(key, [&]() {
-        for (int c = 0; c < CH; ++c) {
-          launch_ku<double>(st, KU_P_UPDATE, g, kw.p.p, kw.z.p, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc,
-                            rs1);
-          launch_pcg_update<double, double>(st, g, y, kw.z.p, kw.p.p, kw.r.p, kw.q.p, sc, rs1);
+        for (int c = 0; c < CH; ++c) {  // CH is even: every chunk starts from p
+          double* pin = (c & 1) ? kw.p2.p : kw.p.p;
+          double* pnew = (c & 1) ? kw.p.p : kw.p2.p;
+          launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+          launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
           vcycle(false, sc);
         }
       });
@@ -535,10 +536,12 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
     }
     for (int c = 0; c < CH && launched < maxIT; ++c, ++launched) {
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c], st));
-      launch_ku<double>(st, KU_P_UPDATE, g, kw.p.p, kw.z.p, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+      double* pin = (launched & 1) ? kw.p2.p : kw.p.p;
+      double* pnew = (launched & 1) ? kw.p.p : kw.p2.p;
+      launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
       sec_begin(SEC_UPDATE);
-      launch_pcg_update<double, double>(st, g, y, kw.z.p, kw.p.p, kw.r.p, kw.q.p, sc, rs1);
+      launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
       sec_end();
       vcycle(false, sc);
     }

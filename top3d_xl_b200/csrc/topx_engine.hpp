@@ -85,6 +85,7 @@ struct IterRecord {
 // Level-1 Krylov vectors of the PCG (always FP64: operator, residual, dots).
 struct KrylovWork {
   DevBuf<double> r, z, p, q;
+  DevBuf<double> p2;  // the direction alternates between p and p2 (K*u reads one, writes the other)
 };
 
 // Multigrid preconditioner workspace in its storage precision TC (double for

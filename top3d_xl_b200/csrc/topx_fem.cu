@@ -182,7 +182,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __restrict__ in, const T* __restrict__ zin,
-                                                  T* __restrict__ out, const T* __restrict__ E,
+                                                  T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
                                                   PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
@@ -314,8 +314,14 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
       out[n] = y[0];
       out[n + S] = y[1];
       out[n + 2 * S] = y[2];
-      if (MODE != KU_PLAIN)
+      if (MODE != KU_PLAIN) {
+        if (pout) {  // the direction p = z (+ beta p_old) for the PCG update (another buffer than in)
+          pout[n] = p[0];
+          pout[n + S] = p[1];
+          pout[n + 2 * S] = p[2];
+        }
         dot += double(p[0]) * double(y[0]) + double(p[1]) * double(y[1]) + double(p[2]) * double(y[2]);
+      }
     }
   }
   cp_async_wait_all();
@@ -332,7 +338,7 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
 // added to the tile kernel's.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_ku_l1_lastrow(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
-                                                       T* __restrict__ out, const T* __restrict__ E,
+                                                       T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                        const uint8_t* __restrict__ fixbits,
                                                        const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
@@ -404,7 +410,14 @@ __global__ void __launch_bounds__(256) k_ku_l1_lastrow(Grid g, const T* __restri
     out[n] = y[0];
     out[n + S] = y[1];
     out[n + 2 * S] = y[2];
-    if (MODE != KU_PLAIN) dot += double(p[0]) * double(y[0]) + double(p[1]) * double(y[1]) + double(p[2]) * double(y[2]);
+    if (MODE != KU_PLAIN) {
+      if (pout) {
+        pout[n] = p[0];
+        pout[n + S] = p[1];
+        pout[n + 2 * S] = p[2];
+      }
+      dot += double(p[0]) * double(y[0]) + double(p[1]) * double(y[1]) + double(p[2]) * double(y[2]);
+    }
   }
   if (MODE != KU_PLAIN) {
     double v[1] = {dot}, tot[1];
@@ -447,7 +460,6 @@ static int ku_z_chunk(int nny, int nnx, int nnz) {
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
-  (void)pout;
   // y-tiles of the tile kernel; a last node row that would fill a tile on its own goes to
   // k_ku_l1_lastrow instead
   const bool lastrow = g.ny >= KY && g.ny % KY == 0;
@@ -456,15 +468,15 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
   dim3 blk(KY, KX, 1);
   dim3 grd((rows + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + zc - 1) / zc);
   if (mode == KU_PLAIN)
-    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   else
-    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   if (lastrow) {
     const unsigned nb = unsigned((int64_t(g.nnx()) * g.nnz() + 255) / 256);
     if (mode == KU_PLAIN)
-      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, 256, 0, st>>>(g, in, z, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, 256, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
     else
-      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, 256, 0, st>>>(g, in, z, out, E, fixbits, cfix, sc, rs),
+      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, 256, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
        topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
@@ -551,7 +563,8 @@ struct Vec2<float> {
   using type = float2;
 };
 
-template <typename T, typename TY>
+// PGIVEN: p already holds the new direction (written by K*u), z is not read and p not written
+template <typename T, typename TY, bool PGIVEN>
 __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z, T* __restrict__ p,
                              T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs) {
   if (sc->done) return;
@@ -569,11 +582,13 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t k = 2 * i + c * S;
-      const V2 zv = *reinterpret_cast<const V2*>(z + k);
       V2 pv = *reinterpret_cast<const V2*>(p + k);
-      pv.x = first ? zv.x : zv.x + beta * pv.x;
-      pv.y = first ? zv.y : zv.y + beta * pv.y;
-      *reinterpret_cast<V2*>(p + k) = pv;
+      if (!PGIVEN) {
+        const V2 zv = *reinterpret_cast<const V2*>(z + k);
+        pv.x = first ? zv.x : zv.x + beta * pv.x;
+        pv.y = first ? zv.y : zv.y + beta * pv.y;
+        *reinterpret_cast<V2*>(p + k) = pv;
+      }
       Y2 yv = *reinterpret_cast<const Y2*>(y + k);
       yv.x = yv.x + lamY * TY(pv.x);
       yv.y = yv.y + lamY * TY(pv.y);
@@ -602,7 +617,10 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
                        RedScratch rs) {
-  (k_pcg_update<T, TY><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
+  if (z)
+    (k_pcg_update<T, TY, false><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
+  else
+    (k_pcg_update<T, TY, true><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

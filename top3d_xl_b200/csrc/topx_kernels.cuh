@@ -30,7 +30,7 @@ struct Grid {
 };
 
 // KU_PLAIN: out = K in.  KU_P_UPDATE: p = z (first PCG step) or z + beta*p_in,
-// out = K p, p'q reduced into sc->pq.
+// out = K p, p'q reduced into sc->pq, and p stored into pout when given (a buffer other than in).
 enum KuMode { KU_PLAIN = 0, KU_P_UPDATE = 2 };
 
 // element matrices in constant memory
@@ -43,7 +43,8 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
 template <typename TE, typename T = TE>
 void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
                     const uint8_t* present, T* d);
-// p = z (+ beta p); y += lambda p; r -= lambda q; ||r|| stop test into sc
+// p = z (+ beta p); y += lambda p; r -= lambda q; ||r|| stop test into sc.  z null: p already holds
+// the new direction (K*u in PCG mode wrote it through pout) and is only read
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
                        RedScratch rs);

@@ -51,7 +51,7 @@ int64_t footprint_estimate(const topx_info& in, int precision) {
   const int64_t nt = topx::gf_tiles(int(m));
   const int64_t inverse = int64_t(topx::gf_scratch_doubles(int(m))) * 8 + int64_t(topx::gf_ctrl_words(int(m))) * 4 +
                           3 * nt * (nt * nt + 2 * nt + 1) * 4;
-  const int64_t per_node = precision == TOPX_MIXED ? 560 : 520, per_elem = 200;
+  const int64_t per_node = precision == TOPX_MIXED ? 584 : 544, per_elem = 200;
   return per_node * nodes + per_elem * elems + slab + inverse + (int64_t(48) << 20);
 }
 
