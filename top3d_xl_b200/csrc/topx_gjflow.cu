@@ -486,10 +486,10 @@ int gj_flow_ctas(bool whole_gpu, int m) {
   TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gj_flow, GF_THREADS, GF_SMEM));
   per = std::max(1, std::min(per, 2));
   if (whole_gpu) return nsm * per;
-  // an engine sharing the GPU: enough CTAs for one step's tile tasks, at most a quarter of the
-  // SMs (each CTA holds its SM's shared memory while it waits for its next task)
+  // an engine sharing the GPU: one CTA per tile row, at most an eighth of the SMs (each CTA holds
+  // its SM's shared memory while it waits for its next task, which the other jobs' kernels need)
   const int nt = gf_tiles(m);
-  return std::max(2, std::min(nsm / 4, nt * nt));
+  return std::max(2, std::min(nsm / 8, nt));
 }
 
 void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,
