@@ -67,10 +67,11 @@ def load_workload(ctx, wl):
     else:
         ctx.load_voxels(src)
 METRIC = "OC iterations/s (GLOBAL, FP64; mixed precision beside it)"
-# DRAM bytes (read + write) per grid node of one K*u launch in PCG mode, from an ncu capture of
-# the 128x256x128 cuboid (dram__bytes_read.sum + dram__bytes_write.sum = 259.68 MB + 86.09 MB
-# over 4,276,737 nodes); the traffic of a launch scales with its node count.
-KU_TRAFFIC_PER_NODE = 345.77e6 / 4276737
+# DRAM bytes (read + write) per grid node of one K*u launch in PCG mode (tile kernel + last-row
+# kernel), from an ncu capture of the 128x256x128 cuboid: dram__bytes_read.sum +
+# dram__bytes_write.sum of two launches, 470.53 MB and 465.26 MB, over 4,276,737 nodes; the
+# traffic of a launch scales with its node count.
+KU_TRAFFIC_PER_NODE = 467.89e6 / 4276737
 # Nominal FP64 rate of a B200 on CUDA cores: 148 SMs x 64 FMA/clk x 2 flop x 1.965 GHz.
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
@@ -423,13 +424,14 @@ def main(argv=None):
     n = min(len(cm), len(cd))
     relerrs = np.abs(cm[:n] - cd[:n]) / np.abs(cd[:n])
     relerr = float(np.max(relerrs))
-    # roofline of the dominant kernel: level-1 K*u in PCG mode (FP64 in both arms).
-    # Per launch it reads p_old and z and writes q (3 doubles per node each), reads the
-    # moduli (1 double per element) and the free-DOF bits (1 byte per node): 73 B/node +
-    # 8 B/element; per node 8 hexes x 3 rows x 24 DOFs + 24 scalings = 600 FMA.
+    # roofline of the dominant kernel: level-1 K*u in PCG mode (FP64 in both arms; the tile
+    # kernel and its last-row kernel).  Per launch it reads p_old and z and writes q and the new
+    # direction p (3 doubles per node each), reads the moduli (1 double per element) and the
+    # free-DOF bits (1 byte per node): 97 B/node + 8 B/element; per node 8 hexes x 3 rows x 24
+    # DOFs + 24 scalings = 600 FMA.
     prof = fp64["prof"]
     nn = fp64["nnodes"]
-    alg_bytes = 73 * nn + 8 * fp64["ne"]
+    alg_bytes = 97 * nn + 8 * fp64["ne"]
     flop = 2 * 600 * nn
     ku_ms = prof["ku_ms"] / max(1, prof["ku_launches"])
     achieved = alg_bytes / (ku_ms * 1e-3) / 1e9
