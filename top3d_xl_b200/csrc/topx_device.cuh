@@ -102,8 +102,12 @@ __device__ __forceinline__ double block_max(double v) {
 // Publish this block's NS partial sums; returns true in every thread of the
 // block that finishes last.  That block then holds the NS totals (summed over
 // blocks in block-index order, so the result is deterministic) in out[].
+// Slot s of block b sits at partials[s * stride + b]: the default stride serves
+// up to kMaxRedSlots slots of any grid; more slots need stride >= the grid's
+// block count and NS * stride <= kMaxRedBlocks * kMaxRedSlots.
 template <int NS>
-__device__ __forceinline__ bool reduce_publish(double (&v)[NS], RedScratch rs, double (&out)[NS]) {
+__device__ __forceinline__ bool reduce_publish(double (&v)[NS], RedScratch rs, double (&out)[NS],
+                                               unsigned stride = kMaxRedBlocks) {
   block_sum<NS>(v);
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nth = blockDim.x * blockDim.y * blockDim.z;
@@ -112,7 +116,7 @@ __device__ __forceinline__ bool reduce_publish(double (&v)[NS], RedScratch rs, d
   __shared__ bool amLast;
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < NS; ++s) rs.partials[s * kMaxRedBlocks + bid] = v[s];
+    for (int s = 0; s < NS; ++s) rs.partials[size_t(s) * stride + bid] = v[s];
     __threadfence();
     const unsigned t = atomicAdd(rs.ticket, 1u);
     amLast = (t == nb - 1);
@@ -122,9 +126,12 @@ __device__ __forceinline__ bool reduce_publish(double (&v)[NS], RedScratch rs, d
   __threadfence();
   double acc[NS];
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    acc[s] = 0.0;
-    for (unsigned b = tid; b < nb; b += nth) acc[s] += __ldcg(&rs.partials[s * kMaxRedBlocks + b]);
+  for (int s = 0; s < NS; ++s) acc[s] = 0.0;
+  // every slot of a block in one iteration: the loads of all slots are in flight together
+#pragma unroll 4
+  for (unsigned b = tid; b < nb; b += nth) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc[s] += __ldcg(&rs.partials[size_t(s) * stride + b]);
   }
   block_sum<NS>(acc);
   __shared__ double tot[NS];

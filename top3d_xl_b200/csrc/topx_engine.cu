@@ -878,8 +878,13 @@ bool Engine::step(IterRecord& rec) {
     sec_begin(SEC_OC);
     const uint8_t* pas = passive.p;
     launch_oc_prep(st, Ne, x.p, dc.p, tmpA.p);  // tmpA is free once the filter has run
-    for (int chunk = 0; chunk < 8; ++chunk) {
-      for (int k = 0; k < 32; ++k) launch_oc_step(st, Ne, x.p, tmpA.p, pas, ocS.p, rs1, 0.2);
+    // at most 258 steps: 60 in the first round trip (the interval test usually passes after
+    // 50-60 steps from (0, 1e9)), then 15 per round trip
+    static_assert(60 % kOcStepsPerLaunch == 0 && 15 % kOcStepsPerLaunch == 0, "steps per round trip");
+    for (int launched = 0; launched * kOcStepsPerLaunch < 256;) {
+      const int n = (launched == 0 ? 60 : 15) / kOcStepsPerLaunch;
+      for (int k = 0; k < n; ++k) launch_oc_bisect(st, Ne, x.p, tmpA.p, pas, ocS.p, rs1, 0.2);
+      launched += n;
       TOPX_CUDA_OK(cudaMemcpyAsync(&oc, ocS.p, sizeof(oc), cudaMemcpyDeviceToHost, st));
       TOPX_CUDA_OK(cudaStreamSynchronize(st));
       if (oc.converged) break;

@@ -365,8 +365,8 @@ void launch_ewise(cudaStream_t st, int op, int64_t n, const double* a, const dou
 
 // ---------------------------------------------------------------------------
 // OC update with Lagrange-multiplier bisection (TOP3D_XL.m:145-156).  Each
-// launch evaluates one bisection step as a grid reduction; once the interval
-// test fails the remaining launches return at once.
+// launch evaluates kOcStepsPerLaunch bisection steps as one grid reduction; once
+// the interval test fails the remaining launches return at once.
 // ---------------------------------------------------------------------------
 // x sqrt(-dc / lmid) evaluated as w * r with w = x sqrt(-dc) formed once per OC iteration
 // (k_oc_prep) and r = 1 / sqrt(lmid) once per bisection step: the bisection then streams x and w
@@ -386,32 +386,97 @@ void launch_oc_prep(cudaStream_t st, int64_t Ne, const double* x, const double* 
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-__global__ void k_oc_step(int64_t Ne, const double* __restrict__ x, const double* __restrict__ w,
-                          const uint8_t* __restrict__ passive, OcState* os, RedScratch rs, double move) {
+// kOcStepsPerLaunch bisection steps per launch.  The multipliers the next D = kOcStepsPerLaunch
+// steps can try form a binary tree below the current interval (l1, l2): node 0 is its midpoint,
+// child 2j+1 the midpoint of node j's lower half (the step found the volume too low, l2 = lmid),
+// child 2j+2 of its upper half (l1 = lmid).  One pass over x and w sums the volume change of all
+// 2^D - 1 nodes; the last block then walks the tree taking exactly the decisions, interval test
+// included, that D launches of a one-step kernel take.  Every node's midpoint and sum are
+// formed as the one-step kernel forms them (same expressions, same per-thread order, same
+// block-order reduction), so l1, l2, lmid and the step count come out bit-identical.
+// In the per-element clamp, max(0, max(x - move, min(1, min(x + move, t)))) is regrouped as
+// max(lo, min(hi, t)) with lo = max(0, x - move), hi = min(1, x + move) formed once per element,
+// and the two outer selections are written as comparisons (a NaN t, from a positive dc, selects
+// hi as fmin does): min and max select one operand exactly, so neither changes a value (up to
+// the sign of a zero term of the sum).
+constexpr int kOcNodes = (1 << kOcStepsPerLaunch) - 1;
+
+__global__ void __launch_bounds__(256) k_oc_bisect(int64_t Ne, const double* __restrict__ x,
+                                                   const double* __restrict__ w, const uint8_t* __restrict__ passive,
+                                                   OcState* os, RedScratch rs, double move) {
   if (os->converged) return;
-  const double lmid = 0.5 * (os->l2 + os->l1);
-  const double r = 1.0 / sqrt(lmid);
-  double s = 0.0;
+  // thread j < kOcNodes forms node j's 1/sqrt(lmid): its interval follows the path from the root
+  __shared__ double sr[kOcNodes];
+  if (threadIdx.x < kOcNodes) {
+    const int j = threadIdx.x;
+    int depth = 0;
+    while ((j + 1) >> (depth + 1)) ++depth;  // node j sits at depth floor(log2(j + 1))
+    double a = os->l1, b = os->l2;
+    for (int d = depth - 1; d >= 0; --d) {  // the branch taken at each level, root first
+      const int node = ((j + 1) >> (d + 1)) - 1;
+      const double lmid = 0.5 * (b + a);
+      if (j + 1 - ((node + 1) << (d + 1)) < (1 << d))  // lower half: l2 = lmid
+        b = lmid;
+      else
+        a = lmid;
+    }
+    sr[j] = 1.0 / sqrt(0.5 * (b + a));
+  }
+  __syncthreads();
+  double r[kOcNodes];
+#pragma unroll
+  for (int j = 0; j < kOcNodes; ++j) r[j] = sr[j];
+  double s[kOcNodes];
+#pragma unroll
+  for (int j = 0; j < kOcNodes; ++j) s[j] = 0.0;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
     const double xv = x[e];
-    const double xn = (passive && passive[e]) ? 1.0 : oc_xnew(xv, w[e], r, move);
-    s += xn - xv;
+    if (passive && passive[e]) {
+#pragma unroll
+      for (int j = 0; j < kOcNodes; ++j) s[j] += 1.0 - xv;
+    } else {
+      const double wv = w[e];
+      const double lo = fmax(0.0, xv - move), hi = fmin(1.0, xv + move);
+#pragma unroll
+      for (int j = 0; j < kOcNodes; ++j) {
+        const double t = wv * r[j];
+        const double u = t < hi ? t : hi;
+        s[j] += (u > lo ? u : lo) - xv;
+      }
+    }
   }
-  double v[1] = {s}, tot[1];
-  if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) {
-    const double gt = os->fval + tot[0];
-    if (gt > 0)
-      os->l1 = lmid;
-    else
-      os->l2 = lmid;
+  double tot[kOcNodes];
+  if (reduce_publish<kOcNodes>(s, rs, tot, gridDim.x) && threadIdx.x == 0) {
+    double l1 = os->l1, l2 = os->l2, lmid = os->lmid;
+    int steps = os->steps, conv = 0, j = 0;
+    for (int d = 0; d < kOcStepsPerLaunch; ++d) {
+      lmid = 0.5 * (l2 + l1);
+      const double gt = os->fval + tot[j];
+      if (gt > 0) {
+        l1 = lmid;
+        j = 2 * j + 2;
+      } else {
+        l2 = lmid;
+        j = 2 * j + 1;
+      }
+      steps += 1;
+      if (!((l2 - l1) / (l1 + l2) > 1e-6)) {
+        conv = 1;
+        break;
+      }
+    }
+    os->l1 = l1;
+    os->l2 = l2;
     os->lmid = lmid;
-    os->steps += 1;
-    if (!((os->l2 - os->l1) / (os->l1 + os->l2) > 1e-6)) os->converged = 1;
+    os->steps = steps;
+    os->converged = conv;
   }
 }
-void launch_oc_step(cudaStream_t st, int64_t Ne, const double* x, const double* w, const uint8_t* passive,
-                    OcState* os, RedScratch rs, double move) {
-  (k_oc_step<<<grid1d(Ne, 256), 256, 0, st>>>(Ne, x, w, passive, os, rs, move), topx::count_launch());
+void launch_oc_bisect(cudaStream_t st, int64_t Ne, const double* x, const double* w, const uint8_t* passive,
+                      OcState* os, RedScratch rs, double move) {
+  const unsigned nb = grid1d(Ne, 256);
+  static_assert(size_t(kOcNodes) * 148 * 16 <= size_t(kMaxRedBlocks) * kMaxRedSlots, "reduction slots");
+  (k_oc_bisect<<<nb, 256, 0, st>>>(Ne, x, w, passive, os, rs, move), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

@@ -50,10 +50,12 @@ void launch_objective(cudaStream_t st, int64_t Ne, const double* ce, const doubl
                       double E0, double penal, double* dc, ObjState* os, RedScratch rs);
 void launch_sum(cudaStream_t st, int64_t n, const double* a, const double* b, double* out, RedScratch rs);
 void launch_ewise(cudaStream_t st, int op, int64_t n, const double* a, const double* b, double* out, double s);
-// OC bisection (TOP3D_XL.m:145-156): w = x sqrt(-dc) once, then bisection steps on lmid
+// OC bisection (TOP3D_XL.m:145-156): w = x sqrt(-dc) once, then bisection steps on lmid,
+// kOcStepsPerLaunch of them per launch of launch_oc_bisect
+constexpr int kOcStepsPerLaunch = 3;
 void launch_oc_prep(cudaStream_t st, int64_t Ne, const double* x, const double* dc, double* w);
-void launch_oc_step(cudaStream_t st, int64_t Ne, const double* x, const double* w, const uint8_t* passive,
-                    OcState* os, RedScratch rs, double move);
+void launch_oc_bisect(cudaStream_t st, int64_t Ne, const double* x, const double* w, const uint8_t* passive,
+                      OcState* os, RedScratch rs, double move);
 void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* w, const uint8_t* passive, double* xPhys,
                      OcState* os, RedScratch rs, RedScratch rs2, double move);
 
