@@ -154,3 +154,41 @@ def test_vcycle_with_large_coarsest_slabs(shape):
         ctx.assemble()  # a second factorisation through the same scratch and control words
         r = np.random.default_rng(6).standard_normal(m.levels[0].numDOFs)
         assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
+
+
+@pytest.mark.parametrize("kind", ["cuboid", "irregular"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ku_and_pcg_with_last_row_kernel(kind, precision):
+    # y extent a multiple of the K*u tile height (32 nodes): the tile kernel stops one node row
+    # short and the grid's last row y = ny runs in its own kernel, in both the plain operator and
+    # the PCG step (direction update, stored direction, p'q); fixed DOFs lie on that row too
+    from top3d_xl_b200 import Context
+    if kind == "cuboid":
+        vox = np.ones((32, 20, 12), bool)
+    else:
+        rng = np.random.default_rng(7)
+        vox = rng.random((64, 18, 10)) < 0.8
+        vox[:, 0, :] = True
+        vox[:, -1, :] = True
+    m = O.build_model(vox)
+    assert m.levels[0].resY % 32 == 0
+    x = np.random.default_rng(8).uniform(0.05, 1.0, m.levels[0].numElements)
+    S = m.S
+    E = S.modulusMin + x ** S.SIMPpenalty * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    with Context(precision) as ctx:
+        ctx.load_voxels(vox)
+        ctx.set_moduli(E)
+        ctx.assemble()
+        u = np.random.default_rng(9).standard_normal(m.levels[0].numDOFs)
+        assert _rel(ctx.ku(u), sol.ku(u)) < 1e-13
+        up, its = ctx.pcg()
+    uo, itso, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], m.S.tol, m.S.maxIT)
+    f = m.F[:, 0]
+    if precision == "fp64":
+        assert its == itso
+        assert abs(f @ up - f @ uo) / abs(f @ uo) < 1e-8
+    else:
+        assert abs(its - itso) <= 1
+        assert abs(f @ up - f @ uo) / abs(f @ uo) < 1e-6

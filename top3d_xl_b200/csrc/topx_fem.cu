@@ -331,65 +331,72 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   }
 }
 
-// The last node row y = ny of the grid, one thread per (x, z) node, when the tile kernel's
-// y-tiles end exactly at it: with ny a multiple of the tile height the tile kernel would
-// otherwise run whole tiles for this one row (node counts here are 2^k + 1).  Same operator,
-// same FMA order per node, neighbour values and moduli read directly; the p'q partial sum is
+// The last node row y = ny of the grid, when the tile kernel's y-tiles end exactly at it: with
+// ny a multiple of the tile height the tile kernel would otherwise run whole tiles for this one
+// row (node counts here are 2^k + 1).  A CTA takes 32 x 8 nodes of the row (x, z); its
+// threads first stage, together, the masked values of rows y = ny - 1 and ny over the tile and
+// a one-node halo, their free bits, and the moduli of element row ny - 1 in shared memory (with
+// y the fastest index every node of this row sits in its own DRAM sectors, so the loads are
+// issued all at once rather than one neighbour at a time), then each thread applies the same
+// operator, in the same FMA order, as the tile kernel to its node.  The p'q partial sum is
 // added to the tile kernel's.
+constexpr int KLX = 32, KLZ = 8;
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_ku_l1_lastrow(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
-                                                       T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
-                                                       const uint8_t* __restrict__ fixbits,
-                                                       const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs) {
+__global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
+                                                             T* __restrict__ pout, T* __restrict__ out,
+                                                             const T* __restrict__ E, const uint8_t* __restrict__ fixbits,
+                                                             const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs) {
   if (MODE != KU_PLAIN && sc->done) return;
+  __shared__ T sp[3][KLZ + 2][KLX + 2][2];  // masked values, [comp][z][x][row y = ny - 1, ny]
+  __shared__ T se[KLZ + 1][KLX + 1];        // moduli of element row ny - 1
+  __shared__ uint8_t sfb[KLZ + 2][KLX + 2][2];
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
   const bool first = (MODE != KU_PLAIN) && sc->first;
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
   const int Y = nny - 1;
+  const int x0 = blockIdx.x * KLX, z0 = blockIdx.y * KLZ;
+  const int tid = threadIdx.x;
+  // stage: position i -> row (i & 1), halo x and z; the two rows of one (x, z) are adjacent in memory
+  constexpr int NPOS = 2 * (KLX + 2) * (KLZ + 2);
+  for (int i = tid; i < NPOS; i += KLX * KLZ) {
+    const int row = i & 1, rest = i >> 1;
+    const int sx = rest % (KLX + 2), sz = rest / (KLX + 2);
+    const int gx = x0 - 1 + sx, gz = z0 - 1 + sz;
+    const bool ok = gx >= 0 && gx < nnx && gz >= 0 && gz < nnz;
+    T v0 = T(0), v1 = T(0), v2 = T(0);
+    uint8_t fb = 0;
+    if (ok) {
+      const int64_t n = (Y - 1 + row) + int64_t(nny) * (gx + int64_t(nnx) * gz);
+      ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
+      fb = fixbits[n];
+    }
+    sp[0][sz][sx][row] = (fb & 1) ? T(0) : v0;
+    sp[1][sz][sx][row] = (fb & 2) ? T(0) : v1;
+    sp[2][sz][sx][row] = (fb & 4) ? T(0) : v2;
+    sfb[sz][sx][row] = fb;
+  }
+  for (int i = tid; i < (KLX + 1) * (KLZ + 1); i += KLX * KLZ) {
+    const int sx = i % (KLX + 1), sz = i / (KLX + 1);
+    const int ex = x0 - 1 + sx, ez = z0 - 1 + sz;
+    const bool ok = ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz;
+    se[sz][sx] = ok ? E[(Y - 1) + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)] : T(0);
+  }
+  __syncthreads();
+  const int lx = tid % KLX, lz = tid / KLX;
+  const int x = x0 + lx, z = z0 + lz;
   double dot = 0.0;
-  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < int64_t(nnx) * nnz;
-       t += int64_t(gridDim.x) * blockDim.x) {
-    const int x = int(t % nnx), z = int(t / nnx);
-    T nb[3][3][3][3];  // [dz+1][c][dx+1][dy+1], masked by the free bits, zero outside the grid
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const int gy = Y + dy, gx = x + dx, gz = z + dz;
-          const bool ok = gy < nny && gx >= 0 && gx < nnx && gz >= 0 && gz < nnz;  // gy >= Y-1 >= 0
-          T v0 = T(0), v1 = T(0), v2 = T(0);
-          uint8_t fb = 0;
-          if (ok) {
-            const int64_t n = gy + int64_t(nny) * (gx + int64_t(nnx) * gz);
-            ku_fetch<T, MODE>(in, zin, n, S, first, beta, v0, v1, v2);
-            fb = fixbits[n];
-          }
-          nb[dz + 1][0][dx + 1][dy + 1] = (fb & 1) ? T(0) : v0;
-          nb[dz + 1][1][dx + 1][dy + 1] = (fb & 2) ? T(0) : v1;
-          nb[dz + 1][2][dx + 1][dy + 1] = (fb & 4) ? T(0) : v2;
-        }
-    T em[2][2][2];  // [oz+1][ox+1][oy+1]: hexes around the node, zero outside the grid
-#pragma unroll
-    for (int oz = -1; oz <= 0; ++oz)
-#pragma unroll
-      for (int ox = -1; ox <= 0; ++ox)
-#pragma unroll
-        for (int oy = -1; oy <= 0; ++oy) {
-          const int ey = Y + oy, ex = x + ox, ez = z + oz;
-          const bool ok = ey >= 0 && ey < g.ny && ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz;
-          em[oz + 1][ox + 1][oy + 1] = ok ? E[ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)] : T(0);
-        }
+  if (x < nnx && z < nnz) {
+    // neighbours at y + 1 and hexes above the row lie outside the grid: zero
+    auto PL = [&](int dz, int c, int dx, int dy) { return dy > 0 ? T(0) : sp[c][lz + 1 + dz][lx + 1 + dx][dy + 1]; };
+    auto EL = [&](int oz, int ox, int oy) { return oy == 0 ? T(0) : se[lz + 1 + oz][lx + 1 + ox]; };
     T y[3] = {T(0), T(0), T(0)};
-    auto PL = [&](int dz, int c, int dx, int dy) { return nb[dz + 1][c][dx + 1][dy + 1]; };
-    auto EL = [&](int oz, int ox, int oy) { return em[oz + 1][ox + 1][oy + 1]; };
     ku_half<T, 0>(PL, EL, y);
     ku_half<T, -1>(PL, EL, y);
     const int64_t n = Y + int64_t(nny) * (x + int64_t(nnx) * z);
-    const uint8_t fbo = fixbits[n];
-    T p[3] = {nb[1][0][1][1], nb[1][1][1][1], nb[1][2][1][1]};
+    const uint8_t fbo = sfb[lz + 1][lx + 1][1];
+    T p[3] = {sp[0][lz + 1][lx + 1][1], sp[1][lz + 1][lx + 1][1], sp[2][lz + 1][lx + 1][1]};
     if (fbo) {
       T p0, p1, p2;
       ku_fetch<T, MODE>(in, zin, n, S, first, beta, p0, p1, p2);
@@ -472,11 +479,12 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
   else
     (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
   if (lastrow) {
-    const unsigned nb = unsigned((int64_t(g.nnx()) * g.nnz() + 255) / 256);
+    const dim3 nb((g.nnx() + KLX - 1) / KLX, (g.nnz() + KLZ - 1) / KLZ);
     if (mode == KU_PLAIN)
-      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, 256, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
+       topx::count_launch());
     else
-      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, 256, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
+      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
        topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
