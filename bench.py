@@ -86,48 +86,60 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks, utilisation and throttle reasons.  As a context manager it
+    samples the enclosed block; run_native starts and stops it around the warm-up and timed
+    iterations only.  sm_mhz is the median over the samples taken while a kernel was running
+    (utilisation >= 50 %), so idle host-side gaps do not read as low clocks."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.lines = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
-        time.sleep(0.3)
-        return self
 
-    def __exit__(self, *a):
-        self.lines = []
+    def stop(self):
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 out, _ = self.proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.lines += [l for l in out.splitlines() if l.strip()]
+            self.proc = None
+
+    def __enter__(self):
+        self.start()
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        sm, busy, mx, reasons = [], [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in self.lines:
             f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
                 sm.append(float(f[1]))
                 mx = float(f[2])
+                if float(f[9]) >= 50:
+                    busy.append(float(f[1]))
             except ValueError:
                 continue
             for n, v in zip(names, f[5:9]):
@@ -135,19 +147,22 @@ class Clocks:
                     reasons.add(n)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(busy or sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm), "samples_under_load": len(busy)}
 
 
-def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False):
+def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False, clk=None):
     """Run `warmup` then `steps` timed OC iterations (device time via CUDA events on the
     engine stream); then, if asked, `profile_steps` more iterations with per-section
-    event timing (direct launches instead of CUDA graphs, outside the timed region)."""
+    event timing (direct launches instead of CUDA graphs, outside the timed region).
+    `clk` (a Clocks) samples the warm-up and timed iterations."""
     from top3d_xl_b200 import Context
     ctx = Context(precision, device=device)
     load_workload(ctx, wl)
     ctx.begin(wl["cons"], wl["V0"], wl["nLoop"], wl["rMin"], wl["rHat"])
     hist = []
+    if clk:
+        clk.start()
     for _ in range(warmup):
         hist.append(ctx.step())
     launches0 = ctx.launch_count()
@@ -157,6 +172,8 @@ def run_native(wl, precision, steps, warmup, device, profile_steps=0, keep=False
         hist.append(ctx.step())
     ms = ctx.timer_stop()
     wall = time.perf_counter() - t0
+    if clk:
+        clk.stop()
     launches = ctx.launch_count() - launches0
     prof = None
     if profile_steps:
@@ -409,8 +426,8 @@ def main(argv=None):
         return 0
     if dist:
         dist.barrier()
-    with Clocks(device) as clk:
-        fp64 = run_native(wl, "fp64", a.steps, a.warmup, device, profile_steps=2)
+    clk = Clocks(device)
+    fp64 = run_native(wl, "fp64", a.steps, a.warmup, device, profile_steps=2, clk=clk)
     ms_local = fp64["ms"]
     ms_max = max_over_ranks(ms_local, dist, torch, "cuda")
     if rank != 0:

@@ -49,3 +49,18 @@ def test_reference_arm_prints_one_json_line():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "OC iterations/s"
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_clock_median_uses_samples_under_load():
+    # nvidia-smi lines: index, clocks.sm, clocks.max.sm, power, reasons mask, hw_slowdown,
+    # hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap, utilization.gpu
+    import bench
+    c = bench.Clocks(0)
+    c.lines = ["0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active, 98",
+               "0, 345, 1965, 150.0, 0x0, Not Active, Not Active, Not Active, Not Active, 0",
+               "0, 1950, 1965, 900.0, 0x4, Not Active, Not Active, Not Active, Active, 100"]
+    s = c.summary()
+    assert s["sm_mhz"] == 1957.5 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] == 3 and s["samples_under_load"] == 2
+    c.lines = [c.lines[1]]  # nothing under load: the median of what was sampled
+    assert bench.Clocks.summary(c)["sm_mhz"] == 345.0
