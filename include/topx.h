@@ -45,6 +45,7 @@ enum {
 
 enum { TOPX_GLOBAL = 0, TOPX_LOCAL = 1 };        /* consType (TX:12-18) */
 enum { TOPX_FP64 = 0, TOPX_MIXED = 1 };          /* arithmetic of the solver */
+enum { TOPX_VCYCLE_ADAPTED = 0, TOPX_VCYCLE_STANDARD = 1 };  /* typeVcycle_ (TX:34, 747-781) */
 
 typedef struct topx_ctx topx_ctx;
 
@@ -63,6 +64,9 @@ typedef struct topx_params {
   int device;              /* CUDA device ordinal */
   int coarse_coop;         /* 1: coarsest solve as one cooperative launch when available (default);
                               0: one launch per chain step (for engines sharing the GPU) */
+  int typeVcycle;          /* TOPX_VCYCLE_ADAPTED (default, the reference's setting) or
+                              TOPX_VCYCLE_STANDARD (smoothing against K x on every level; FP64 only,
+                              otherwise topx_create returns TOPX_ERR_ARG) */
 } topx_params;
 
 /* sizes of the loaded model */

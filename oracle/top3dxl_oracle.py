@@ -584,7 +584,8 @@ def _scatter(vals, enod, nnodes):
 
 
 class Solver:
-    """Multigrid-preconditioned PCG of the reference (Adapted V-cycle)."""
+    """Multigrid-preconditioned PCG of the reference ('Adapted' or 'Standard' V-cycle, per
+    ``model.S.typeVcycle``)."""
 
     def __init__(self, model: Model):
         self.m = model
@@ -625,6 +626,17 @@ class Solver:
                 self.m.uniqueKesFixed[self.fix_slot]
             Ye[self.fix_idx] = np.einsum("ki,kij->kj", Ue[self.fix_idx], Mf)
         return _scatter(Ye, l1.eNodMat, l1.numNodes)
+
+    def ku_level(self, u, ii):
+        """Solving_KbyU_MatrixFree on level ii (1-based, TX:684-744): level 1 matrix-free; coarser
+        levels the row-vector products u_e' Ks(:,:,e) with the stored Galerkin matrices
+        (TX:727-743), scattered in the same element-node order."""
+        if ii == 1:
+            return self.ku(u)
+        lv = self.m.levels[ii - 1]
+        Ue = _gather_u(u, lv.eNodMat)
+        Ye = np.einsum("ei,eij->ej", Ue, self.Ks_levels[ii])
+        return _scatter(Ye, lv.eNodMat, lv.numNodes)
 
     def element_mats_level1(self):
         """Per-element 24x24 matrices of level 1 as used by ku (for assembled-K tests)."""
@@ -668,20 +680,30 @@ class Solver:
         return xf.ravel()
 
     def vcycle(self, r):
-        """Solving_Vcycle, 'Adapted' (TX:747-781)."""
+        """Solving_Vcycle (TX:747-781), 'Adapted' or 'Standard' (TX:758-763, 772-777)."""
         L = self.m.levels
         nl = self.m.numLevels
         w = self.S.weightFactorJacobi
+        std = self.S.typeVcycle == "Standard"
+        if not std and self.S.typeVcycle != "Adapted":
+            raise ValueError("typeVcycle must be 'Adapted' or 'Standard'")
         xs = [None] * nl
         rs = [None] * nl
         rs[0] = r
         for ii in range(nl - 1):
             xs[ii] = w * (rs[ii] / L[ii].diagK)
-            rs[ii + 1] = self.restrict(rs[ii], ii + 2)
+            if std:
+                d = rs[ii] - self.ku_level(xs[ii], ii + 1)
+                rs[ii + 1] = self.restrict(d, ii + 2)
+            else:
+                rs[ii + 1] = self.restrict(rs[ii], ii + 2)
         xs[-1] = self.coarse_solve(rs[-1])
         for ii in range(nl - 2, -1, -1):
             xs[ii] = xs[ii] + self.prolong(xs[ii + 1], ii + 2)
-            xs[ii] = xs[ii] + w * rs[ii] / L[ii].diagK
+            if std:
+                xs[ii] = xs[ii] + w * (rs[ii] - self.ku_level(xs[ii], ii + 1)) / L[ii].diagK
+            else:
+                xs[ii] = xs[ii] + w * rs[ii] / L[ii].diagK
         return xs[0]
 
     def coarse_solve(self, r):
@@ -698,6 +720,7 @@ class Solver:
         nl = m.numLevels
         self.E = np.asarray(E, dtype=np.float64).ravel()
         Ks = None
+        self.Ks_levels = {}
         for ii in range(2, nl + 1):
             lv = L[ii - 1]
             s = lv.spanWidth
@@ -736,6 +759,7 @@ class Solver:
                             continue
                         Kf[np.ix_(ed[c], ed[c])] += prevKs[up[j, c] - 1]
                     Ks[j] = I.T @ Kf @ I
+            self.Ks_levels[ii] = Ks
             if ii < nl:
                 dg = np.zeros((lv.numNodes, 3))
                 e0 = (lv.eNodMat - 1).ravel(order="F")

@@ -135,6 +135,19 @@ def test_errors_are_status_codes():
     ctx.close()
 
 
+def test_standard_vcycle_is_an_fp64_setting():
+    from top3d_xl_b200 import Context, TopxError
+    Context("fp64", typeVcycle="Standard").close()
+    Context("fp64", typeVcycle="Adapted").close()
+    with pytest.raises(TopxError) as e:
+        Context("mixed", typeVcycle="Standard")
+    assert "TOPX_ERR_ARG" in str(e.value)
+    with pytest.raises(TopxError):
+        Context("fp64", typeVcycle=2)
+    with pytest.raises(ValueError):
+        Context("fp64", typeVcycle="W")
+
+
 def test_local_requires_rhat():
     from top3d_xl_b200 import TOP3D_XL
     with pytest.raises(ValueError, match="Wrong Input!"):

@@ -192,3 +192,42 @@ def test_ku_and_pcg_with_last_row_kernel(kind, precision):
     else:
         assert abs(its - itso) <= 1
         assert abs(f @ up - f @ uo) / abs(f @ uo) < 1e-6
+
+
+@pytest.mark.parametrize("kind", ["cuboid", "irregular"])
+def test_standard_vcycle(kind):
+    # typeVcycle 'Standard' (TX:758-763, 772-777): level-1 and coarse-level K*u inside the
+    # V-cycle.  The operator matches at the default omega; PCG runs at omega 0.4, where the cycle
+    # is positive definite (at 0.6 it is indefinite and PCG stalls, in the oracle as well)
+    from top3d_xl_b200 import Context
+    if kind == "cuboid":
+        vox = np.ones((12, 24, 12), bool)
+    else:
+        rng = np.random.default_rng(5)
+        vox = rng.random((13, 27, 11)) < 0.75
+        vox[:, 0, :] = True
+        vox[:, -1, :] = True
+    m = O.build_model(vox)
+    x = np.random.default_rng(1).uniform(0.05, 1.0, m.levels[0].numElements)
+    S = m.S
+    E = S.modulusMin + x ** S.SIMPpenalty * (S.modulus - S.modulusMin)
+    sol = O.Solver(m)
+    sol.assemble(E)
+    m.S.typeVcycle = "Standard"
+    r = np.random.default_rng(3).standard_normal(m.levels[0].numDOFs)
+    with Context("fp64", typeVcycle="Standard") as ctx:
+        ctx.load_voxels(vox)
+        ctx.set_moduli(E)
+        ctx.assemble()
+        assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
+    m.S.weightFactorJacobi = 0.4
+    with Context("fp64", typeVcycle="Standard", weightFactorJacobi=0.4) as ctx:
+        ctx.load_voxels(vox)
+        ctx.set_moduli(E)
+        ctx.assemble()
+        assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
+        u, its = ctx.pcg()
+    uo, itso, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], m.S.tol, m.S.maxIT)
+    f = m.F[:, 0]
+    assert abs(its - itso) <= 1
+    assert abs(f @ u - f @ uo) / abs(f @ uo) < 1e-8

@@ -120,6 +120,32 @@ def test_vcycle_is_symmetric():
     assert abs(a @ sol.vcycle(b) - b @ sol.vcycle(a)) < 1e-10 * abs(a @ sol.vcycle(b))
 
 
+def test_standard_vcycle():
+    # 'Standard' V-cycle (TX:758-763, 772-777): Jacobi smoothing against K x on every level but
+    # the coarsest, K applied with the stored Galerkin matrices on coarse levels.  It is
+    # symmetric.  With the reference's omega 0.6 the smoother overshoots the top of D^-1 K's
+    # spectrum here (omega * lambda_max ~ 2.5 > 2), so the cycle is indefinite and PCG stalls;
+    # with omega 0.4 it is positive definite and needs fewer PCG iterations than 'Adapted'.
+    m, sol, E = _small()
+    nl = m.numLevels
+    u = np.random.default_rng(5).standard_normal(m.levels[nl - 1].numDOFs)
+    assert np.allclose(sol.ku_level(u, nl), sol.K_coarsest @ u, rtol=1e-12, atol=1e-12)
+    m.S.typeVcycle = "Standard"
+    rng = np.random.default_rng(3)
+    a, b = rng.standard_normal((2, m.levels[0].numDOFs))
+    assert abs(a @ sol.vcycle(b) - b @ sol.vcycle(a)) < 1e-10 * abs(a @ sol.vcycle(b))
+    f = m.F[:, 0]
+    m.S.weightFactorJacobi = 0.4
+    us, its_std, _ = O.pcg(sol.ku, sol.vcycle, f, m.S.tol, m.S.maxIT)
+    m.S.typeVcycle, m.S.weightFactorJacobi = "Adapted", 0.6
+    ua, its_ad, _ = O.pcg(sol.ku, sol.vcycle, f, m.S.tol, m.S.maxIT)
+    assert its_std < its_ad
+    assert abs(f @ us - f @ ua) < 1e-5 * abs(f @ ua)
+    m.S.typeVcycle = "V"
+    with pytest.raises(ValueError):
+        sol.vcycle(a)
+
+
 def test_filter_preserves_constants_and_is_symmetric():
     m, sol, E = _small()
     flt = O.PDEFilter(m, math.sqrt(3), m.S)

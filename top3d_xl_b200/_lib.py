@@ -25,7 +25,7 @@ class Params(C.Structure):
                 ("SIMPpenalty", C.c_double), ("cellSize", C.c_double), ("tol", C.c_double),
                 ("maxIT", C.c_int), ("weightFactorJacobi", C.c_double),
                 ("coarsestResolutionControl", C.c_int64), ("precision", C.c_int), ("device", C.c_int),
-                ("coarse_coop", C.c_int)]
+                ("coarse_coop", C.c_int), ("typeVcycle", C.c_int)]
 
 
 class Info(C.Structure):

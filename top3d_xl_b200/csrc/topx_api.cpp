@@ -58,6 +58,7 @@ void apply_params(topx::Settings& S, const topx_params& p) {
   S.maxIT = p.maxIT;
   S.weightFactorJacobi = p.weightFactorJacobi;
   S.coarsestResolutionControl = p.coarsestResolutionControl;
+  S.typeVcycle = p.typeVcycle;
 }
 
 topx_status need_model(topx_ctx* c) {
@@ -148,6 +149,7 @@ topx_status topx_default_params(topx_params* p) {
   p->precision = TOPX_FP64;
   p->device = 0;
   p->coarse_coop = 1;
+  p->typeVcycle = TOPX_VCYCLE_ADAPTED;
   return TOPX_OK;
 }
 
@@ -160,7 +162,10 @@ topx_status topx_create(topx_ctx** ctx, const topx_params* p) {
       c->params = *p;
     else
       topx_default_params(&c->params);
-    if (c->params.precision != TOPX_FP64 && c->params.precision != TOPX_MIXED) {
+    const topx_params& q = c->params;
+    const bool vc_ok = q.typeVcycle == TOPX_VCYCLE_ADAPTED ||
+                       (q.typeVcycle == TOPX_VCYCLE_STANDARD && q.precision == TOPX_FP64);
+    if ((q.precision != TOPX_FP64 && q.precision != TOPX_MIXED) || !vc_ok) {
       delete c;
       return TOPX_ERR_ARG;
     }

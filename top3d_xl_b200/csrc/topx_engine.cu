@@ -241,7 +241,12 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     if (prec == PREC_FP64) {
       alloc_vwork(v64);
       alloc_fwork(f64);
+      if (M.S.typeVcycle == 1) {
+        vq.resize(nl);
+        for (int l = 1; l < nl - 1; ++l) vq[l].alloc(size_t(G[l].stride) * 3);
+      }
     } else {
+      if (M.S.typeVcycle == 1) throw std::invalid_argument("the 'Standard' V-cycle runs in FP64 precision");
       alloc_vwork(v32);
       alloc_fwork(f32);
     }
@@ -490,8 +495,57 @@ void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
   sec_end();
 }
 
+// ---------------------------------------------------------------------------
+// 'Standard' V-cycle (TOP3D_XL.m:747-781 with typeVcycle_ = 'Standard'), FP64: on each level
+// but the coarsest x = omega*(r/d), the residual r - K x is restricted; after the coarse-grid
+// correction x += omega*(r - K x)/d.  Level 1 uses the matrix-free K*u (x in z, K x in q, both
+// free while the V-cycle runs); coarser levels the stored Galerkin matrices.
+// ---------------------------------------------------------------------------
+void Engine::vcycle_standard(bool init, PcgScalars* sc) {
+  VWork<double>& v = v64;
+  const double om = M.S.weightFactorJacobi;
+  sec_begin(SEC_RESTRICT);
+  launch_jacobi_pre<double, double, double>(st, G[0], kw.r.p, v.d1.p, present[0].p, kw.z.p, om, sc);
+  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+  launch_residual_inplace<double, double>(st, G[0], kw.r.p, kw.q.p, sc);
+  launch_restrict<double, double>(st, M.levels[1].span, kw.q.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
+  for (int l = 1; l < nl - 1; ++l) {
+    launch_jacobi_pre<double, double, double>(st, G[l], v.rl[l].p, v.dl[l].p, present[l].p, v.xl[l].p, om, sc);
+    launch_ku_coarse(st, G[l], Ks[l].p, epresent[l].p, present[l].p, v.xl[l].p, vq[l].p, sc);
+    launch_residual_inplace<double, double>(st, G[l], v.rl[l].p, vq[l].p, sc);
+    launch_restrict<double, double>(st, M.levels[l + 1].span, vq[l].p, G[l], v.tmp1.p, v.tmp2.p, v.rl[l + 1].p,
+                                    G[l + 1]);
+  }
+  sec_end();
+  sec_begin(SEC_COARSE_SOLVE);
+  if (coopCtas)
+    launch_slab_solve_coop<double, double>(st, coopCtas, G[nl - 1], si, slabSinv.p, slabL.p, slabLT.p,
+                                           v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc,
+                                           coopBar.p);
+  else
+    launch_slab_solve<double, double>(st, G[nl - 1], si, slabSinv.p, slabL.p, slabLT.p, v.rl[nl - 1].p, slabBS.p,
+                                      slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc);
+  sec_end();
+  sec_begin(SEC_PROLONG);
+  for (int l = nl - 2; l >= 1; --l) {
+    launch_prolong_add<double, double, double>(st, M.levels[l + 1].span, v.xl[l + 1].p, G[l + 1], v.rl[l].p,
+                                               v.dl[l].p, present[l].p, v.xl[l].p, G[l], om, sc);
+    launch_ku_coarse(st, G[l], Ks[l].p, epresent[l].p, present[l].p, v.xl[l].p, vq[l].p, sc);
+    launch_jacobi_correct<double, double, double>(st, G[l], v.rl[l].p, vq[l].p, v.dl[l].p, present[l].p,
+                                                  v.xl[l].p, om, false, false, sc, rs1);
+  }
+  launch_prolong_add<double, double, double>(st, M.levels[1].span, v.xl[1].p, G[1], kw.r.p, v.d1.p, present[0].p,
+                                             kw.z.p, G[0], om, sc);
+  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+  launch_jacobi_correct<double, double, double>(st, G[0], kw.r.p, kw.q.p, v.d1.p, present[0].p, kw.z.p, om, true,
+                                                init, sc, rs1);
+  sec_end();
+}
+
 void Engine::vcycle(bool init, PcgScalars* sc) {
-  if (prec == PREC_FP64)
+  if (prec == PREC_FP64 && M.S.typeVcycle == 1)
+    vcycle_standard(init, sc);
+  else if (prec == PREC_FP64)
     vcycle_t<double>(v64, init, sc);
   else
     vcycle_t<float>(v32, init, sc);

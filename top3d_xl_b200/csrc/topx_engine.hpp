@@ -175,6 +175,7 @@ class Engine {
   void alloc_fwork(FWork<TF>& f);
   template <typename TC>
   void vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc);
+  void vcycle_standard(bool init, PcgScalars* sc);
   void vcycle(bool init, PcgScalars* sc);
   int pcg(const double* b, double* y, bool warm, double tol, int maxIT);
   template <typename TF>
@@ -211,6 +212,7 @@ class Engine {
   // workspaces
   KrylovWork kw;
   VWork<double> v64;
+  std::vector<DevBuf<double>> vq;  // 'Standard' V-cycle: K x per coarse smoothing level (index = level-1)
   VWork<float> v32;
   FWork<double> f64;
   FWork<float> f32;

@@ -699,12 +699,14 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
 //   x = omega*(r./d) + P*xc + (omega*r)./d   on present fine nodes.
 // The level-1 instance also reduces z'r and updates beta/x1 (TOP3D_XL.m:626-630).
 // ---------------------------------------------------------------------------
-template <typename TX, typename T, typename TD, int S, bool DOT>
+// SMOOTH = false (the 'Standard' V-cycle) stops after omega*(r/d) + P(xc); the Jacobi
+// correction against K x follows in k_jacobi_correct.
+template <typename TX, typename T, typename TD, int S, bool DOT, bool SMOOTH = true>
 __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __restrict__ r,
                                                         const TD* __restrict__ dinv,
                                                         const uint8_t* __restrict__ present, T* __restrict__ x,
                                                         Grid gf, T omega, PcgScalars* sc, RedScratch rs, int init) {
-  if (DOT && sc->done) return;
+  if ((DOT || !SMOOTH) && sc->done) return;
   const int fny = gf.nny(), fnx = gf.nnx();
   const int64_t nn = gf.nnodes();
   const int cny = gc.nny(), cnx = gc.nnx();
@@ -744,7 +746,7 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
       for (int c = 0; c < 3; ++c) {
         T t = omega * (rv[c] * di[c]);
         t = t + pc[c];
-        t = t + (omega * rv[c]) * di[c];
+        if (SMOOTH) t = t + (omega * rv[c]) * di[c];
         v[c] = t;
         if (DOT) zr += double(t) * double(rv[c]);
       }
@@ -782,6 +784,159 @@ void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, con
     else
       (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
   }
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+template <typename TX, typename T, typename TD>
+void launch_prolong_add(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
+                        const uint8_t* present, T* x, Grid gf, double omega, PcgScalars* sc) {
+  const unsigned nb = grid1d(gf.nnodes(), 256, 148 * 8);
+  const T w = T(omega);
+  RedScratch none{nullptr, nullptr};
+  if (span == 4)
+    (k_prolong_smooth<TX, T, TD, 4, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, none, 0),
+     topx::count_launch());
+  else
+    (k_prolong_smooth<TX, T, TD, 2, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, none, 0),
+     topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// 'Standard' V-cycle pieces (TOP3D_XL.m:758-763, 772-777): pre-smoothing from zero, the
+// residual r - K x, and the Jacobi correction after the coarse-grid correction.  All return at
+// once when the PCG has finished (sc->done), like the prolongation that writes the V-cycle
+// output.
+// ---------------------------------------------------------------------------
+// x = omega*(r/d) on present nodes (the first line of the restriction loop, TX:757)
+template <typename TR, typename T, typename TD>
+__global__ void k_jacobi_pre(Grid g, const TR* __restrict__ r, const TD* __restrict__ dinv,
+                             const uint8_t* __restrict__ present, T* __restrict__ x, T omega, const PcgScalars* sc) {
+  if (sc->done) return;
+  const int64_t N = g.nnodes();
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    const bool pres = present[n] != 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      x[n + c * g.stride] = pres ? omega * (T(r[n + c * g.stride]) * T(dinv[n + c * g.stride])) : T(0);
+  }
+}
+template <typename TR, typename T, typename TD>
+void launch_jacobi_pre(cudaStream_t st, Grid g, const TR* r, const TD* d, const uint8_t* present, T* x, double omega,
+                       const PcgScalars* sc) {
+  (k_jacobi_pre<TR, T, TD><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, r, d, present, x, T(omega), sc),
+   topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// q = r - q: the residual after pre-smoothing, restricted next (TX:761-762)
+template <typename TR, typename T>
+__global__ void k_residual_inplace(Grid g, const TR* __restrict__ r, T* __restrict__ q, const PcgScalars* sc) {
+  if (sc->done) return;
+  const int64_t N = g.nnodes();
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) q[n + c * g.stride] = T(r[n + c * g.stride]) - q[n + c * g.stride];
+  }
+}
+template <typename TR, typename T>
+void launch_residual_inplace(cudaStream_t st, Grid g, const TR* r, T* q, const PcgScalars* sc) {
+  (k_residual_inplace<TR, T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, r, q, sc), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// x = x + omega*(r - q)/d on present nodes, q = K x (TX:775-776); the finest instance also
+// reduces z'r and updates beta/x1 like the 'Adapted' prolongation (TX:626-630)
+template <typename TR, typename T, typename TD, bool DOT>
+__global__ void __launch_bounds__(256) k_jacobi_correct(Grid g, const TR* __restrict__ r, const T* __restrict__ q,
+                                                        const TD* __restrict__ dinv,
+                                                        const uint8_t* __restrict__ present, T* __restrict__ x,
+                                                        T omega, PcgScalars* sc, RedScratch rs, int init) {
+  if (sc->done) return;
+  const int64_t N = g.nnodes();
+  double zr = 0.0;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    const bool pres = present[n] != 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = n + c * g.stride;
+      const T rv = T(r[i]);
+      const T t = pres ? x[i] + (omega * (rv - q[i])) * T(dinv[i]) : T(0);
+      x[i] = t;
+      if (DOT) zr += double(t) * double(rv);
+    }
+  }
+  if (DOT) {
+    double vv[1] = {zr}, tot[1];
+    if (reduce_publish<1>(vv, rs, tot) && threadIdx.x == 0) {
+      if (init) {
+        sc->x1 = tot[0];
+      } else {
+        sc->beta = tot[0] / sc->x1;
+        sc->x1 = tot[0];
+      }
+    }
+  }
+}
+template <typename TR, typename T, typename TD>
+void launch_jacobi_correct(cudaStream_t st, Grid g, const TR* r, const T* q, const TD* d, const uint8_t* present,
+                           T* x, double omega, bool dot, bool init, PcgScalars* sc, RedScratch rs) {
+  const unsigned nb = grid1d(g.nnodes(), 256, 148 * 8);
+  if (dot)
+    (k_jacobi_correct<TR, T, TD, true><<<nb, 256, 0, st>>>(g, r, q, d, present, x, T(omega), sc, rs, init ? 1 : 0),
+     topx::count_launch());
+  else
+    (k_jacobi_correct<TR, T, TD, false><<<nb, 256, 0, st>>>(g, r, q, d, present, x, T(omega), sc, rs, init ? 1 : 0),
+     topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+// K*u on a coarse level with its stored Galerkin matrices (Solving_KbyU_MatrixFree for
+// iLevel > 1, TOP3D_XL.m:727-743).  One thread per node: for each hex around it, in
+// local-node order (the order accumarray adds them), the product of the node's three rows of
+// Ks_e with the hex's 24 DOFs, then the sum over hexes.  Deterministic, no atomics.  The
+// reference forms u_e' Ks_e; the Galerkin matrices are symmetric, so rows serve for columns (up
+// to the rounding of their assembly).
+__global__ void __launch_bounds__(256) k_ku_coarse(Grid g, const double* __restrict__ Ks,
+                                                   const uint8_t* __restrict__ epresent,
+                                                   const uint8_t* __restrict__ present, const double* __restrict__ u,
+                                                   double* __restrict__ y, const PcgScalars* sc) {
+  if (sc->done) return;
+  const int64_t N = g.nnodes();
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    double s[3] = {0.0, 0.0, 0.0};
+    if (present[n]) {
+      const int gy = int(n % nny), gx = int((n / nny) % nnx), gz = int(n / (int64_t(nny) * nnx));
+      for (int a = 0; a < 8; ++a) {
+        const int ey = gy - hex_ly(a), ex = gx - hex_lx(a), ez = gz - hex_lz(a);
+        if (ey < 0 || ey >= g.ny || ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+        const int64_t e = ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez);
+        if (!epresent[e]) continue;
+        const double* K = Ks + e * 576 + (3 * a) * 24;  // rows 3a .. 3a + 2
+        double t[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const int64_t m = (ey + hex_ly(b)) + int64_t(nny) * ((ex + hex_lx(b)) + int64_t(nnx) * (ez + hex_lz(b)));
+          const double u0 = u[m], u1 = u[m + g.stride], u2 = u[m + 2 * g.stride];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            t[c] = fma(K[c * 24 + 3 * b], u0, t[c]);
+            t[c] = fma(K[c * 24 + 3 * b + 1], u1, t[c]);
+            t[c] = fma(K[c * 24 + 3 * b + 2], u2, t[c]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s[c] += t[c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) y[n + c * g.stride] = s[c];
+  }
+}
+void launch_ku_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* epresent, const uint8_t* present,
+                      const double* u, double* y, const PcgScalars* sc) {
+  (k_ku_coarse<<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, Ks, epresent, present, u, y, sc), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -903,6 +1058,15 @@ template void launch_restrict<double, float>(cudaStream_t, int, const double*, G
 template void launch_prolong_smooth<float, double, float>(cudaStream_t, int, const float*, Grid, const double*,
                                                           const float*, const uint8_t*, double*, Grid, double, bool,
                                                           bool, PcgScalars*, RedScratch);
+template void launch_prolong_add<double, double, double>(cudaStream_t, int, const double*, Grid, const double*,
+                                                        const double*, const uint8_t*, double*, Grid, double,
+                                                        PcgScalars*);
+template void launch_jacobi_pre<double, double, double>(cudaStream_t, Grid, const double*, const double*,
+                                                        const uint8_t*, double*, double, const PcgScalars*);
+template void launch_residual_inplace<double, double>(cudaStream_t, Grid, const double*, double*, const PcgScalars*);
+template void launch_jacobi_correct<double, double, double>(cudaStream_t, Grid, const double*, const double*,
+                                                            const double*, const uint8_t*, double*, double, bool,
+                                                            bool, PcgScalars*, RedScratch);
 template void launch_convert<double, float>(cudaStream_t, const double*, float*, int64_t);
 template void launch_convert<float, double>(cudaStream_t, const float*, double*, int64_t);
 template void launch_convert<double, double>(cudaStream_t, const double*, double*, int64_t);

@@ -60,6 +60,22 @@ template <typename TX, typename T, typename TD>
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
                            PcgScalars* sc, RedScratch rs);
+// 'Standard' V-cycle (TX:758-763, 772-777): x = omega*(r/d) + P(xc) without the smoothing term;
+// x = omega*(r/d); q = r - q; x += omega*(r - q)/d (with dot: z.r into sc as above); coarse-level
+// K*u with the stored Galerkin matrices Ks (dense elements x 576).  All skip once sc->done.
+template <typename TX, typename T, typename TD>
+void launch_prolong_add(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
+                        const uint8_t* present, T* x, Grid gf, double omega, PcgScalars* sc);
+template <typename TR, typename T, typename TD>
+void launch_jacobi_pre(cudaStream_t st, Grid g, const TR* r, const TD* d, const uint8_t* present, T* x, double omega,
+                       const PcgScalars* sc);
+template <typename TR, typename T>
+void launch_residual_inplace(cudaStream_t st, Grid g, const TR* r, T* q, const PcgScalars* sc);
+template <typename TR, typename T, typename TD>
+void launch_jacobi_correct(cudaStream_t st, Grid g, const TR* r, const T* q, const TD* d, const uint8_t* present,
+                           T* x, double omega, bool dot, bool init, PcgScalars* sc, RedScratch rs);
+void launch_ku_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* epresent, const uint8_t* present,
+                      const double* u, double* y, const PcgScalars* sc);
 // --- conversions -----------------------------------------------------------
 template <typename TA, typename TB>
 void launch_convert(cudaStream_t st, const TA* a, TB* b, int64_t n);

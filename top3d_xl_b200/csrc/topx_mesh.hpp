@@ -24,6 +24,7 @@ struct Settings {
   int maxIT = 800;
   double weightFactorJacobi = 0.6;
   int64_t coarsestResolutionControl = 50000;
+  int typeVcycle = 0;  // 0 'Adapted' (the reference's setting), 1 'Standard' (TX:34)
   int nonDyadic = 1;
 };
 

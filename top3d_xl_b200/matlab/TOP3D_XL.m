@@ -2,13 +2,16 @@
 %% optimisation loop on a B200 through the topx_mex gateway (libtopx.so).
 %% Same signature, argument checks, console lines and ./out/ files as the reference; the padded
 %% density volume is saved with niftiwrite when available, else as DesignVolume.mat.
-%% Optional trailing name/value: 'precision', 'fp64' | 'mixed'.
+%% Optional trailing name/value pairs: 'precision', 'fp64' | 'mixed'; 'typeVcycle',
+%% 'Adapted' (default, the reference's typeVcycle_) | 'Standard' (FP64 only).
 function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
 	precision = 'fp64';
+	typeVcycle = 'Adapted';
 	rHat = [];
 	args = varargin;
-	if numel(args) >= 2 && ischar(args{end-1}) && strcmp(args{end-1}, 'precision')
-		precision = args{end}; args = args(1:end-2);
+	while numel(args) >= 2 && ischar(args{end-1}) && any(strcmp(args{end-1}, {'precision', 'typeVcycle'}))
+		if strcmp(args{end-1}, 'precision'), precision = args{end}; else, typeVcycle = args{end}; end
+		args = args(1:end-2);
 	end
 	switch consType
 		case 'GLOBAL'
@@ -24,7 +27,7 @@ function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
 	outPath = './out/'; if ~exist(outPath, 'dir'), mkdir(outPath); end
 	fid = fopen(strcat(outPath, 'RunLog.log'), 'w'); fclose(fid); diary(strcat(outPath, 'RunLog.log'));
 	tStartTotal = tic;
-	[hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision);
+	[hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision, typeVcycle);
 	disp(['Compliance of Fully Solid Domain: ' sprintf('%16.6e', hist.cSolid)]);
 	for loop = 1:numel(hist.c)
 		if strcmp(consType, 'GLOBAL')

@@ -42,7 +42,7 @@ static double scalar_arg(const mxArray* a, const char* name) {
 }
 
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
-  char cons[16], prec[16];
+  char cons[16], prec[16], vcyc[16];
   topx_params p;
   topx_info info;
   topx_iter* hist = NULL;
@@ -58,9 +58,14 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   if (nrhs >= 6 && !mxIsEmpty(prhs[5])) rHat = scalar_arg(prhs[5], "rHat");
   strcpy(prec, "fp64");
   if (nrhs >= 7) mxGetString(prhs[6], prec, sizeof(prec));
+  strcpy(vcyc, "Adapted");
+  if (nrhs >= 8) mxGetString(prhs[7], vcyc, sizeof(vcyc));
+  if (strcmp(vcyc, "Adapted") != 0 && strcmp(vcyc, "Standard") != 0)
+    mexErrMsgIdAndTxt("topx:arg", "typeVcycle must be 'Adapted' or 'Standard'");
 
   topx_default_params(&p);
   p.precision = strcmp(prec, "mixed") == 0 ? TOPX_MIXED : TOPX_FP64;
+  p.typeVcycle = strcmp(vcyc, "Standard") == 0 ? TOPX_VCYCLE_STANDARD : TOPX_VCYCLE_ADAPTED;
   topx_mex_cleanup();
   check(topx_create(&g_ctx, &p), "topx_create");
   mexAtExit(topx_mex_cleanup);

@@ -44,6 +44,10 @@ class Context:
         for k, v in settings.items():
             if not hasattr(p, k):
                 raise ValueError(f"unknown setting {k}")
+            if k == "typeVcycle" and isinstance(v, str):  # the reference's spelling (TX:34)
+                if v not in ("Adapted", "Standard"):
+                    raise ValueError("typeVcycle must be 'Adapted' or 'Standard'")
+                v = 0 if v == "Adapted" else 1
             setattr(p, k, v)
         self.params = p
         self._h = C.c_void_p()
