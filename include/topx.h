@@ -151,6 +151,17 @@ topx_status topx_ku_noalloc(topx_ctx* ctx, const double* u_dev, double* y_dev, s
 topx_status topx_assemble(topx_ctx* ctx);
 /* Solving_Vcycle (TX:747-781): z = M r in the context's precision */
 topx_status topx_vcycle(topx_ctx* ctx, const double* r, double* z, size_t ndof);
+
+/* Design output files (host only, no context).  vol is the padded density volume V(y, x, z),
+   column-major ny x nx x nz as the reference forms it (TX:206-208, 565-568; void = 0).
+   topx_write_design_nii: IO_ExportDesignInVolume_nii (TX:564-570), NIfTI-1 FLOAT64.
+   topx_write_design_stl: the 'Vis.' block and IO_ExportDesignInTriSurface_stl (TX:206-222,
+   572-577): V flipped along y, its isosurface at `iso` (the reference uses 0.5) closed by caps on
+   the volume boundary, in MATLAB's vertex coordinates (x = column, y = row, z = page, from 1),
+   as binary STL with outward normals; *ntriangles (may be NULL) gets the triangle count. */
+topx_status topx_write_design_nii(const double* vol, int ny, int nx, int nz, const char* path);
+topx_status topx_write_design_stl(const double* vol, int ny, int nx, int nz, double iso, const char* path,
+                                  int64_t* ntriangles);
 /* Jacobi diagonal meshHierarchy_(level).diagK (level < numLevels), interleaved */
 topx_status topx_get_diag(topx_ctx* ctx, int level, double* out, size_t n);
 /* Solving_PCG with K*u and the V-cycle (TX:600-639), warm start from u; its = iterations */

@@ -19,6 +19,7 @@ int mxIsChar(const mxArray* a);
 char* mxArrayToString(const mxArray* a);
 void mxFree(void* p);
 int mxIsLogical(const mxArray* a);
+int mxIsDouble(const mxArray* a);
 mwSize mxGetNumberOfDimensions(const mxArray* a);
 const mwSize* mxGetDimensions(const mxArray* a);
 mxLogical* mxGetLogicals(const mxArray* a);

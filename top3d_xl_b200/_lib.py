@@ -97,6 +97,8 @@ SIGNATURES = {
     "topx_ku_noalloc": [_P, C.c_void_p, C.c_void_p, _SZ],
     "topx_assemble": [_P],
     "topx_vcycle": [_P, _D, _D, _SZ],
+    "topx_write_design_nii": [_D, C.c_int, C.c_int, C.c_int, C.c_char_p],
+    "topx_write_design_stl": [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_char_p, C.POINTER(C.c_int64)],
     "topx_get_diag": [_P, C.c_int, _D, _SZ],
     "topx_pcg": [_P, C.c_int, _D, _SZ, C.POINTER(C.c_int)],
     "topx_filter": [_P, C.c_double, _D, _D, _SZ, C.POINTER(C.c_int)],

@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libtopx.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["topx_fem.cu", "topx_coarse.cu", "topx_gjflow.cu", "topx_opt.cu", "topx_engine.cu", "topx_noalloc.cu"]
-CXX_SOURCES = ["topx_mesh.cpp", "topx_api.cpp", "topx_server.cpp"]
+CXX_SOURCES = ["topx_mesh.cpp", "topx_api.cpp", "topx_server.cpp", "topx_export.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

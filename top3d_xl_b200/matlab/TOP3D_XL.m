@@ -1,7 +1,7 @@
 %% Drop-in replacement of TOP3D_XL(inputModel, consType, V0, nLoop, rMin, ...) that runs the
 %% optimisation loop on a B200 through the topx_mex gateway (libtopx.so).
-%% Same signature, argument checks, console lines and ./out/ files as the reference; the padded
-%% density volume is saved with niftiwrite when available, else as DesignVolume.mat.
+%% Same signature, argument checks, console lines and ./out/ files as the reference, including
+%% DesignVolume.nii (the padded density volume) and DesignVolume.stl (its 0.5 isosurface with caps).
 %% Optional trailing name/value pairs: 'precision', 'fp64' | 'mixed'; 'typeVcycle',
 %% 'Adapted' (default, the reference's typeVcycle_) | 'Standard' (FP64 only).
 function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
@@ -45,8 +45,7 @@ function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
 	V = zeros(grid.resX * grid.resY * grid.resZ, 1);
 	V(double(grid.eleMapBack)) = xPhys;
 	V = reshape(V, grid.resY, grid.resX, grid.resZ);
-	if exist('niftiwrite', 'file'), niftiwrite(V, strcat(outPath, 'DesignVolume.nii'));
-	else, save(strcat(outPath, 'DesignVolume.mat'), 'V'); end
+	topx_mex('write_design', V, outPath);   % DesignVolume.nii and DesignVolume.stl
 	disp(['..........Performing Topology Optimization Costs (in total): ', sprintf('%10.4e', toc(tStartTotal)), 's.']);
 	diary off;
 end

@@ -17,6 +17,7 @@
  * Every library status is turned into mexErrMsgIdAndTxt; no C++ exception crosses this file.
  */
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include "mex.h"
@@ -41,8 +42,31 @@ static double scalar_arg(const mxArray* a, const char* name) {
   return mxGetScalar(a);
 }
 
+/* topx_mex('write_design', V, outPath): DesignVolume.nii and DesignVolume.stl of the padded density
+   volume V (ny x nx x nz double), TOP3D_XL.m:206-222 and 564-577 */
+static void write_design(const mxArray* V, const mxArray* dir) {
+  char path[4096], base[4000];
+  const mwSize* d;
+  if (!mxIsDouble(V) || mxGetNumberOfDimensions(V) != 3) mexErrMsgIdAndTxt("topx:arg", "V must be a 3-D double array");
+  if (mxGetString(dir, base, sizeof(base))) mexErrMsgIdAndTxt("topx:arg", "outPath must be a string");
+  d = mxGetDimensions(V);
+  snprintf(path, sizeof(path), "%sDesignVolume.nii", base);
+  if (topx_write_design_nii(mxGetPr(V), (int)d[0], (int)d[1], (int)d[2], path) != TOPX_OK)
+    mexErrMsgIdAndTxt("topx:error", "cannot write %s", path);
+  snprintf(path, sizeof(path), "%sDesignVolume.stl", base);
+  if (topx_write_design_stl(mxGetPr(V), (int)d[0], (int)d[1], (int)d[2], 0.5, path, NULL) != TOPX_OK)
+    mexErrMsgIdAndTxt("topx:error", "cannot write %s", path);
+}
+
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   char cons[16], prec[16], vcyc[16];
+  if (nrhs == 3 && mxIsChar(prhs[0])) {
+    char cmd[16];
+    mxGetString(prhs[0], cmd, sizeof(cmd));
+    if (strcmp(cmd, "write_design") != 0) mexErrMsgIdAndTxt("topx:arg", "Wrong Input!");
+    write_design(prhs[1], prhs[2]);
+    return;
+  }
   topx_params p;
   topx_info info;
   topx_iter* hist = NULL;

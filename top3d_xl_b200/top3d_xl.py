@@ -4,8 +4,9 @@
 ``Context`` wraps one ``topx_ctx`` (one design job on one GPU); ``TOP3D_XL`` keeps
 the reference's signature, argument checks, console lines and ``./out/`` files
 (RunLog.log, c_Target.dat, iters_Target.dat, sharp_Target.dat,
-timing_Target.dat, TOP3D_XL.m:186-204).  The padded density volume that the
-reference writes as NIfTI (TOP3D_XL.m:564-570) is written as DesignVolume.npy.
+timing_Target.dat, TOP3D_XL.m:186-204) and the design files DesignVolume.nii (the padded
+density volume, TOP3D_XL.m:564-570) and DesignVolume.stl (its 0.5 isosurface with caps,
+TOP3D_XL.m:206-222, 572-577); the volume is also saved as DesignVolume.npy.
 """
 from __future__ import annotations
 
@@ -234,6 +235,26 @@ class Context:
         return out
 
 
+def write_design_files(vol, ny, nx, nz, out_dir, iso=0.5):
+    """DesignVolume.nii and DesignVolume.stl from the padded density volume (column-major
+    ny x nx x nz, void = 0) through topx_write_design_nii / topx_write_design_stl; returns the
+    STL's triangle count."""
+    lib = L.load()
+    v = np.ascontiguousarray(np.asarray(vol, dtype=np.float64).reshape(-1, order="F") if np.ndim(vol) == 3
+                             else np.asarray(vol, dtype=np.float64))
+    if v.size != ny * nx * nz:
+        raise ValueError("volume size does not match ny x nx x nz")
+    st = lib.topx_write_design_nii(_dptr(v), ny, nx, nz, os.path.join(out_dir, "DesignVolume.nii").encode())
+    if st != L.TOPX_OK:
+        raise TopxError(st, "writing DesignVolume.nii")
+    n = C.c_int64(0)
+    st = lib.topx_write_design_stl(_dptr(v), ny, nx, nz, float(iso), os.path.join(out_dir, "DesignVolume.stl").encode(),
+                                   C.byref(n))
+    if st != L.TOPX_OK:
+        raise TopxError(st, "writing DesignVolume.stl")
+    return int(n.value)
+
+
 def TOP3D_XL(inputModel, consType, V0, nLoop, rMin, *varargin, precision="fp64", out_dir="./out", verbose=True,
              device=0):
     """Drop-in for ``TOP3D_XL(inputModel, consType, V0, nLoop, rMin, [rHat])`` (TOP3D_XL.m:4-19).
@@ -310,6 +331,7 @@ def TOP3D_XL(inputModel, consType, V0, nLoop, rMin, *varargin, precision="fp64",
         vol[emb - 1] = xPhys
         np.save(os.path.join(out_dir, "DesignVolume.npy"),
                 vol.reshape((info.resY[0], info.resX[0], info.resZ[0]), order="F"))
+        write_design_files(vol, info.resY[0], info.resX[0], info.resZ[0], out_dir)
         say("..........Performing Topology Optimization Costs (in total): %10.4es." % (time.perf_counter() - t_all))
         return dict(cSolid=cSolid, history=hist, xPhys=xPhys, info=info)
     finally:
