@@ -122,6 +122,15 @@ const char* topx_version(void);
 topx_status topx_load_voxels(topx_ctx* ctx, const uint8_t* vox, int nely, int nelx, int nelz);
 /* CreateVoxelFEAmodel, .TopVoxel v1.0 input (TX:448-528) */
 topx_status topx_load_topvoxel(topx_ctx* ctx, const char* path);
+/* Boundary conditions of the loaded model as a .TopVoxel file gives them (TX:480-497,
+   AdaptBCExternalMdl TX:1439-1490, then FEA_ApplyBoundaryCondition TX:1294-1336), replacing the
+   built-in ones of topx_load_voxels or the file's.  Node ids are 1-based in the input model's own
+   (nely+1) x (nelx+1) x (nelz+1) node grid, y fastest.  fixing: nfix rows (node, fixX, fixY,
+   fixZ), a direction fixed where its value is 1; loads: nload rows (node, Fx, Fy, Fz, loadCase),
+   load cases numbered from 1 (the reference's additional load cases).  Repeated nodes: the first
+   row counts.  A node outside the grid returns TOPX_ERR_ARG, one outside the solid model
+   TOPX_ERR_MODEL, no loads TOPX_ERR_MODEL ('No Loads!'). */
+topx_status topx_set_bc(topx_ctx* ctx, const double* fixing, int64_t nfix, const double* loads, int64_t nload);
 topx_status topx_get_info(const topx_ctx* ctx, topx_info* out);
 /* element stiffness matrix (TX:1254-1292), 24x24 row-major */
 topx_status topx_get_ke(const topx_ctx* ctx, double* out576);

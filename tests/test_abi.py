@@ -121,6 +121,54 @@ def test_topvoxel_reader_matches_oracle(tmp_path):
     ctx.close()
 
 
+def test_set_bc_matches_the_same_topvoxel_file(tmp_path):
+    # topx_set_bc on a voxel array gives the model that a .TopVoxel file with the same voxels and
+    # boundary conditions gives: fixings with partial directions, repeated nodes (first row
+    # counts), two load cases
+    from top3d_xl_b200 import Context, TopxError
+    rng = np.random.default_rng(4)
+    ny, nx, nz = 9, 18, 8
+    vox = np.ones((ny, nx, nz), bool)
+    vox[rng.random(vox.shape) < 0.1] = False
+    vox[:, :2, :] = True
+    vox[:, -1, :] = True
+    vox[0:3, 5:8, 0:3] = False  # node (y 1, x 6, z 1) touches void voxels only
+    nny, nnx = ny + 1, nx + 1
+    fixed = [(iy + 1 + nny * nnx * iz, 1, 1, int(iz % 2 == 0)) for iz in range(nz + 1) for iy in range(nny)]
+    fixed.append((1, 0, 0, 0))  # repeated node: ignored
+    case1 = [(1 + iy + nny * nx + nny * nnx * 4, 0.0, 0.0, -0.25) for iy in range(4)]
+    case2 = [(1 + iy + nny * nx + nny * nnx * 6, 0.0, 0.3, 0.0) for iy in range(3)]
+    path = str(tmp_path / "bc.TopVoxel")
+    _write_topvoxel(path, vox, fixed, [case1, case2])
+    a = Context()
+    a.load_topvoxel(path)
+    b = Context()
+    b.load_voxels(vox)
+    info = b.set_bc(fixed, [r + (1,) for r in case1] + [r + (2,) for r in case2])
+    assert info.numLoadCases == 2
+    for name in ("ENODMAT", "FIXEDDOFS", "MAPUNIQUEKES"):
+        assert np.array_equal(a.index_array(1, name), b.index_array(1, name)), name
+    for lc in (0, 1):
+        assert np.array_equal(a.load_vector(lc), b.load_vector(lc))
+    m = O.Model()
+    m.load_topvoxel(path)
+    m.apply_boundary_condition()
+    m.setup()
+    assert np.array_equal(b.index_array(1, "FIXEDDOFS"), m.fixedDOFs.astype(np.int32))
+    assert np.array_equal(b.load_vector(1), m.F[:, 1])
+    with pytest.raises(TopxError) as e:  # node id outside the grid
+        b.set_bc([(0, 1, 1, 1)], case1)
+    assert "TOPX_ERR_ARG" in str(e.value)
+    with pytest.raises(TopxError) as e:  # a node outside the solid model
+        b.set_bc(fixed + [(1 + 1 + nny * (6 + nnx * 1), 1, 1, 1)], case1)
+    assert "TOPX_ERR_MODEL" in str(e.value)
+    with pytest.raises(TopxError) as e:  # no loads
+        b.set_bc(fixed, np.empty((0, 5)))
+    assert "TOPX_ERR_MODEL" in str(e.value)
+    a.close()
+    b.close()
+
+
 def test_errors_are_status_codes():
     from top3d_xl_b200 import Context, TopxError
     ctx = Context()

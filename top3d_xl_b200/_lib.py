@@ -87,6 +87,7 @@ SIGNATURES = {
     "topx_version": [],
     "topx_load_voxels": [_P, C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_int],
     "topx_load_topvoxel": [_P, C.c_char_p],
+    "topx_set_bc": [_P, _D, C.c_int64, _D, C.c_int64],
     "topx_get_info": [_P, C.POINTER(Info)],
     "topx_get_ke": [_P, _D],
     "topx_get_index_array": [_P, C.c_int, C.c_int, _I32, _SZ, C.POINTER(_SZ)],

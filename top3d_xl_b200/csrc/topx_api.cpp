@@ -19,6 +19,10 @@ struct topx_ctx {
   std::unique_ptr<topx::Engine> engine;
   std::string err;
   bool begun = false;
+  // the loaded input, to rebuild the model when topx_set_bc replaces its boundary conditions
+  std::vector<uint8_t> vox;
+  int vny = 0, vnx = 0, vnz = 0;
+  std::string topvoxel;
 };
 
 namespace {
@@ -201,6 +205,11 @@ topx_status topx_load_voxels(topx_ctx* ctx, const uint8_t* vox, int nely, int ne
     m->apply_boundary_condition();
     m->setup();
     ctx->model = std::move(m);
+    ctx->vox.assign(vox, vox + size_t(nely) * nelx * nelz);
+    ctx->vny = nely;
+    ctx->vnx = nelx;
+    ctx->vnz = nelz;
+    ctx->topvoxel.clear();
     return TOPX_OK;
   });
 }
@@ -215,6 +224,46 @@ topx_status topx_load_topvoxel(topx_ctx* ctx, const char* path) {
     m->load_topvoxel(path);
     m->apply_boundary_condition();
     m->setup();
+    ctx->model = std::move(m);
+    ctx->topvoxel = path;
+    ctx->vox.clear();
+    return TOPX_OK;
+  });
+}
+
+topx_status topx_set_bc(topx_ctx* ctx, const double* fixing, int64_t nfix, const double* loads, int64_t nload) {
+  return guarded(ctx, [&]() -> topx_status {
+    topx_status s = need_model(ctx);
+    if (s != TOPX_OK) return s;
+    if (nfix < 0 || nload < 0 || (nfix > 0 && !fixing) || (nload > 0 && !loads))
+      return fail(ctx, TOPX_ERR_ARG, "bad boundary-condition arrays");
+    auto node_id = [&](double v) -> int64_t {
+      if (!(v >= 1.0) || v != std::floor(v)) throw std::invalid_argument("boundary-condition node id out of range");
+      return int64_t(v);
+    };
+    // as the .TopVoxel reader: unique node ids, the first row of a node kept
+    std::map<int64_t, std::array<double, 3>> fix;
+    for (int64_t i = 0; i < nfix; ++i) {
+      const double* r = fixing + 4 * i;
+      fix.emplace(node_id(r[0]), std::array<double, 3>{r[1], r[2], r[3]});
+    }
+    std::map<int, std::map<int64_t, std::array<double, 3>>> ld;
+    for (int64_t i = 0; i < nload; ++i) {
+      const double* r = loads + 5 * i;
+      if (!(r[4] >= 1.0) || r[4] != std::floor(r[4]) || r[4] > 1e6) return fail(ctx, TOPX_ERR_ARG, "bad load case");
+      ld[int(r[4])].emplace(node_id(r[0]), std::array<double, 3>{r[1], r[2], r[3]});
+    }
+    std::unique_ptr<topx::Model> m(new topx::Model());
+    apply_params(m->S, ctx->params);
+    if (!ctx->topvoxel.empty())
+      m->load_topvoxel(ctx->topvoxel);
+    else
+      m->load_cuboid(ctx->vox.data(), ctx->vny, ctx->vnx, ctx->vnz);
+    m->set_external_bc(fix, ld);
+    m->apply_boundary_condition();
+    m->setup();
+    ctx->engine.reset();
+    ctx->begun = false;
     ctx->model = std::move(m);
     return TOPX_OK;
   });

@@ -436,31 +436,7 @@ void Model::load_topvoxel(const std::string& path) {
   }
   discretize_level1(*this, vox);
   const Level& l1 = levels[0];
-  // re-index an original-grid node id into the padded node grid
-  const int64_t ony = nely + 1, onx = nelx + 1;
-  const int64_t ANY = l1.resY + 1, ANX = l1.resX + 1;
-  auto adapt = [&](int64_t n1) -> int64_t {
-    const int64_t k = n1 - 1;
-    const int64_t iy = k % ony, ix = (k / ony) % onx, iz = k / (ony * onx);
-    return iy + ANY * ix + ANY * ANX * iz;
-  };
-  fixNode.clear();
-  fixState.clear();
-  for (auto& kv : fix) {
-    fixNode.push_back(l1.nodMapForward[adapt(kv.first)]);
-    fixState.push_back({uint8_t(kv.second[0] == 1), uint8_t(kv.second[1] == 1), uint8_t(kv.second[2] == 1)});
-  }
-  loads.clear();
-  const int nL = ld.empty() ? 1 : ld.rbegin()->first;
-  for (int i = 1; i <= nL; ++i) {
-    LoadCase lc;
-    for (auto& kv : ld[i]) {
-      lc.node.push_back(l1.nodMapForward[adapt(kv.first)]);
-      lc.f.push_back(kv.second);
-    }
-    loads.push_back(lc);
-  }
-  objWeighting.assign(nL, 1.0 / nL);
+  set_external_bc(fix, ld);
   passiveElements.clear();
   for (auto p : passive) {
     const int64_t k = p - 1;
@@ -470,6 +446,45 @@ void Model::load_topvoxel(const std::string& path) {
   }
   std::sort(passiveElements.begin(), passiveElements.end());
   passiveElements.erase(std::unique(passiveElements.begin(), passiveElements.end()), passiveElements.end());
+}
+
+void Model::set_external_bc(const std::map<int64_t, std::array<double, 3>>& fix,
+                            const std::map<int, std::map<int64_t, std::array<double, 3>>>& ld) {
+  const Level& l1 = levels.at(0);
+  // re-index an original-grid node id into the padded node grid
+  const int64_t ony = nely + 1, onx = nelx + 1;
+  const int64_t ANY = l1.resY + 1, ANX = l1.resX + 1;
+  const int64_t nOrig = ony * onx * (int64_t(nelz) + 1);
+  auto adapt = [&](int64_t n1) -> int64_t {
+    if (n1 < 1 || n1 > nOrig) throw std::invalid_argument("boundary-condition node id out of range");
+    const int64_t k = n1 - 1;
+    const int64_t iy = k % ony, ix = (k / ony) % onx, iz = k / (ony * onx);
+    return iy + ANY * ix + ANY * ANX * iz;
+  };
+  fixNode.clear();
+  fixState.clear();
+  auto solid = [&](int64_t n1) -> int32_t {
+    const int32_t n = l1.nodMapForward[adapt(n1)];
+    if (n <= 0) throw std::runtime_error("boundary-condition node is not a node of the solid model");
+    return n;
+  };
+  for (auto& kv : fix) {
+    fixNode.push_back(solid(kv.first));
+    fixState.push_back({uint8_t(kv.second[0] == 1), uint8_t(kv.second[1] == 1), uint8_t(kv.second[2] == 1)});
+  }
+  loads.clear();
+  const int nL = ld.empty() ? 1 : ld.rbegin()->first;
+  for (int i = 1; i <= nL; ++i) {
+    LoadCase lc;
+    const auto it = ld.find(i);
+    if (it != ld.end())
+      for (auto& kv : it->second) {
+        lc.node.push_back(solid(kv.first));
+        lc.f.push_back(kv.second);
+      }
+    loads.push_back(lc);
+  }
+  objWeighting.assign(nL, 1.0 / nL);
 }
 
 void Model::apply_boundary_condition() {

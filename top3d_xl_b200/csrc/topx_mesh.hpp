@@ -9,6 +9,7 @@
 #include <array>
 #include <cstdint>
 #include <string>
+#include <map>
 #include <vector>
 
 namespace topx {
@@ -80,6 +81,12 @@ struct Model {
   // build steps
   void load_cuboid(const uint8_t* vox, int ny, int nx, int nz);
   void load_topvoxel(const std::string& path);
+  // fixings (node -> fixed flags per direction, a direction fixed where its value is 1) and loads
+  // (load case from 1 -> node -> force) with node ids 1-based in the input model's own
+  // (nely+1) x (nelx+1) x (nelz+1) node grid, as a .TopVoxel file gives them; replaces the
+  // model's fixings, loads and load-case weights (AdaptBCExternalMdl, TOP3D_XL.m:1439-1490)
+  void set_external_bc(const std::map<int64_t, std::array<double, 3>>& fix,
+                       const std::map<int, std::map<int64_t, std::array<double, 3>>>& ld);
   void apply_boundary_condition();
   void setup();  // Ke + hierarchy + BC element matrices
 };

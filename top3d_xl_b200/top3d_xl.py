@@ -91,6 +91,19 @@ class Context:
         self._check(self.lib.topx_load_topvoxel(self._h, os.fsencode(path)))
         return self._load_info()
 
+    def set_bc(self, fixing, loads):
+        """Boundary conditions as a .TopVoxel file gives them (topx_set_bc): ``fixing`` rows
+        (node, fixX, fixY, fixZ), ``loads`` rows (node, Fx, Fy, Fz[, loadCase]) with 1-based node
+        ids of the input model's (nely+1, nelx+1, nelz+1) node grid, y fastest."""
+        fx = np.ascontiguousarray(np.asarray(fixing, dtype=np.float64).reshape(-1, 4))
+        ld = np.asarray(loads, dtype=np.float64)
+        ld = ld.reshape(-1, ld.shape[-1] if ld.ndim > 1 else 5)
+        if ld.shape[1] == 4:
+            ld = np.column_stack([ld, np.ones(len(ld))])
+        ld = np.ascontiguousarray(ld)
+        self._check(self.lib.topx_set_bc(self._h, _dptr(fx), len(fx), _dptr(ld), len(ld)))
+        return self._load_info()
+
     def _load_info(self):
         inf = L.Info()
         self._check(self.lib.topx_get_info(self._h, C.byref(inf)))
