@@ -67,6 +67,9 @@ typedef struct topx_params {
   int typeVcycle;          /* TOPX_VCYCLE_ADAPTED (default, the reference's setting) or
                               TOPX_VCYCLE_STANDARD (smoothing against K x on every level; FP64 only,
                               otherwise topx_create returns TOPX_ERR_ARG) */
+  int specifyPassiveRegions[3]; /* specifyPassiveRegions_ (TX:37): layers of passive elements on the
+                              boundary, near loads, near fixations; {0, 0, 0} (default) adds none.
+                              Applied when a model is loaded (TopOpti_SetPassiveElements, TX:1511) */
 } topx_params;
 
 /* sizes of the loaded model */
@@ -106,7 +109,8 @@ enum {
   TOPX_ARR_SOLIDNODEMAP = 7,       /* solidNodeMapCoarser2Finer (levels >= 2) */
   TOPX_ARR_FIXEDDOFS = 8,          /* numDOFs 0/1 (level 1) */
   TOPX_ARR_MAPUNIQUEKES = 9,       /* numElements (level 1) */
-  TOPX_ARR_ISTHISELE2NDLEVEL = 10  /* level-2 elements holding fixed DOFs (level 2) */
+  TOPX_ARR_ISTHISELE2NDLEVEL = 10, /* level-2 elements holding fixed DOFs (level 2) */
+  TOPX_ARR_PASSIVEELEMENTS = 11    /* passiveElements_, sorted compact ids (level 1) */
 };
 
 /* ---- lifecycle ------------------------------------------------------------ */

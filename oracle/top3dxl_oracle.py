@@ -493,6 +493,63 @@ class Model:
         self.fixedDOFs = np.zeros(l1.numDOFs, dtype=bool)
         self.fixedDOFs[fixed - 1] = True
 
+    def include_adjacent_elements(self, eles):
+        """Common_IncludeAdjacentElements (TX:1578-1606): the elements of the 3x3x3 block of padded
+        grid cells around each listed element, compact ids, sorted unique."""
+        l1 = self.levels[0]
+        ny, nx, nz = l1.resY, l1.resX, l1.resZ
+        g = l1.eleMapBack[np.asarray(eles, dtype=np.int64) - 1].astype(np.int64) - 1
+        iy, ix, iz = g % ny, (g // ny) % nx, g // (ny * nx)
+        out = []
+        for dz in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    y, x, z = iy + dy, ix + dx, iz + dz
+                    ok = (y >= 0) & (y < ny) & (x >= 0) & (x < nx) & (z >= 0) & (z < nz)
+                    out.append(l1.eleMapForward[(y + ny * (x + nx * z))[ok]])
+        out = np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
+        return np.unique(out[out > 0]).astype(np.int64)
+
+    def set_passive_elements(self):
+        """TopOpti_SetPassiveElements (TX:1511-1574) for S.specifyPassiveRegions = (layers on the
+        boundary, near loads, near fixations).  As written, the loaded and fixed node ids (compact)
+        index the list of boundary nodes (TX:1557, 1569); an id past its end is MATLAB's index
+        error."""
+        l1 = self.levels[0]
+        nb, nl, nf = (int(mround(v)) for v in self.S.specifyPassiveRegions)
+        existing = self.passiveElements
+        on_b = np.zeros(0, dtype=np.int64)
+        if nb > 0:
+            on_b = l1.elementsOnBoundary.astype(np.int64)
+            for _ in range(2, nb + 1):
+                on_b = self.include_adjacent_elements(on_b)
+        near_l = np.zeros(0, dtype=np.int64)
+        near_f = np.zeros(0, dtype=np.int64)
+        if nl > 0 or nf > 0:
+            # node -> boundary elements containing it (TX:1536-1548)
+            node_eles = {}
+            for e in np.sort(l1.elementsOnBoundary.astype(np.int64)):
+                for n in l1.eNodMat[e - 1]:
+                    node_eles.setdefault(int(n), []).append(int(e))
+            nob = l1.nodesOnBoundary.astype(np.int64)
+
+            def around(ids):
+                ids = np.asarray(ids, dtype=np.int64)
+                if ids.size and (ids.min() < 1 or ids.max() > nob.size):
+                    raise IndexError("Index exceeds the number of array elements (nodesOnBoundary)")
+                es = [e for n in nob[ids - 1] for e in node_eles.get(int(n), [])]
+                return np.unique(np.array(es, dtype=np.int64))
+
+            if nl > 0:
+                near_l = np.concatenate([around(iL[:, 0]) for iL in self.loadingCond])
+                for _ in range(2, nl + 1):
+                    near_l = self.include_adjacent_elements(near_l)
+            if nf > 0:
+                near_f = around(self.fixingCond[:, 0])
+                for _ in range(2, nf + 1):
+                    near_f = self.include_adjacent_elements(near_f)
+        self.passiveElements = np.unique(np.concatenate([existing, on_b, near_l, near_f])).astype(np.int64)
+
     def setup(self):
         """FEA_SetupVoxelBased (TX:1238-1252) + BCs on Ke (TX:1338-1437)."""
         S = self.S
@@ -1058,6 +1115,7 @@ def build_model(input_model, S: Settings | None = None) -> Model:
         m.load_cuboid(input_model)
     m.apply_boundary_condition()
     m.setup()
+    m.set_passive_elements()  # TX:79 / 272
     return m
 
 

@@ -169,6 +169,45 @@ def test_set_bc_matches_the_same_topvoxel_file(tmp_path):
     b.close()
 
 
+def test_passive_layers_match_oracle(tmp_path):
+    # specifyPassiveRegions_ (TopOpti_SetPassiveElements, TX:1511-1574): boundary layers on a cuboid;
+    # layers near loads and fixations on a model whose BC node ids lie within the boundary-node
+    # list (the reference indexes that list with them); the built-in cuboid's fixed node ids run
+    # past it, which is the reference's index error
+    from top3d_xl_b200 import Context, TopxError
+    vox = np.ones((8, 16, 8), bool)
+    S = O.Settings()
+    S.specifyPassiveRegions = (2, 0, 0)
+    m = O.build_model(vox, S)
+    with Context(specifyPassiveRegions=(2, 0, 0)) as ctx:
+        info = ctx.load_voxels(vox)
+        assert info.numPassive == len(m.passiveElements) > 0
+        assert np.array_equal(ctx.index_array(1, "PASSIVEELEMENTS"), m.passiveElements.astype(np.int32))
+    ny, nx, nz = 6, 12, 6
+    v2 = np.ones((ny, nx, nz), bool)
+    nny = ny + 1
+    fixed = [(iy + 1, 1, 1, 1) for iy in range(nny)]            # x = 0, z = 0 column
+    loads = [[(nny + iy + 1, 0.0, 0.0, -0.5) for iy in range(2)],  # x = 1, z = 0
+             [(2 * nny + iy + 1, 0.2, 0.0, 0.0) for iy in range(3)]]
+    path = str(tmp_path / "p.TopVoxel")
+    _write_topvoxel(path, v2, fixed, loads, passive=[3])
+    for reg in ((0, 2, 1), (1, 1, 2)):
+        S = O.Settings()
+        S.specifyPassiveRegions = reg
+        mo = O.build_model(path, S)
+        with Context(specifyPassiveRegions=reg) as ctx:
+            ctx.load_topvoxel(path)
+            assert np.array_equal(ctx.index_array(1, "PASSIVEELEMENTS"), mo.passiveElements.astype(np.int32)), reg
+    S = O.Settings()
+    S.specifyPassiveRegions = (0, 0, 1)
+    with pytest.raises(IndexError):
+        O.build_model(vox, S)
+    with Context(specifyPassiveRegions=(0, 0, 1)) as ctx:
+        with pytest.raises(TopxError) as e:
+            ctx.load_voxels(vox)
+        assert "TOPX_ERR_MODEL" in str(e.value)
+
+
 def test_errors_are_status_codes():
     from top3d_xl_b200 import Context, TopxError
     ctx = Context()

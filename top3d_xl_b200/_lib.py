@@ -17,7 +17,7 @@ ERRORS = {-1: "TOPX_ERR_ARG", -2: "TOPX_ERR_STATE", -3: "TOPX_ERR_CUDA", -4: "TO
 
 ARR = dict(ENODMAT=0, ELEMAPBACK=1, NODMAPBACK=2, NODESONBOUNDARY=3, ELEMENTSONBOUNDARY=4,
            ELEMENTUPWARDMAP=5, TRANSFERMAT=6, SOLIDNODEMAP=7, FIXEDDOFS=8, MAPUNIQUEKES=9,
-           ISTHISELE2NDLEVEL=10)
+           ISTHISELE2NDLEVEL=10, PASSIVEELEMENTS=11)
 
 
 class Params(C.Structure):
@@ -25,7 +25,7 @@ class Params(C.Structure):
                 ("SIMPpenalty", C.c_double), ("cellSize", C.c_double), ("tol", C.c_double),
                 ("maxIT", C.c_int), ("weightFactorJacobi", C.c_double),
                 ("coarsestResolutionControl", C.c_int64), ("precision", C.c_int), ("device", C.c_int),
-                ("coarse_coop", C.c_int), ("typeVcycle", C.c_int)]
+                ("coarse_coop", C.c_int), ("typeVcycle", C.c_int), ("specifyPassiveRegions", C.c_int * 3)]
 
 
 class Info(C.Structure):

@@ -63,6 +63,7 @@ void apply_params(topx::Settings& S, const topx_params& p) {
   S.weightFactorJacobi = p.weightFactorJacobi;
   S.coarsestResolutionControl = p.coarsestResolutionControl;
   S.typeVcycle = p.typeVcycle;
+  for (int i = 0; i < 3; ++i) S.specifyPassiveRegions[i] = p.specifyPassiveRegions[i];
 }
 
 topx_status need_model(topx_ctx* c) {
@@ -154,6 +155,7 @@ topx_status topx_default_params(topx_params* p) {
   p->device = 0;
   p->coarse_coop = 1;
   p->typeVcycle = TOPX_VCYCLE_ADAPTED;
+  for (int i = 0; i < 3; ++i) p->specifyPassiveRegions[i] = 0;
   return TOPX_OK;
 }
 
@@ -204,6 +206,7 @@ topx_status topx_load_voxels(topx_ctx* ctx, const uint8_t* vox, int nely, int ne
     m->load_cuboid(vox, nely, nelx, nelz);
     m->apply_boundary_condition();
     m->setup();
+    m->set_passive_elements();
     ctx->model = std::move(m);
     ctx->vox.assign(vox, vox + size_t(nely) * nelx * nelz);
     ctx->vny = nely;
@@ -224,6 +227,7 @@ topx_status topx_load_topvoxel(topx_ctx* ctx, const char* path) {
     m->load_topvoxel(path);
     m->apply_boundary_condition();
     m->setup();
+    m->set_passive_elements();
     ctx->model = std::move(m);
     ctx->topvoxel = path;
     ctx->vox.clear();
@@ -262,6 +266,7 @@ topx_status topx_set_bc(topx_ctx* ctx, const double* fixing, int64_t nfix, const
     m->set_external_bc(fix, ld);
     m->apply_boundary_condition();
     m->setup();
+    m->set_passive_elements();
     ctx->engine.reset();
     ctx->begun = false;
     ctx->model = std::move(m);
@@ -334,6 +339,7 @@ topx_status topx_get_index_array(const topx_ctx* cctx, int level, int which, int
         break;
       case TOPX_ARR_MAPUNIQUEKES: src = &M.mapUniqueKes; break;
       case TOPX_ARR_ISTHISELE2NDLEVEL: src = &M.isThisEle2ndLevel; break;
+      case TOPX_ARR_PASSIVEELEMENTS: src = &M.passiveElements; break;
       default: return fail(ctx, TOPX_ERR_ARG, "bad array id");
     }
     if (n_needed) *n_needed = src->size();

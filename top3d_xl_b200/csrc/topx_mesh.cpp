@@ -487,6 +487,82 @@ void Model::set_external_bc(const std::map<int64_t, std::array<double, 3>>& fix,
   objWeighting.assign(nL, 1.0 / nL);
 }
 
+// Common_IncludeAdjacentElements (TOP3D_XL.m:1578-1606): the elements of the 3x3x3 block of padded
+// grid cells around each listed element, sorted unique compact ids
+static std::vector<int32_t> include_adjacent_elements(const Level& l1, const std::vector<int32_t>& in) {
+  const int64_t ny = l1.resY, nx = l1.resX, nz = l1.resZ;
+  std::vector<int32_t> out;
+  out.reserve(in.size() * 27);
+  for (int32_t e : in) {
+    const int64_t g = l1.eleMapBack[e - 1] - 1;
+    const int64_t iy = g % ny, ix = (g / ny) % nx, iz = g / (ny * nx);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int64_t y = iy + dy, x = ix + dx, z = iz + dz;
+          if (y < 0 || y >= ny || x < 0 || x >= nx || z < 0 || z >= nz) continue;
+          const int32_t f = l1.eleMapForward[y + ny * (x + nx * z)];
+          if (f > 0) out.push_back(f);
+        }
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return out;
+}
+
+void Model::set_passive_elements() {
+  // TopOpti_SetPassiveElements (TOP3D_XL.m:1511-1574).  As written there, the loaded and fixed
+  // node ids (compact) index the list of boundary nodes (TOP3D_XL.m:1557, 1569); an id past its end
+  // is MATLAB's index error.
+  const int nb = S.specifyPassiveRegions[0], nl = S.specifyPassiveRegions[1], nf = S.specifyPassiveRegions[2];
+  if (nb <= 0 && nl <= 0 && nf <= 0) return;
+  const Level& l1 = levels.at(0);
+  std::vector<int32_t> all = passiveElements;
+  if (nb > 0) {
+    std::vector<int32_t> onB = l1.elementsOnBoundary;
+    for (int i = 2; i <= nb; ++i) onB = include_adjacent_elements(l1, onB);
+    all.insert(all.end(), onB.begin(), onB.end());
+  }
+  if (nl > 0 || nf > 0) {
+    // node -> the boundary elements containing it (TOP3D_XL.m:1536-1548)
+    std::vector<std::vector<int32_t>> nodeEles(size_t(l1.numNodes) + 1);
+    std::vector<int32_t> be = l1.elementsOnBoundary;
+    std::sort(be.begin(), be.end());
+    for (int32_t e : be)
+      for (int j = 0; j < 8; ++j) nodeEles[l1.eNodMat[size_t(e - 1) * 8 + j]].push_back(e);
+    const auto& nob = l1.nodesOnBoundary;
+    auto around = [&](const std::vector<int32_t>& ids) {
+      std::vector<int32_t> es;
+      for (int32_t id : ids) {
+        if (id < 1 || size_t(id) > nob.size())
+          throw std::runtime_error("passive layers near loads or fixations: node id exceeds the boundary-node list");
+        const auto& v = nodeEles[nob[id - 1]];
+        es.insert(es.end(), v.begin(), v.end());
+      }
+      std::sort(es.begin(), es.end());
+      es.erase(std::unique(es.begin(), es.end()), es.end());
+      return es;
+    };
+    if (nl > 0) {
+      std::vector<int32_t> nearL;
+      for (const auto& lc : loads) {
+        const auto es = around(lc.node);
+        nearL.insert(nearL.end(), es.begin(), es.end());
+      }
+      for (int i = 2; i <= nl; ++i) nearL = include_adjacent_elements(l1, nearL);
+      all.insert(all.end(), nearL.begin(), nearL.end());
+    }
+    if (nf > 0) {
+      std::vector<int32_t> nearF = around(fixNode);
+      for (int i = 2; i <= nf; ++i) nearF = include_adjacent_elements(l1, nearF);
+      all.insert(all.end(), nearF.begin(), nearF.end());
+    }
+  }
+  std::sort(all.begin(), all.end());
+  all.erase(std::unique(all.begin(), all.end()), all.end());
+  passiveElements = all;
+}
+
 void Model::apply_boundary_condition() {
   // FEA_ApplyBoundaryCondition (TOP3D_XL.m:1294-1336)
   if (loads.empty()) throw std::runtime_error("No Loads!");

@@ -26,6 +26,7 @@ struct Settings {
   double weightFactorJacobi = 0.6;
   int64_t coarsestResolutionControl = 50000;
   int typeVcycle = 0;  // 0 'Adapted' (the reference's setting), 1 'Standard' (TX:34)
+  int specifyPassiveRegions[3] = {0, 0, 0};  // layers on the boundary, near loads, near fixations (TX:37)
   int nonDyadic = 1;
 };
 
@@ -89,6 +90,8 @@ struct Model {
                        const std::map<int, std::map<int64_t, std::array<double, 3>>>& ld);
   void apply_boundary_condition();
   void setup();  // Ke + hierarchy + BC element matrices
+  // TopOpti_SetPassiveElements (TOP3D_XL.m:1511-1574) for S.specifyPassiveRegions, after setup
+  void set_passive_elements();
 };
 
 // Element matrices (TOP3D_XL.m:1254-1292, 1768-1798, 1617-1627, 816-853)

@@ -3,14 +3,21 @@
 %% Same signature, argument checks, console lines and ./out/ files as the reference, including
 %% DesignVolume.nii (the padded density volume) and DesignVolume.stl (its 0.5 isosurface with caps).
 %% Optional trailing name/value pairs: 'precision', 'fp64' | 'mixed'; 'typeVcycle',
-%% 'Adapted' (default, the reference's typeVcycle_) | 'Standard' (FP64 only).
+%% 'Adapted' (default, the reference's typeVcycle_) | 'Standard' (FP64 only);
+%% 'specifyPassiveRegions', [#LayersBoundary #LayersLoads #LayersFixations] (default [0 0 0]).
 function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
 	precision = 'fp64';
 	typeVcycle = 'Adapted';
+	passiveRegions = [0 0 0];
 	rHat = [];
 	args = varargin;
-	while numel(args) >= 2 && ischar(args{end-1}) && any(strcmp(args{end-1}, {'precision', 'typeVcycle'}))
-		if strcmp(args{end-1}, 'precision'), precision = args{end}; else, typeVcycle = args{end}; end
+	while numel(args) >= 2 && ischar(args{end-1}) && ...
+			any(strcmp(args{end-1}, {'precision', 'typeVcycle', 'specifyPassiveRegions'}))
+		switch args{end-1}
+			case 'precision', precision = args{end};
+			case 'typeVcycle', typeVcycle = args{end};
+			otherwise, passiveRegions = args{end};
+		end
 		args = args(1:end-2);
 	end
 	switch consType
@@ -27,7 +34,8 @@ function TOP3D_XL(inputModel, consType, V0, nLoop, rMin, varargin)
 	outPath = './out/'; if ~exist(outPath, 'dir'), mkdir(outPath); end
 	fid = fopen(strcat(outPath, 'RunLog.log'), 'w'); fclose(fid); diary(strcat(outPath, 'RunLog.log'));
 	tStartTotal = tic;
-	[hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision, typeVcycle);
+	[hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision, typeVcycle, ...
+		double(passiveRegions));
 	disp(['Compliance of Fully Solid Domain: ' sprintf('%16.6e', hist.cSolid)]);
 	for loop = 1:numel(hist.c)
 		if strcmp(consType, 'GLOBAL')

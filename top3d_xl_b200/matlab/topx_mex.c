@@ -90,6 +90,11 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   topx_default_params(&p);
   p.precision = strcmp(prec, "mixed") == 0 ? TOPX_MIXED : TOPX_FP64;
   p.typeVcycle = strcmp(vcyc, "Standard") == 0 ? TOPX_VCYCLE_STANDARD : TOPX_VCYCLE_ADAPTED;
+  if (nrhs >= 9) {
+    if (!mxIsNumeric(prhs[8]) || mxGetNumberOfElements(prhs[8]) != 3)
+      mexErrMsgIdAndTxt("topx:arg", "specifyPassiveRegions must have 3 entries");
+    for (k = 0; k < 3; ++k) p.specifyPassiveRegions[k] = (int)(mxGetPr(prhs[8])[k] + (mxGetPr(prhs[8])[k] >= 0 ? 0.5 : -0.5));
+  }
   topx_mex_cleanup();
   check(topx_create(&g_ctx, &p), "topx_create");
   mexAtExit(topx_mex_cleanup);

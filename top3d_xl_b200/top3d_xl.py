@@ -49,6 +49,8 @@ class Context:
                 if v not in ("Adapted", "Standard"):
                     raise ValueError("typeVcycle must be 'Adapted' or 'Standard'")
                 v = 0 if v == "Adapted" else 1
+            if k == "specifyPassiveRegions":
+                v = (C.c_int * 3)(*[int(round(t)) for t in v])
             setattr(p, k, v)
         self.params = p
         self._h = C.c_void_p()
