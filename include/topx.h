@@ -40,7 +40,9 @@ enum {
   TOPX_ERR_CUDA = -3,     /* CUDA runtime error or no usable device */
   TOPX_ERR_MODEL = -4,    /* model/BC error (format, no loads, no fixations, unsupported BCs) */
   TOPX_ERR_NUMERIC = -5,  /* solver failure (MMA dual solve did not finish, non-finite values) */
-  TOPX_ERR_INTERNAL = -6
+  TOPX_ERR_INTERNAL = -6,
+  TOPX_ERR_TIMEOUT = -7   /* a bounded wait inside a kernel gave up (its poll limit, about a second,
+                             ran out); the error word was cleared and the context stays usable */
 };
 
 enum { TOPX_GLOBAL = 0, TOPX_LOCAL = 1 };        /* consType (TX:12-18) */
@@ -84,6 +86,11 @@ typedef struct topx_info {
   int64_t numPassive;
 } topx_info;
 
+/* Load cases a model may have.  The reference allows any number (TX:483-493); a model with more
+   is refused by topx_load_topvoxel / topx_set_bc with TOPX_ERR_MODEL, so that no history row
+   (topx_iter.its) is ever truncated. */
+#define TOPX_MAX_LOAD_CASES 8
+
 /* one optimisation iteration (history row of TX:186-191 / TX:393-399) */
 typedef struct topx_iter {
   int loop;
@@ -92,7 +99,7 @@ typedef struct topx_iter {
   double sharp;    /* sharpness after the update */
   double cons;     /* fval: constraint value */
   double change;   /* max density change */
-  int its[8];      /* PCG iterations per load case (iters_Target.dat) */
+  int its[TOPX_MAX_LOAD_CASES]; /* PCG iterations per load case (iters_Target.dat) */
   int filter_its;  /* PDE-filter PCG iterations summed over the filters of this iteration */
   double t_assemble, t_cg, t_opt, t_filter, t_total;  /* seconds */
 } topx_iter;
@@ -158,7 +165,11 @@ topx_status topx_ku(topx_ctx* ctx, const double* u, double* y, size_t ndof);
    array, enough for level-1 grids of up to 699,040 padded nodes; larger models get
    TOPX_ERR_ARG.  The context's device state must exist already (e.g. after topx_set_moduli).
    The first call on each GPU looks up the array's address; make it before any stream capture.
-   All calls share the array: calls that overlap on the GPU race.  Returns after y is written. */
+   All calls share the array: calls that overlap on the GPU race.  The call runs after the work
+   already queued on the legacy default stream (stream 0), so u may be written there
+   asynchronously just before; work pending on the caller's other streams (non-blocking or
+   per-thread default streams) is not waited for and must be synchronised by the caller.
+   Returns after y is written. */
 topx_status topx_ku_noalloc(topx_ctx* ctx, const double* u_dev, double* y_dev, size_t ndof);
 /* Solving_AssembleFEAstencil (TX:919-1066) for the current moduli */
 topx_status topx_assemble(topx_ctx* ctx);
@@ -198,6 +209,16 @@ topx_status topx_get_density(topx_ctx* ctx, double* out, size_t ne);
 topx_status topx_set_density(topx_ctx* ctx, const double* xPhys, size_t ne);
 /* displacement U(:,lc), interleaved DOFs */
 topx_status topx_get_displacement(topx_ctx* ctx, int lc, double* out, size_t ndof);
+
+/* ---- failure handling (no reference counterpart) ----------------------------- */
+/* Test of the give-up path of the kernels' bounded waits: runs one wait primitive against a word
+   that nothing writes, so that it exhausts its poll limit (about a second) and sets its error
+   word.  which: 0 the coarse solve's grid barrier (a CTA that never arrives), 1 its wait for one
+   solve-vector entry, 2 its wait for a vector of entries (0-2 need the cooperative coarse solve,
+   topx_params.coarse_coop = 1), 3 the coarse Gauss-Jordan inverse's dependency wait.  Returns
+   TOPX_ERR_TIMEOUT with a message naming the wait, as a real give-up inside a solve would; the
+   context stays usable. */
+topx_status topx_selftest_wait(topx_ctx* ctx, int which);
 
 /* ---- measurement (no reference counterpart) --------------------------------- */
 #define TOPX_PROFILE_SECTIONS 14

@@ -165,6 +165,17 @@ def test_set_bc_matches_the_same_topvoxel_file(tmp_path):
     with pytest.raises(TopxError) as e:  # no loads
         b.set_bc(fixed, np.empty((0, 5)))
     assert "TOPX_ERR_MODEL" in str(e.value)
+    # more load cases than a history row holds (TOPX_MAX_LOAD_CASES = 8) are refused, not truncated
+    many = [(1 + iy + nny * nx + nny * nnx * 4, 0.0, 0.0, -0.25, lc) for lc in range(1, 10) for iy in range(2)]
+    assert b.set_bc(fixed, many[:16]).numLoadCases == 8
+    with pytest.raises(TopxError) as e:
+        b.set_bc(fixed, many)
+    assert "TOPX_ERR_MODEL" in str(e.value) and "load cases" in str(e.value)
+    path9 = str(tmp_path / "bc9.TopVoxel")
+    _write_topvoxel(path9, vox, fixed, [[r[:4] for r in many if r[4] == lc] for lc in range(1, 10)])
+    with pytest.raises(TopxError) as e:
+        a.load_topvoxel(path9)
+    assert "TOPX_ERR_MODEL" in str(e.value) and "load cases" in str(e.value)
     a.close()
     b.close()
 

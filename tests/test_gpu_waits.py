@@ -1,0 +1,63 @@
+"""Give-up path of the kernels' bounded waits, on the GPU, through the C ABI.
+
+The coarsest-level solve polls for its grid barrier and for the solve-vector entries that other
+CTAs produce, and the coarse Gauss-Jordan inverse polls the version words of the tiles it reads.
+Each wait has a poll limit (about a second), after which it sets an error word and its kernel
+returns; the host reads the word after the stream synchronises, clears it and raises
+TOPX_ERR_TIMEOUT.  topx_selftest_wait runs each wait primitive against a word that nothing
+writes (no kernel faults, traps or spins without a limit), so the limit must run out.  The test
+then checks the status and message, and that the same context still computes the V-cycle and
+the PCG solve exactly as before and as the oracle does.
+"""
+import numpy as np
+import pytest
+
+from oracle import top3dxl_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOPX_ERR_TIMEOUT = -7
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def setup():
+    from top3d_xl_b200 import Context
+    vox = np.ones((12, 24, 12), bool)
+    m = O.build_model(vox)
+    ctx = Context("fp64")
+    ctx.load_voxels(vox)
+    x = np.random.default_rng(1).uniform(0.05, 1.0, m.levels[0].numElements)
+    E = m.S.modulusMin + x ** m.S.SIMPpenalty * (m.S.modulus - m.S.modulusMin)
+    ctx.set_moduli(E)
+    ctx.assemble()
+    sol = O.Solver(m)
+    sol.assemble(E)
+    r = np.random.default_rng(3).standard_normal(m.levels[0].numDOFs)
+    yield dict(ctx=ctx, m=m, sol=sol, r=r, z0=ctx.vcycle(r), u0=ctx.pcg())
+    ctx.close()
+
+
+@pytest.mark.parametrize("which,needle", [(0, b"grid barrier"), (1, b"solve vector"), (2, b"solve vector"),
+                                          (3, b"Gauss-Jordan")])
+def test_bounded_wait_gives_up_and_context_stays_usable(setup, which, needle):
+    ctx = setup["ctx"]
+    st = ctx.lib.topx_selftest_wait(ctx._h, which)
+    assert st == TOPX_ERR_TIMEOUT, (st, ctx.lib.topx_last_error(ctx._h))
+    assert needle in ctx.lib.topx_last_error(ctx._h)
+    # the error word was cleared: the factorisation, the cooperative solve and the PCG run as before
+    ctx.assemble()
+    z = ctx.vcycle(setup["r"])
+    assert _rel(z, setup["z0"]) < 1e-14
+    assert _rel(z, setup["sol"].vcycle(setup["r"])) < 1e-11
+    u, its = ctx.pcg()
+    assert its == setup["u0"][1]
+    assert _rel(u, setup["u0"][0]) < 1e-12
+
+
+def test_bad_selftest_case_is_refused(setup):
+    ctx = setup["ctx"]
+    assert ctx.lib.topx_selftest_wait(ctx._h, 7) == -1  # TOPX_ERR_ARG

@@ -31,6 +31,11 @@ def _cudart():
         rt.cudaFree.argtypes = [C.c_void_p]
         rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
         rt.cudaMemset.argtypes = [C.c_void_p, C.c_int, C.c_size_t]
+        rt.cudaMemsetAsync.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]
+        rt.cudaMemcpyAsync.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]
+        rt.cudaMallocHost.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+        rt.cudaFreeHost.argtypes = [C.c_void_p]
+        rt.cudaDeviceSynchronize.argtypes = []
         return rt
     pytest.skip("libcudart not found")
 
@@ -114,4 +119,37 @@ def test_ku_noalloc_refuses_models_beyond_the_fixed_scratch():
         assert st == -1  # TOPX_ERR_ARG
         assert b"fixed scratch" in ctx.lib.topx_last_error(ctx._h)
     finally:
+        ctx.close()
+
+
+def test_ku_noalloc_runs_after_work_queued_on_the_default_stream():
+    """A gpuArray-style caller writes u on the legacy default stream and calls at once, with no
+    synchronisation in between: the call must see the finished u (the stream 0 work is first
+    a NaN fill of u, then the asynchronous copy of its values from page-locked memory)."""
+    rt = _cudart()
+    ctx = _model(np.ones((24, 48, 24), bool), 4)
+    hbuf = C.c_void_p()
+    try:
+        ndof = ctx.numDOFs
+        u = np.random.default_rng(7).standard_normal(ndof)
+        y_ref = ctx.ku(u)
+        assert rt.cudaMallocHost(C.byref(hbuf), 8 * ndof) == 0
+        C.memmove(hbuf, u.ctypes.data, 8 * ndof)
+        du, dy = _DeviceVector(rt, ndof), _DeviceVector(rt, ndof)
+        try:
+            for _ in range(2):
+                assert rt.cudaMemsetAsync(du.p, 0xFF, 8 * ndof, None) == 0
+                assert rt.cudaMemcpyAsync(du.p, hbuf, 8 * ndof, H2D, None) == 0
+                st = ctx.lib.topx_ku_noalloc(ctx._h, du.p, dy.p, ndof)
+                assert st == 0, ctx.lib.topx_last_error(ctx._h)
+                y = dy.download()
+                assert np.all(np.isfinite(y))
+                assert _rel(y, y_ref) <= KU_REL_TOL, _rel(y, y_ref)
+        finally:
+            rt.cudaDeviceSynchronize()
+            du.free()
+            dy.free()
+    finally:
+        if hbuf.value:
+            rt.cudaFreeHost(hbuf)
         ctx.close()

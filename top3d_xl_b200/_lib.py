@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libtopx.so")
 
 TOPX_OK, TOPX_STOP = 0, 1
 ERRORS = {-1: "TOPX_ERR_ARG", -2: "TOPX_ERR_STATE", -3: "TOPX_ERR_CUDA", -4: "TOPX_ERR_MODEL",
-          -5: "TOPX_ERR_NUMERIC", -6: "TOPX_ERR_INTERNAL"}
+          -5: "TOPX_ERR_NUMERIC", -6: "TOPX_ERR_INTERNAL", -7: "TOPX_ERR_TIMEOUT"}
 
 ARR = dict(ENODMAT=0, ELEMAPBACK=1, NODMAPBACK=2, NODESONBOUNDARY=3, ELEMENTSONBOUNDARY=4,
            ELEMENTUPWARDMAP=5, TRANSFERMAT=6, SOLIDNODEMAP=7, FIXEDDOFS=8, MAPUNIQUEKES=9,
@@ -97,6 +97,7 @@ SIGNATURES = {
     "topx_ku": [_P, _D, _D, _SZ],
     "topx_ku_noalloc": [_P, C.c_void_p, C.c_void_p, _SZ],
     "topx_assemble": [_P],
+    "topx_selftest_wait": [_P, C.c_int],
     "topx_vcycle": [_P, _D, _D, _SZ],
     "topx_write_design_nii": [_D, C.c_int, C.c_int, C.c_int, C.c_char_p],
     "topx_write_design_stl": [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_char_p, C.POINTER(C.c_int64)],

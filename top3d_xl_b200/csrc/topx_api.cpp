@@ -39,6 +39,8 @@ topx_status guarded(topx_ctx* c, F&& f) {
     return f();
   } catch (const topx::CudaError& e) {
     return fail(c, TOPX_ERR_CUDA, e.what());
+  } catch (const topx::DeviceWaitError& e) {
+    return fail(c, TOPX_ERR_TIMEOUT, e.what());
   } catch (const std::invalid_argument& e) {
     return fail(c, TOPX_ERR_ARG, e.what());
   } catch (const std::runtime_error& e) {
@@ -64,6 +66,14 @@ void apply_params(topx::Settings& S, const topx_params& p) {
   S.coarsestResolutionControl = p.coarsestResolutionControl;
   S.typeVcycle = p.typeVcycle;
   for (int i = 0; i < 3; ++i) S.specifyPassiveRegions[i] = p.specifyPassiveRegions[i];
+}
+
+// The history rows carry at most TOPX_MAX_LOAD_CASES PCG counts: refuse larger models
+// instead of dropping the counts of the further load cases.
+void check_load_cases(const topx::Model& m) {
+  if (m.loads.size() > size_t(TOPX_MAX_LOAD_CASES))
+    throw std::runtime_error("the model has " + std::to_string(m.loads.size()) + " load cases; at most " +
+                             std::to_string(TOPX_MAX_LOAD_CASES) + " are supported");
 }
 
 topx_status need_model(topx_ctx* c) {
@@ -98,7 +108,7 @@ void fill_iter(topx_iter* out, const topx::IterRecord& r) {
   out->sharp = r.sharp;
   out->cons = r.cons;
   out->change = r.change;
-  for (size_t i = 0; i < r.its.size() && i < 8; ++i) out->its[i] = r.its[i];
+  for (size_t i = 0; i < r.its.size() && i < size_t(TOPX_MAX_LOAD_CASES); ++i) out->its[i] = r.its[i];
   out->filter_its = r.filter_its;
   out->t_assemble = r.t_assemble;
   out->t_cg = r.t_cg;
@@ -207,6 +217,7 @@ topx_status topx_load_voxels(topx_ctx* ctx, const uint8_t* vox, int nely, int ne
     m->apply_boundary_condition();
     m->setup();
     m->set_passive_elements();
+    check_load_cases(*m);
     ctx->model = std::move(m);
     ctx->vox.assign(vox, vox + size_t(nely) * nelx * nelz);
     ctx->vny = nely;
@@ -228,6 +239,7 @@ topx_status topx_load_topvoxel(topx_ctx* ctx, const char* path) {
     m->apply_boundary_condition();
     m->setup();
     m->set_passive_elements();
+    check_load_cases(*m);
     ctx->model = std::move(m);
     ctx->topvoxel = path;
     ctx->vox.clear();
@@ -267,6 +279,7 @@ topx_status topx_set_bc(topx_ctx* ctx, const double* fixing, int64_t nfix, const
     m->apply_boundary_condition();
     m->setup();
     m->set_passive_elements();
+    check_load_cases(*m);
     ctx->engine.reset();
     ctx->begun = false;
     ctx->model = std::move(m);
@@ -421,6 +434,16 @@ topx_status topx_ku_noalloc(topx_ctx* ctx, const double* u_dev, double* y_dev, s
                                      "context's GPU");
     double* s = topx::noalloc_scratch(ctx->params.device);
     eng.apply_K_device(u_dev, y_dev, s, s + grid);
+    return TOPX_OK;
+  });
+}
+
+topx_status topx_selftest_wait(topx_ctx* ctx, int which) {
+  return guarded(ctx, [&]() -> topx_status {
+    topx_status s = need_engine(ctx);
+    if (s != TOPX_OK) return s;
+    DeviceScope scope(ctx->params.device);
+    ctx->engine->selftest_wait(which);
     return TOPX_OK;
   });
 }

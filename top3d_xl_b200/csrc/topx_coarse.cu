@@ -654,6 +654,7 @@ constexpr int COOP_WARPS = COOP_THREADS / 32;
 constexpr unsigned kCoopSpinLimit = 1u << 20;
 constexpr unsigned kFlowSpinLimit = 1u << 20;
 constexpr unsigned long long kAbsent = 0x7FF4DEADBEEF0001ull;
+static_assert(kCoopErrBarrier != 0 && kCoopErrVector != 0 && kCoopErrBarrier != kCoopErrVector, "error codes");
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
@@ -691,7 +692,7 @@ __device__ bool coop_barrier(CoopBarrier* bar, unsigned& epoch) {
       unsigned it = 0;
       while (ld_acquire_gpu(&bar->count) < target) {
         if (++it > kCoopSpinLimit || ld_volatile_int(&bar->err)) {
-          atomicExch(&bar->err, 1);
+          atomicCAS(&bar->err, 0, kCoopErrBarrier);
           ok = 0;
           break;
         }
@@ -731,7 +732,7 @@ __device__ bool coop_wait_vector(TS* su, const double* g0, const double* g1, int
     if (__syncthreads_and(ok)) return true;
     const int bad = threadIdx.x == 0 && (it >= kFlowSpinLimit || ld_volatile_int(&bar->err));
     if (__syncthreads_or(bad)) {
-      if (threadIdx.x == 0) atomicExch(&bar->err, 1);
+      if (threadIdx.x == 0) atomicCAS(&bar->err, 0, kCoopErrVector);
       return false;
     }
     __nanosleep(64);
@@ -744,7 +745,7 @@ __device__ double coop_wait_value(const double* p, CoopBarrier* bar) {
     const double v = ld_relaxed_f64(p);
     if (coop_has(v)) return v;
     if (it >= kFlowSpinLimit || ld_volatile_int(&bar->err)) {
-      atomicExch(&bar->err, 1);
+      atomicCAS(&bar->err, 0, kCoopErrVector);
       return 0.0;
     }
     __nanosleep(64);
@@ -1076,6 +1077,36 @@ template void launch_slab_solve_coop<double, double>(cudaStream_t, int, Grid, Sl
 template void launch_slab_solve_coop<float, float>(cudaStream_t, int, Grid, SlabInfo, const float*, const float*,
                                                    const float*, const float*, double*, double*, double*, double*,
                                                    float*, const PcgScalars*, CoopBarrier*);
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded waits above: each case runs one wait primitive against a word that
+// nothing writes, so the wait must give up after its poll limit, set the error word and return.
+//  0: grid barrier of a two-CTA grid whose second CTA leaves without arriving;
+//  1: coop_wait_value on an entry left absent;
+//  2: coop_wait_vector on 64 entries left absent.
+// `absent` holds at least 64 doubles.  The launch ends within the poll limits (about a second).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(COOP_THREADS) k_coop_wait_selftest(int which, CoopBarrier* bar, double* absent) {
+  __shared__ double su[64];
+  for (int j = threadIdx.x; j < 64; j += COOP_THREADS)
+    reinterpret_cast<unsigned long long*>(absent)[j] = kAbsent;  // this CTA's own stores: seen below
+  __syncthreads();
+  if (which == 0) {
+    if (blockIdx.x != 0) return;  // never arrives
+    unsigned epoch = 0;
+    coop_barrier(bar, epoch);
+  } else if (which == 1) {
+    if (threadIdx.x == 0) absent[64] = coop_wait_value(absent, bar);
+  } else {
+    coop_wait_vector<double>(su, absent, absent, 64, 64, bar);
+  }
+}
+
+void launch_coop_wait_selftest(cudaStream_t st, int which, CoopBarrier* bar, double* absent) {
+  const unsigned grid = which == 0 ? 2u : 1u;
+  (k_coop_wait_selftest<<<grid, COOP_THREADS, 0, st>>>(which, bar, absent), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
 
 template void launch_diag_coarse<double>(cudaStream_t, Grid, const double*, const uint8_t*, double*);
 template void launch_diag_coarse<float>(cudaStream_t, Grid, const double*, const uint8_t*, float*);

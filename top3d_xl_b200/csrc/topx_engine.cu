@@ -284,6 +284,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     ev.push_back(e);
   }
   for (int i = 0; i < 2; ++i) TOPX_CUDA_OK(cudaEventCreate(&tev[i]));
+  TOPX_CUDA_OK(cudaEventCreateWithFlags(&ev_legacy, cudaEventDisableTiming));
   for (int i = 0; i < 16; ++i) {
     cudaEvent_t e;
     TOPX_CUDA_OK(cudaEventCreate(&e));
@@ -312,6 +313,7 @@ Engine::~Engine() {
   for (auto e : pev) cudaEventDestroy(e);
   for (auto e : tev)
     if (e) cudaEventDestroy(e);
+  if (ev_legacy) cudaEventDestroy(ev_legacy);
   if (h_sc) cudaFreeHost(h_sc);
   if (h_bar) cudaFreeHost(h_bar);
   if (h_gferr) cudaFreeHost(h_gferr);
@@ -368,14 +370,38 @@ void Engine::check_coop_barrier() {
 // cleared (so the engine stays usable) and reported.
 void Engine::check_device_waits() const {
   if (coopCtas && h_bar->err) {
+    const int code = h_bar->err;
+    h_bar->err = 0;
     TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
-    throw std::runtime_error("coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)");
+    throw DeviceWaitError(code == kCoopErrBarrier
+                              ? "coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)"
+                              : "coarse solve: a wait for an entry of a solve vector gave up");
   }
   if (gf.ctrl && *h_gferr) {
     *h_gferr = 0;
     TOPX_CUDA_OK(cudaMemset(gf.ctrl, 0, sizeof(int)));
-    throw std::runtime_error("coarse factorisation: a dependency wait of the Gauss-Jordan inverse gave up");
+    throw DeviceWaitError("coarse factorisation: a dependency wait of the Gauss-Jordan inverse gave up");
   }
+}
+
+// Drives one bounded device wait to its poll limit against a word that nothing writes (0: the
+// coarse solve's grid barrier, 1: its wait for one solve-vector entry, 2: its wait for a vector
+// of entries, 3: the Gauss-Jordan inverse's dependency wait).  The wait gives up within about a
+// second and the check below throws DeviceWaitError after clearing the error word.
+void Engine::selftest_wait(int which) {
+  if (which < 0 || which > 3) throw std::invalid_argument("selftest_wait: which must be 0, 1, 2 or 3");
+  if (which <= 2 && !coopCtas)
+    throw std::invalid_argument("selftest_wait: this context runs the coarse solve without a cooperative launch");
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+  DevBuf<double> words;
+  words.alloc(80);
+  if (which <= 2) {
+    TOPX_CUDA_OK(cudaMemsetAsync(coopBar.p, 0, sizeof(CoopBarrier), st));
+    launch_coop_wait_selftest(st, which, coopBar.p, words.p);
+  } else {
+    launch_gf_wait_selftest(st, gf.ctrl, reinterpret_cast<unsigned*>(words.p));
+  }
+  check_coop_barrier();
 }
 
 // ---------------------------------------------------------------------------

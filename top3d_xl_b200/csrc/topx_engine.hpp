@@ -134,6 +134,8 @@ class Engine {
   // y = K u on device vectors (compact DOF order) with caller-provided grid scratch; topx_noalloc.cu
   void apply_K_device(const double* d_u, double* d_y, double* grid_u, double* grid_y);
   void apply_vcycle(const double* h_r, double* h_z);
+  // runs one bounded device wait into its poll limit (test of the give-up path)
+  void selftest_wait(int which);
   void get_diag(int level, double* h_d) const;
 
   // ---- optimisation drivers ------------------------------------------------
@@ -261,6 +263,7 @@ class Engine {
  public:
   bool use_graphs = true;
   cudaEvent_t tev[2] = {nullptr, nullptr};
+  cudaEvent_t ev_legacy = nullptr;  // orders device-pointer calls after the legacy default stream
 };
 
 // Fixed device scratch of the allocation-free operator call (topx_noalloc.cu): its size in

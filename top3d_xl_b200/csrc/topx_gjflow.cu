@@ -492,6 +492,18 @@ int gj_flow_ctas(bool whole_gpu, int m) {
   return std::max(2, std::min(nsm / 8, nt));
 }
 
+// One thread waits, through the inverse's own wait primitive, for a version word that nothing
+// writes: it gives up after GF_SPIN_LIMIT polls and sets the error word.
+__global__ void k_gf_wait_selftest(unsigned* ctrl, const unsigned* word) {
+  if (threadIdx.x == 0) gf_wait(word, 1u, nullptr, 0, nullptr, 0, reinterpret_cast<int*>(ctrl + GF_ERR));
+}
+
+void launch_gf_wait_selftest(cudaStream_t st, unsigned* ctrl, unsigned* word) {
+  TOPX_CUDA_OK(cudaMemsetAsync(word, 0, sizeof(unsigned), st));
+  (k_gf_wait_selftest<<<1, 32, 0, st>>>(ctrl, word), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
 void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,
                     unsigned ntasks, double* scratch, unsigned* ctrl, int nctas) {
   // the error word (ctrl[0]) is left alone: the host reads and clears it after the factorisation

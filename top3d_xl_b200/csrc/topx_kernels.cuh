@@ -16,6 +16,11 @@ struct CudaError : std::runtime_error {
                            " (" + expr + ")"),
         code(e) {}
 };
+// A bounded device wait gave up (its poll limit ran out); the engine has cleared the error word
+// and stays usable.
+struct DeviceWaitError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 // Dense padded grid of one multigrid level: ny, nx, nz elements; node fields
 // are SoA with plane stride `stride` (>= (ny+1)(nx+1)(nz+1)).
@@ -146,9 +151,17 @@ void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, cons
 struct CoopBarrier {
   unsigned count;
   unsigned gen;
-  int err;
+  int err;  // 0, or the kind of wait that gave up first (kCoopErrBarrier, kCoopErrVector)
   int pad;
 };
+constexpr int kCoopErrBarrier = 1;  // a grid barrier wait gave up
+constexpr int kCoopErrVector = 2;   // a wait for an entry of a solve vector gave up
+// Self-test of the coarse solve's bounded waits (which: 0 grid barrier, 1 single entry, 2 vector
+// of entries) against words that nothing writes; `absent` holds 65 doubles of scratch.
+void launch_coop_wait_selftest(cudaStream_t st, int which, CoopBarrier* bar, double* absent);
+// Self-test of the Gauss-Jordan inverse's bounded dependency wait: waits for *word >= 1 where
+// nothing writes `word` (zeroed here); gives up and sets ctrl[0].
+void launch_gf_wait_selftest(cudaStream_t st, unsigned* ctrl, unsigned* word);
 // CTAs of launch_slab_solve_coop on the current device (one per SM), or 0 when cooperative
 // launch is unavailable; sets the kernels' shared-memory limit (call outside stream capture).
 int slab_solve_coop_ctas(int m);

@@ -55,6 +55,12 @@ double* noalloc_scratch(int device) {
 // order, like apply_K); grid_u and grid_y are caller-provided scratch of 3 * stride doubles.
 void Engine::apply_K_device(const double* d_u, double* d_y, double* grid_u, double* grid_y) {
   const Grid& g = G[0];
+  // The engine stream is non-blocking, so nothing orders it after work the caller still has
+  // queued on the legacy default stream (a gpuArray kernel, an asynchronous copy into u):
+  // wait for that work first.  Work on the caller's own non-blocking or per-thread streams is
+  // not seen here; the caller synchronises it before the call.
+  TOPX_CUDA_OK(cudaEventRecord(ev_legacy, cudaStreamLegacy));
+  TOPX_CUDA_OK(cudaStreamWaitEvent(st, ev_legacy, 0));
   // the scratch keeps the previous call's contents: grid nodes outside the domain must read 0
   TOPX_CUDA_OK(cudaMemsetAsync(grid_u, 0, sizeof(double) * size_t(g.stride) * 3, st));
   launch_compact_to_grid_nodes<double>(st, d_u, grid_u, g, nodMapBack0.p, Nn);

@@ -132,7 +132,7 @@ void topx_server::run(Job& j) {
     if (st != TOPX_OK) break;
     j.hist.push_back(it);
     j.res.c_last = it.c;
-    for (int lc = 0; lc < info.numLoadCases && lc < 8; ++lc) j.res.pcg_its += it.its[lc];
+    for (int lc = 0; lc < info.numLoadCases && lc < TOPX_MAX_LOAD_CASES; ++lc) j.res.pcg_its += it.its[lc];
     ++loops;
   }
   j.res.loops = loops;

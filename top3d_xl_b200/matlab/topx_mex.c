@@ -5,10 +5,14 @@
  *   mex -I../../include topx_mex.c -L.. -ltopx            (MATLAB)
  *   mkoctfile --mex -I../../include topx_mex.c -L.. -ltopx (Octave)
  *
- *   [hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision)
+ *   [hist, xPhys, grid] = topx_mex(inputModel, consType, V0, nLoop, rMin, rHat, precision, ...
+ *                                  typeVcycle, specifyPassiveRegions)
+ *   topx_mex('write_design', vol, prefix)
  *
  * inputModel: logical (nely, nelx, nelz) array (built-in cuboid BCs) or a .TopVoxel path;
- * consType 'GLOBAL' | 'LOCAL'; precision 'fp64' | 'mixed'.
+ * consType 'GLOBAL' | 'LOCAL'; rHat may be [] for GLOBAL; precision 'fp64' (default) | 'mixed';
+ * typeVcycle 'Adapted' (default) | 'Standard'; specifyPassiveRegions a 3-vector of layer counts
+ * (boundary, near loads, near fixations), default [0 0 0].  Arguments 6 to 9 are optional.
  * hist: struct with fields cSolid, c, vol, sharp, cons, change, its, tAssemble, tCG, tOpti, tFilter, tTotal.
  * xPhys: densityLayout_ (numElements x 1, eleMapBack order).
  * grid: struct with resX, resY, resZ, eleMapBack (for the padded volume of IO_ExportDesignInVolume_nii).
