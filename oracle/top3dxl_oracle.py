@@ -1128,9 +1128,28 @@ def _solve_all(solver: Solver, model: Model, U, its_list=None):
     return U
 
 
+def oc_update(x, dc, dv, fval, passive, move=0.2):
+    """The OC bisection of TOP3D_XL_TO (TX:145-156): the volume multiplier is bisected from
+    (0, 1e9) until (l2 - l1)/(l1 + l2) <= 1e-6; gt is fval plus the SUM of the density change
+    (as written in the reference).  Returns the new densities and the last midpoint."""
+    l1_, l2_ = 0.0, 1e9
+    while (l2_ - l1_) / (l1_ + l2_) > 1e-6:
+        lmid = 0.5 * (l2_ + l1_)
+        xnew = np.maximum(0, np.maximum(x - move, np.minimum(1, np.minimum(x + move, x * np.sqrt(-dc / dv / lmid)))))
+        xnew[passive] = 1.0
+        gt = fval + np.sum(dv * (xnew - x))
+        if gt > 0:
+            l1_ = lmid
+        else:
+            l2_ = lmid
+    return xnew, lmid
+
+
 def run_global(input_model, V0, nLoop, rMin, S: Settings | None = None, model: Model | None = None,
-               max_loops=None, keep_U=False):
-    """TOP3D_XL_TO (TX:40-223) without file/graphics output.  Returns a history dict."""
+               max_loops=None, keep_U=False, hook=None):
+    """TOP3D_XL_TO (TX:40-223) without file/graphics output.  Returns a history dict.
+    `hook(loop)`, if given, is called once cSolid is known (loop 0) and after each iteration;
+    a true return value ends the loop there (used to time a bounded number of iterations)."""
     model = model or build_model(input_model, S)
     S = model.S
     l1 = model.levels[0]
@@ -1149,6 +1168,8 @@ def run_global(input_model, V0, nLoop, rMin, S: Settings | None = None, model: M
     hist = dict(cSolid=cSolid, c=[], vol=[], sharp=[], cons=[], change=[], its=[], filter_its=[])
     E0, Emin, p = S.modulus, S.modulusMin, S.SIMPpenalty
     stop = nLoop if max_loops is None else min(nLoop, max_loops)
+    if hook is not None and hook(0):
+        stop = 0
     while loop < stop and change > 0.0001 and sharpness > 0.01:
         loop += 1
         E = Emin + xPhys ** p * (E0 - Emin)
@@ -1164,16 +1185,7 @@ def run_global(input_model, V0, nLoop, rMin, S: Settings | None = None, model: M
         dc = flt(x * dc) / np.maximum(1e-3, x)
         hist["filter_its"].append(flt.last_its)
         fval = np.mean(xPhys) - V0
-        l1_, l2_, move = 0.0, 1e9, 0.2
-        while (l2_ - l1_) / (l1_ + l2_) > 1e-6:
-            lmid = 0.5 * (l2_ + l1_)
-            xnew = np.maximum(0, np.maximum(x - move, np.minimum(1, np.minimum(x + move, x * np.sqrt(-dc / dv / lmid)))))
-            xnew[passive] = 1.0
-            gt = fval + np.sum(dv * (xnew - x))
-            if gt > 0:
-                l1_ = lmid
-            else:
-                l2_ = lmid
+        xnew, lmid = oc_update(x, dc, dv, fval, passive)
         change = float(np.max(np.abs(xnew - x)))
         x = xnew
         xPhys = xnew.copy()
@@ -1185,6 +1197,8 @@ def run_global(input_model, V0, nLoop, rMin, S: Settings | None = None, model: M
         hist["sharp"].append(sharpness)
         hist["change"].append(change)
         hist.setdefault("lmid", []).append(lmid)
+        if hook is not None and hook(loop):
+            break
     hist["xPhys"] = xPhys
     hist["loops"] = loop
     if keep_U:
@@ -1193,8 +1207,9 @@ def run_global(input_model, V0, nLoop, rMin, S: Settings | None = None, model: M
 
 
 def run_local(input_model, Ve0, nLoop, rMin, rHat, S: Settings | None = None, model: Model | None = None,
-              max_loops=None):
-    """TOP3D_XL_PIO (TX:225-440) without file/graphics output.  Returns a history dict."""
+              max_loops=None, hook=None):
+    """TOP3D_XL_PIO (TX:225-440) without file/graphics output.  Returns a history dict.
+    `hook` as in run_global."""
     model = model or build_model(input_model, S)
     S = model.S
     l1 = model.levels[0]
@@ -1219,6 +1234,8 @@ def run_local(input_model, Ve0, nLoop, rMin, rHat, S: Settings | None = None, mo
     hist = dict(cSolid=cSolid, c=[], vol=[], sharp=[], cons=[], change=[], its=[], beta=[])
     E0, Emin, p = S.modulus, S.modulusMin, S.SIMPpenalty
     stop = nLoop if max_loops is None else min(nLoop, max_loops)
+    if hook is not None and hook(0):
+        stop = 0
     xold1 = xold2 = low = upp = None
     while loop < stop and change > 0.0001 and sharpness > 0.01:
         loopbeta += 1
@@ -1269,6 +1286,8 @@ def run_local(input_model, Ve0, nLoop, rMin, rHat, S: Settings | None = None, mo
         hist["sharp"].append(sharpness)
         hist["change"].append(change)
         hist["beta"].append(betaPIO)
+        if hook is not None and hook(loop):
+            break
     hist["xPhys"] = xPhys
     hist["loops"] = loop
     return hist

@@ -43,12 +43,16 @@ def test_single_process_is_the_identity():
 
 
 def test_reference_arm_prints_one_json_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "cuboid25", "--steps", "1",
+    # whole OC iterations of the oracle are timed; `steps` is the number actually timed
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "cuboid25", "--steps", "2",
                         "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "OC iterations/s"
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["steps"] == 2 and line["steps_requested"] == 2
+    assert line["ms_per_step"] == pytest.approx(1000.0 * line["steps"] / line["value"] / line["steps"])
+    assert "whole OC iterations" in line["cpu_baseline"]["sample"]
 
 
 def test_clock_median_uses_samples_under_load():

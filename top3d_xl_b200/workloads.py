@@ -101,6 +101,29 @@ def irregular_domain(seed=8, box=(192, 384, 192), n_ellipsoids=12, n_cylinders=6
     return vox, sorted(fixed), loads
 
 
+def two_load_case_model(ny=10, nx=20, nz=10):
+    """A cuboid with two load cases and passive elements, as a ``.TopVoxel`` file gives them.
+
+    Fixed: every node of the bottom face (z = 0), all three directions.  Load case 1: the four
+    nodes of the top face's centre with force (0, 0, -1/4) each.  Load case 2: the nodes of the
+    top face's edge at x = nx, force (0.5/(ny+1), 0, 0) each.  Passive: a 2 x 2 x 2 block of
+    elements under the centre of the top face (compact ids of the full cuboid, 1-based).  The
+    bottom-face node ids are all smaller than the boundary-node count, so passive layers near
+    the fixations (specifyPassiveRegions_(3), TOP3D_XL.m:1563-1574) index that list as the
+    reference does.  Returns vox, fixed, [case1, case2], passive.
+    """
+    vox = np.ones((ny, nx, nz), bool)
+    nny, nnx = ny + 1, nx + 1
+    node = lambda y, x, z: 1 + y + nny * (x + nnx * z)  # noqa: E731
+    fixed = [node(y, x, 0) for x in range(nnx) for y in range(nny)]
+    cy, cx = ny // 2, nx // 2
+    case1 = [(node(cy + dy, cx + dx, nz), 0.0, 0.0, -0.25) for dx in (0, 1) for dy in (0, 1)]
+    case2 = [(node(y, nx, nz), 0.5 / nny, 0.0, 0.0) for y in range(nny)]
+    elem = lambda y, x, z: 1 + y + ny * (x + nx * z)  # noqa: E731
+    passive = sorted(elem(cy - 1 + dy, cx - 1 + dx, nz - 2 + dz) for dx in (0, 1) for dy in (0, 1) for dz in (0, 1))
+    return vox, fixed, [case1, case2], passive
+
+
 def write_topvoxel(path, vox, fixed, loads, passive=(), additional_loads=()):
     """Write a ``.TopVoxel`` v1.0 file (TOP3D_XL.m:448-497): fixed nodes get all three DOFs."""
     ny, nx, nz = vox.shape
