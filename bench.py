@@ -9,8 +9,8 @@ factorisation, multigrid PCG, compliance, PDE sensitivity filter, OC update),
 with all state resident in HBM.
 
 `value` is the FP64 engine (the reference's own precision).  The mixed-precision
-engine (FP64 Krylov iteration and operator, FP32 multigrid preconditioner and
-filter) is measured beside it, with its per-iteration relative compliance
+engine (FP64 Krylov iteration, operator and filter, FP32 multigrid preconditioner)
+is measured beside it, with its per-iteration relative compliance
 error against FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
@@ -386,13 +386,15 @@ def main(argv=None):
     ap.add_argument("--serve", action="store_true",
                     help="run only the served stream (continuous batching) and print its line")
     ap.add_argument("--serve-jobs", type=int, default=256)
-    ap.add_argument("--serve-precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--serve-precision", choices=["mixed", "mixed32", "fp64"], default="mixed")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-seq-jobs", type=int, default=32,
                     help="jobs of the stream also run one at a time in FP64 for the baseline")
     ap.add_argument("--ref-budget-s", type=float, default=240.0,
                     help="reference arm: time spent on timed whole OC iterations (at least one runs)")
-    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--mixed", choices=["mixed", "mixed32"], default="mixed",
+                    help="precision of the mixed arm: FP32 preconditioner (mixed), also FP32 filter (mixed32)")
+    ap.add_argument("--only", choices=["mixed", "mixed32", "fp64"], default=None,
                     help="run one precision arm only (profiling); prints its timing and exits")
     a = ap.parse_args(argv)
     wl = WORKLOADS[a.workload]
@@ -474,7 +476,7 @@ def main(argv=None):
         if dist:
             dist.destroy_process_group()
         return 0
-    mixed = run_native(wl, "mixed", a.steps, a.warmup, device)
+    mixed = run_native(wl, a.mixed, a.steps, a.warmup, device)
     value = replicas_value(ws, a.steps, ms_max)
     cm = np.array([h["c"] for h in mixed["hist"]])
     cd = np.array([h["c"] for h in fp64["hist"]])
@@ -507,8 +509,9 @@ def main(argv=None):
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (built-in cuboid BCs)", "config": cfg,
             "mixed": {"value": a.steps / (mixed["ms"] / 1000.0), "ms_per_step": mixed["ms"] / a.steps,
-                      "dtype": "f64 Krylov iteration, operator, dots, compliance, OC; f32 multigrid "
-                               "preconditioner and filter",
+                      "dtype": "f64 Krylov iteration, operator, dots, compliance, OC%s; f32 multigrid "
+                               "preconditioner%s" % ((", filter", "") if a.mixed == "mixed" else ("", " and filter")),
+                      "precision": a.mixed,
                       "pcg_its_per_step": float(np.mean(its_mixed)),
                       "max_rel_compliance_err_vs_fp64": relerr, "iterations_compared": n,
                       "rel_compliance_err_per_iteration": [float("%.3g" % e) for e in relerrs]},

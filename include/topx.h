@@ -46,7 +46,11 @@ enum {
 };
 
 enum { TOPX_GLOBAL = 0, TOPX_LOCAL = 1 };        /* consType (TX:12-18) */
-enum { TOPX_FP64 = 0, TOPX_MIXED = 1 };          /* arithmetic of the solver */
+/* arithmetic of the solver: TOPX_FP64 everything in FP64 (the reference's precision);
+   TOPX_MIXED the multigrid preconditioner in FP32 inside the FP64 Krylov iteration (operator,
+   residual, dots, compliance, optimiser and PDE filter in FP64); TOPX_MIXED_F32_FILTER the PDE
+   filter's CG in FP32 as well */
+enum { TOPX_FP64 = 0, TOPX_MIXED = 1, TOPX_MIXED_F32_FILTER = 2 };
 enum { TOPX_VCYCLE_ADAPTED = 0, TOPX_VCYCLE_STANDARD = 1 };  /* typeVcycle_ (TX:34, 747-781) */
 
 typedef struct topx_ctx topx_ctx;
@@ -62,7 +66,7 @@ typedef struct topx_params {
   int maxIT;               /* PCG iteration cap, 800 */
   double weightFactorJacobi; /* 0.6 */
   int64_t coarsestResolutionControl; /* 50000 */
-  int precision;           /* TOPX_FP64 or TOPX_MIXED */
+  int precision;           /* TOPX_FP64, TOPX_MIXED or TOPX_MIXED_F32_FILTER */
   int device;              /* CUDA device ordinal */
   int coarse_coop;         /* 1: coarsest solve as one cooperative launch when available (default);
                               0: one launch per chain step (for engines sharing the GPU) */
@@ -249,7 +253,7 @@ typedef struct topx_server topx_server;
 typedef struct topx_server_params {
   int slots;                /* jobs on the device at once (worker threads), default 6 */
   double hbm_budget_bytes;  /* device memory admitted jobs may hold; <= 0: 85% of free memory */
-  int precision;            /* TOPX_FP64 or TOPX_MIXED */
+  int precision;            /* TOPX_FP64, TOPX_MIXED or TOPX_MIXED_F32_FILTER */
   int device;               /* CUDA device ordinal */
 } topx_server_params;
 typedef struct topx_job {

@@ -181,7 +181,7 @@ topx_status topx_create(topx_ctx** ctx, const topx_params* p) {
     const topx_params& q = c->params;
     const bool vc_ok = q.typeVcycle == TOPX_VCYCLE_ADAPTED ||
                        (q.typeVcycle == TOPX_VCYCLE_STANDARD && q.precision == TOPX_FP64);
-    if ((q.precision != TOPX_FP64 && q.precision != TOPX_MIXED) || !vc_ok) {
+    if ((q.precision != TOPX_FP64 && q.precision != TOPX_MIXED && q.precision != TOPX_MIXED_F32_FILTER) || !vc_ok) {
       delete c;
       return TOPX_ERR_ARG;
     }

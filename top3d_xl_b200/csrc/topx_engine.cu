@@ -204,7 +204,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     slabSinv.alloc(mm * si.ns);
     slabL.alloc(mm * nsm1);
     slabLT.alloc(mm * nsm1);
-    if (prec == PREC_MIXED) {
+    if (pre32()) {
       slabSinv32.alloc(mm * si.ns);
       slabL32.alloc(mm * nsm1);
       slabLT32.alloc(mm * nsm1);
@@ -238,9 +238,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     for (DevBuf<double>* b : {&kw.r, &kw.z, &kw.p, &kw.q, &kw.p2}) b->alloc(S1);
     E64.alloc(size_t(G[0].nelems()));
     cfix64.upload(cf.data(), cf.size());
-    if (prec == PREC_FP64) {
+    if (!pre32()) {
       alloc_vwork(v64);
-      alloc_fwork(f64);
       if (M.S.typeVcycle == 1) {
         vq.resize(nl);
         for (int l = 1; l < nl - 1; ++l) vq[l].alloc(size_t(G[l].stride) * 3);
@@ -248,8 +247,11 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     } else {
       if (M.S.typeVcycle == 1) throw std::invalid_argument("the 'Standard' V-cycle runs in FP64 precision");
       alloc_vwork(v32);
-      alloc_fwork(f32);
     }
+    if (flt32())
+      alloc_fwork(f32);
+    else
+      alloc_fwork(f64);
   }
   // ---- reductions and scalars ---------------------------------------------------
   red1.alloc(size_t(kMaxRedBlocks) * kMaxRedSlots);
@@ -450,7 +452,7 @@ void Engine::assemble() {
 
 void Engine::assemble_launches() {
   sec_begin(SEC_DIAG);
-  if (prec == PREC_FP64)
+  if (!pre32())
     launch_diag_l1<double>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v64.d1.p);
   else
     launch_diag_l1<double, float>(st, G[0], E64.p, fixbits.p, cfix64.p, present[0].p, v32.d1.p);
@@ -464,7 +466,7 @@ void Engine::assemble_launches() {
   sec_end();
   sec_begin(SEC_DIAG);
   for (int l = 1; l < nl - 1; ++l) {
-    if (prec == PREC_FP64)
+    if (!pre32())
       launch_diag_coarse<double>(st, G[l], Ks[l].p, present[l].p, v64.dl[l].p);
     else
       launch_diag_coarse<float>(st, G[l], Ks[l].p, present[l].p, v32.dl[l].p);
@@ -480,7 +482,7 @@ void Engine::factor_coarsest() {
   sec_begin(SEC_INVERSE);
   launch_slab_factor(st, gf, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p);
   sec_end();
-  if (prec == PREC_MIXED) {
+  if (pre32()) {
     launch_convert<double, float>(st, slabSinv.p, slabSinv32.p, int64_t(slabSinv.n));
     launch_convert<double, float>(st, slabL.p, slabL32.p, int64_t(slabL.n));
     launch_convert<double, float>(st, slabLT.p, slabLT32.p, int64_t(slabLT.n));
@@ -569,9 +571,9 @@ void Engine::vcycle_standard(bool init, PcgScalars* sc) {
 }
 
 void Engine::vcycle(bool init, PcgScalars* sc) {
-  if (prec == PREC_FP64 && M.S.typeVcycle == 1)
+  if (!pre32() && M.S.typeVcycle == 1)
     vcycle_standard(init, sc);
-  else if (prec == PREC_FP64)
+  else if (!pre32())
     vcycle_t<double>(v64, init, sc);
   else
     vcycle_t<float>(v32, init, sc);
@@ -660,7 +662,7 @@ void Engine::setup_filter(int slot, double rmin) {
   filterKe64[slot] = filter_ke<double>(KF.data());
   filterKe32[slot] = filter_ke<float>(KF.data());
   filterR[slot] = rmin;
-  if (prec == PREC_FP64)
+  if (!flt32())
     launch_filter_diag<double>(st, G[0], solid1.p, filterKe64[slot], f64.fdp[slot].p);
   else
     launch_filter_diag<float>(st, G[0], solid1.p, filterKe64[slot], f32.fdp[slot].p);
@@ -711,7 +713,7 @@ int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) 
 }
 
 int Engine::filter(int slot, const double* d_src, double* d_out) {
-  if (prec == PREC_FP64) return filter_t<double>(f64, slot, d_src, d_out);
+  if (!flt32()) return filter_t<double>(f64, slot, d_src, d_out);
   return filter_t<float>(f32, slot, d_src, d_out);
 }
 
@@ -864,7 +866,7 @@ void Engine::get_diag(int level, double* h_d) const {
   const Level& L = M.levels[level - 1];
   const Grid& g = G[level - 1];
   std::vector<double> dense(size_t(g.stride) * 3);
-  if (prec == PREC_FP64) {
+  if (!pre32()) {
     const double* src = level == 1 ? v64.d1.p : v64.dl[level - 1].p;
     TOPX_CUDA_OK(cudaStreamSynchronize(st));
     TOPX_CUDA_OK(cudaMemcpy(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost));

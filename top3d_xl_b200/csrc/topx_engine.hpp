@@ -72,7 +72,9 @@ struct DevBuf {
   size_t bytes() const { return sizeof(T) * n; }
 };
 
-enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
+// PREC_FP64: everything in FP64.  PREC_MIXED: FP32 multigrid preconditioner inside the FP64 Krylov
+// iteration, FP64 PDE filter.  PREC_MIXED_F32_FILTER: the PDE filter's CG in FP32 as well.
+enum Precision { PREC_FP64 = 0, PREC_MIXED = 1, PREC_MIXED_F32_FILTER = 2 };
 
 struct IterRecord {
   int loop = 0;
@@ -164,6 +166,8 @@ class Engine {
 
   Model& M;
   int prec;
+  bool pre32() const { return prec != PREC_FP64; }              // FP32 multigrid preconditioner
+  bool flt32() const { return prec == PREC_MIXED_F32_FILTER; }  // FP32 PDE-filter CG
   cudaStream_t st = nullptr;
   GJFlow gf{};  // dataflow inverse of the coarse factorisation: plans, scratch, control words
   int nl = 0;

@@ -46,12 +46,12 @@ int64_t footprint_estimate(const topx_info& in, int precision) {
   int64_t d[3] = {in.resY[L] + 1, in.resX[L] + 1, in.resZ[L] + 1};
   std::sort(d, d + 3);
   const int64_t ns = d[2], m = 3 * d[0] * d[1];
-  const int64_t slab = (2 * ns + 2 * (ns - 1) + 2) * m * m * 8 + (precision == TOPX_MIXED ? 3 * ns * m * m * 4 : 0);
+  const int64_t slab = (2 * ns + 2 * (ns - 1) + 2) * m * m * 8 + (precision != TOPX_FP64 ? 3 * ns * m * m * 4 : 0);
   // the Gauss-Jordan inverse's ring scratch, control words and task plans (~nt^3 tasks each)
   const int64_t nt = topx::gf_tiles(int(m));
   const int64_t inverse = int64_t(topx::gf_scratch_doubles(int(m))) * 8 + int64_t(topx::gf_ctrl_words(int(m))) * 4 +
                           3 * nt * (nt * nt + 2 * nt + 1) * 4;
-  const int64_t per_node = precision == TOPX_MIXED ? 584 : 544, per_elem = 200;
+  const int64_t per_node = precision != TOPX_FP64 ? 584 : 544, per_elem = 200;
   return per_node * nodes + per_elem * elems + slab + inverse + (int64_t(48) << 20);
 }
 
@@ -196,7 +196,9 @@ topx_status topx_server_create(topx_server** out, const topx_server_params* p) {
   else
     topx_server_default_params(&s->params);
   if (s->params.slots < 1 || s->params.slots > 64) return TOPX_ERR_ARG;
-  if (s->params.precision != TOPX_FP64 && s->params.precision != TOPX_MIXED) return TOPX_ERR_ARG;
+  if (s->params.precision != TOPX_FP64 && s->params.precision != TOPX_MIXED &&
+      s->params.precision != TOPX_MIXED_F32_FILTER)
+    return TOPX_ERR_ARG;
   // worker threads wait on their streams a lot: yield the core instead of spinning on it
   // (takes effect only if this process has not touched the device yet)
   if (cudaSetDeviceFlags(cudaDeviceScheduleYield) != cudaSuccess) cudaGetLastError();

@@ -18,6 +18,10 @@ import numpy as np
 
 from . import _lib as L
 
+# topx_params.precision: "mixed" runs the multigrid preconditioner in FP32 inside the FP64 Krylov
+# iteration; "mixed32" also the PDE filter's CG in FP32
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed32": 2}
+
 
 class TopxError(RuntimeError):
     """A libtopx call returned an error status."""
@@ -38,9 +42,9 @@ class Context:
         self.lib = L.load()
         p = L.Params()
         self.lib.topx_default_params(C.byref(p))
-        if precision not in ("fp64", "mixed"):
-            raise ValueError("precision must be 'fp64' or 'mixed'")
-        p.precision = 0 if precision == "fp64" else 1
+        if precision not in PRECISIONS:
+            raise ValueError("precision must be one of %s" % ", ".join(PRECISIONS))
+        p.precision = PRECISIONS[precision]
         p.device = device
         for k, v in settings.items():
             if not hasattr(p, k):
@@ -367,7 +371,7 @@ class Server:
         p = L.ServerParams()
         self.lib.topx_server_default_params(C.byref(p))
         p.slots = int(slots)
-        p.precision = {"fp64": 0, "mixed": 1}[precision]
+        p.precision = PRECISIONS[precision]
         p.hbm_budget_bytes = float(hbm_budget_bytes)
         p.device = int(device)
         self._h = C.c_void_p()
