@@ -19,8 +19,8 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtopx.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CUDA_SOURCES = ["topx_fem.cu", "topx_coarse.cu", "topx_gjflow.cu", "topx_opt.cu", "topx_engine.cu", "topx_noalloc.cu"]
-CXX_SOURCES = ["topx_mesh.cpp", "topx_api.cpp", "topx_server.cpp", "topx_export.cpp"]
+CUDA_SOURCES = ["topx_fem.cu", "topx_coarse.cu", "topx_nd.cu", "topx_opt.cu", "topx_engine.cu", "topx_noalloc.cu"]
+CXX_SOURCES = ["topx_mesh.cpp", "topx_nd_plan.cpp", "topx_api.cpp", "topx_server.cpp", "topx_export.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

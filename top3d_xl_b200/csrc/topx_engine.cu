@@ -1,6 +1,5 @@
 // Device engine of the TOP3D_XL B200 path (see topx_engine.hpp).
 #include "topx_engine.hpp"
-#include "topx_gjflow.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -22,8 +21,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   // other host threads (and their synchronous set-up copies) never stall or break this one's
   // graph captures; every host-side copy below waits for this stream first
   TOPX_CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  prepare_coarse_kernels();
   prepare_fem_kernels();
+  prepare_nd_kernels();
   nl = M.numLevels;
   if (nl < 3 || int(M.levels.size()) != nl) throw std::runtime_error("model hierarchy not built");
   for (int l = 0; l < nl; ++l) {
@@ -177,60 +176,50 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   }
   Ks.resize(nl);
   for (int l = 1; l < nl; ++l) Ks[l].alloc(size_t(G[l].nelems()) * 576);
-  // ---- coarsest slab structure -------------------------------------------------
+  // ---- coarsest level: nested-dissection plan and factor storage -----------------
   {
     const Grid& g = G[nl - 1];
-    const int dims[3] = {g.nny(), g.nnx(), g.nnz()};
-    int ax = 0;
-    for (int a = 1; a < 3; ++a)
-      if (dims[a] > dims[ax]) ax = a;
-    si.axis = ax;
-    si.ns = dims[ax];
-    if (ax == 0) {
-      si.nu = dims[1];
-      si.nv = dims[2];
-    } else if (ax == 1) {
-      si.nu = dims[0];
-      si.nv = dims[2];
-    } else {
-      si.nu = dims[0];
-      si.nv = dims[1];
-    }
-    si.m = 3 * si.nu * si.nv;
-    if (si.m > 4096) throw std::runtime_error("coarsest level too large for the slab solver");
-    const size_t mm = size_t(si.m) * si.m;
-    const size_t nsm1 = size_t(std::max(1, si.ns - 1));
-    slabA.alloc(mm * si.ns);
-    slabSinv.alloc(mm * si.ns);
-    slabL.alloc(mm * nsm1);
-    slabLT.alloc(mm * nsm1);
-    if (pre32()) {
-      slabSinv32.alloc(mm * si.ns);
-      slabL32.alloc(mm * nsm1);
-      slabLT32.alloc(mm * nsm1);
-    }
-    slabBup.alloc(size_t(si.nu) * si.nv * 81 * nsm1);
-    for (int nset = 1; nset <= 2; ++nset) {
-      const std::vector<uint32_t> plan = gf_plan(si.m, nset);
-      gf_check_plan(plan, si.m, nset);
-      gfTasks[nset - 1].upload(plan.data(), plan.size());
-      gf.tasks[nset - 1] = gfTasks[nset - 1].p;
-      gf.ntasks[nset - 1] = unsigned(plan.size());
-    }
-    gfScr.alloc(gf_scratch_doubles(si.m), false);
-    gfCtrl.alloc(gf_ctrl_words(si.m));
-    gfY.alloc(2 * mm, false);
-    gf.scratch = gfScr.p;
-    gf.ctrl = gfCtrl.p;
-    gf.ytmp = gfY.p;
-    // an engine alone on the GPU fills it; engines sharing it leave room for their neighbours
-    gf.nctas = gj_flow_ctas(coarse_coop, si.m);
-    for (DevBuf<double>* b : {&slabBS, &slabW, &slabV, &slabXS}) b->alloc(size_t(si.m) * si.ns);
+    const Level& Lc = M.levels[nl - 1];
+    std::vector<uint8_t> pc(size_t(g.nnodes()), 0);
+    for (auto k : Lc.nodMapBack) pc[k - 1] = 1;
+    nd = nd_plan(g.nny(), g.nnx(), g.nnz(), g.stride, pc);
+    ndFronts.upload(nd.fronts.data(), nd.fronts.size());
+    ndTasks.upload(nd.tasks.data(), nd.tasks.size());
+    ndAsm.upload(nd.asmb.data(), nd.asmb.size());
+    ndPad.upload(nd.pad_diag.data(), nd.pad_diag.size());
+    ndMap.upload(nd.upd_map.data(), nd.upd_map.size());
+    ndSep.upload(nd.sep_dof.data(), nd.sep_dof.size());
+    ndUpd.upload(nd.upd_dof.data(), nd.upd_dof.size());
+    ndSrc0.upload(nd.src[0].data(), nd.src[0].size());
+    ndSrc1.upload(nd.src[1].data(), nd.src[1].size());
+    const size_t tile = size_t(ND_T) * ND_T;
+    ndPool.alloc(size_t(nd.ntiles) * tile, false);
+    ndScr.alloc(size_t(nd.nscr) * tile, false);
+    ndW.alloc(size_t(nd.npos));
+    ndPart.alloc(size_t(nd.nsolve_tasks) * ND_T, false);
+    ndCnt.alloc(size_t(nd.npos / ND_T));
+    if (pre32()) ndPool32.alloc(size_t(nd.ntiles) * tile, false);
+    ndd.fronts = ndFronts.p;
+    ndd.tasks = ndTasks.p;
+    ndd.asmb = ndAsm.p;
+    ndd.pad = ndPad.p;
+    ndd.upd_map = ndMap.p;
+    ndd.sep_dof = ndSep.p;
+    ndd.upd_dof = ndUpd.p;
+    ndd.src0 = ndSrc0.p;
+    ndd.src1 = ndSrc1.p;
+    ndd.pool = ndPool.p;
+    ndd.scr = ndScr.p;
+    ndd.wvec = ndW.p;
+    ndd.part = ndPart.p;
+    ndd.cnt = ndCnt.p;
     coopBar.alloc(1);
-    // the cooperative solve beats the chain of small launches at every slab size measured
-    // (m = 75 .. 1875); below m = 600 a grid of 64 CTAs polls faster than one of every SM
-    coopCtas = coarse_coop ? slab_solve_coop_ctas(si.m) : 0;
-    if (coopCtas && si.m < 600) coopCtas = std::min(coopCtas, 64);
+    // an engine alone on the GPU runs the solve as one persistent launch; engines sharing the
+    // GPU (the job server) launch it level by level, since a persistent launch needs all its CTAs
+    // resident at once
+    coopCtas = coarse_coop ? nd_solve_coop_ctas() : 0;
+    ndd.coop_ctas = coopCtas;
+    ndd.bar = coopBar.p;
   }
   // ---- workspaces ------------------------------------------------------------
   {
@@ -267,8 +256,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   dscal.alloc(16);
   TOPX_CUDA_OK(cudaMallocHost(&h_sc, sizeof(PcgScalars)));
   TOPX_CUDA_OK(cudaMallocHost(&h_bar, sizeof(CoopBarrier)));
-  TOPX_CUDA_OK(cudaMallocHost(&h_gferr, sizeof(int)));
-  *h_gferr = 0;
+  h_bar->err = 0;
   // ---- optimiser state -------------------------------------------------------
   for (DevBuf<double>* b : {&x, &xPhys, &dc, &ce, &tmpA, &tmpB, &xTilde, &xhat, &dfdx, &dxv, &volMax})
     b->alloc(size_t(Ne));
@@ -301,7 +289,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   std::ostringstream os;
   os << "levels=" << nl;
   for (int l = 0; l < nl; ++l) os << " L" << (l + 1) << "=" << G[l].nx << "x" << G[l].ny << "x" << G[l].nz;
-  os << " slab(axis=" << si.axis << ",ns=" << si.ns << ",m=" << si.m << ") flagged=" << nflag;
+  os << " nd(fronts=" << nd.fronts.size() << ",levels=" << nd.levels.size() << ",maxn1=" << nd.max_n1
+     << ",maxn2=" << nd.max_n2 << ",tilesMB=" << (double(nd.ntiles) * ND_T * ND_T * 8 / 1e6) << ") flagged=" << nflag;
   info_ = os.str();
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
 }
@@ -318,7 +307,6 @@ Engine::~Engine() {
   if (ev_legacy) cudaEventDestroy(ev_legacy);
   if (h_sc) cudaFreeHost(h_sc);
   if (h_bar) cudaFreeHost(h_bar);
-  if (h_gferr) cudaFreeHost(h_gferr);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -354,7 +342,6 @@ void Engine::alloc_fwork(FWork<TF>& f) {
 void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
   TOPX_CUDA_OK(cudaMemcpyAsync(h_sc, d, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
   if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
-  if (gf.ctrl) TOPX_CUDA_OK(cudaMemcpyAsync(h_gferr, gf.ctrl, sizeof(int), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   h = *h_sc;
   check_device_waits();
@@ -362,47 +349,31 @@ void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
 
 void Engine::check_coop_barrier() {
   if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
-  if (gf.ctrl) TOPX_CUDA_OK(cudaMemcpyAsync(h_gferr, gf.ctrl, sizeof(int), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   check_device_waits();
 }
 
-// The bounded waits of the device code set an error word instead of spinning on; the words
-// were copied into pinned memory before the caller's stream sync.  A word that is set is
-// cleared (so the engine stays usable) and reported.
+// The persistent coarse solve's grid barrier sets an error word instead of spinning on (its wait
+// is bounded); the word was copied into pinned memory before the caller's stream sync.  A word
+// that is set is cleared (so the engine stays usable) and reported.
 void Engine::check_device_waits() const {
   if (coopCtas && h_bar->err) {
-    const int code = h_bar->err;
     h_bar->err = 0;
     TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
-    throw DeviceWaitError(code == kCoopErrBarrier
-                              ? "coarse solve: a grid barrier wait gave up (cooperative launch not co-resident)"
-                              : "coarse solve: a wait for an entry of a solve vector gave up");
-  }
-  if (gf.ctrl && *h_gferr) {
-    *h_gferr = 0;
-    TOPX_CUDA_OK(cudaMemset(gf.ctrl, 0, sizeof(int)));
-    throw DeviceWaitError("coarse factorisation: a dependency wait of the Gauss-Jordan inverse gave up");
+    throw DeviceWaitError("coarse solve: a grid barrier wait gave up (persistent launch not co-resident)");
   }
 }
 
-// Drives one bounded device wait to its poll limit against a word that nothing writes (0: the
-// coarse solve's grid barrier, 1: its wait for one solve-vector entry, 2: its wait for a vector
-// of entries, 3: the Gauss-Jordan inverse's dependency wait).  The wait gives up within about a
-// second and the check below throws DeviceWaitError after clearing the error word.
+// Drives the grid barrier's bounded wait to its poll limit: a two-CTA grid whose second CTA
+// leaves without arriving.  The wait gives up within about a second and the check below throws
+// DeviceWaitError after clearing the error word.
 void Engine::selftest_wait(int which) {
-  if (which < 0 || which > 3) throw std::invalid_argument("selftest_wait: which must be 0, 1, 2 or 3");
-  if (which <= 2 && !coopCtas)
-    throw std::invalid_argument("selftest_wait: this context runs the coarse solve without a cooperative launch");
+  if (which != 0) throw std::invalid_argument("selftest_wait: which must be 0 (the coarse solve's grid barrier)");
+  if (!coopCtas)
+    throw std::invalid_argument("selftest_wait: this context runs the coarse solve without a persistent launch");
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  DevBuf<double> words;
-  words.alloc(80);
-  if (which <= 2) {
-    TOPX_CUDA_OK(cudaMemsetAsync(coopBar.p, 0, sizeof(CoopBarrier), st));
-    launch_coop_wait_selftest(st, which, coopBar.p, words.p);
-  } else {
-    launch_gf_wait_selftest(st, gf.ctrl, reinterpret_cast<unsigned*>(words.p));
-  }
+  TOPX_CUDA_OK(cudaMemsetAsync(coopBar.p, 0, sizeof(CoopBarrier), st));
+  launch_coop_barrier_selftest(st, coopBar.p);
   check_coop_barrier();
 }
 
@@ -476,17 +447,10 @@ void Engine::assemble_launches() {
 }
 
 void Engine::factor_coarsest() {
-  sec_begin(SEC_SLAB_ASSEMBLE);
-  launch_slab_assemble(st, G[nl - 1], si, Ks[nl - 1].p, present[nl - 1].p, slabA.p, slabBup.p);
-  sec_end();
   sec_begin(SEC_INVERSE);
-  launch_slab_factor(st, gf, si, slabA.p, slabBup.p, slabSinv.p, slabL.p, slabLT.p);
+  ndd.factor(st, nd, G[nl - 1], Ks[nl - 1].p);
+  if (pre32()) launch_convert<double, float>(st, ndPool.p, ndPool32.p, int64_t(ndPool.n));
   sec_end();
-  if (pre32()) {
-    launch_convert<double, float>(st, slabSinv.p, slabSinv32.p, int64_t(slabSinv.n));
-    launch_convert<double, float>(st, slabL.p, slabL32.p, int64_t(slabL.n));
-    launch_convert<double, float>(st, slabLT.p, slabLT32.p, int64_t(slabLT.n));
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -501,16 +465,8 @@ void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
   sec_end();
   sec_begin(SEC_COARSE_SOLVE);
   {
-    const bool f64 = std::is_same<TC, double>::value;
-    const TC* Inv = f64 ? (const TC*)slabSinv.p : (const TC*)slabSinv32.p;
-    const TC* Lf = f64 ? (const TC*)slabL.p : (const TC*)slabL32.p;
-    const TC* LT = f64 ? (const TC*)slabLT.p : (const TC*)slabLT32.p;
-    if (coopCtas)
-      launch_slab_solve_coop<TC, TC>(st, coopCtas, G[nl - 1], si, Inv, Lf, LT, v.rl[nl - 1].p, slabBS.p, slabW.p,
-                                     slabV.p, slabXS.p, v.xl[nl - 1].p, sc, coopBar.p);
-    else
-      launch_slab_solve<TC, TC>(st, G[nl - 1], si, Inv, Lf, LT, v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p,
-                                slabXS.p, v.xl[nl - 1].p, sc);
+    const TC* tiles = std::is_same<TC, double>::value ? (const TC*)ndPool.p : (const TC*)ndPool32.p;
+    ndd.solve<TC, TC>(st, nd, tiles, v.rl[nl - 1].p, v.xl[nl - 1].p, sc);
   }
   sec_end();
   sec_begin(SEC_PROLONG);
@@ -546,13 +502,7 @@ void Engine::vcycle_standard(bool init, PcgScalars* sc) {
   }
   sec_end();
   sec_begin(SEC_COARSE_SOLVE);
-  if (coopCtas)
-    launch_slab_solve_coop<double, double>(st, coopCtas, G[nl - 1], si, slabSinv.p, slabL.p, slabLT.p,
-                                           v.rl[nl - 1].p, slabBS.p, slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc,
-                                           coopBar.p);
-  else
-    launch_slab_solve<double, double>(st, G[nl - 1], si, slabSinv.p, slabL.p, slabLT.p, v.rl[nl - 1].p, slabBS.p,
-                                      slabW.p, slabV.p, slabXS.p, v.xl[nl - 1].p, sc);
+  ndd.solve<double, double>(st, nd, ndPool.p, v.rl[nl - 1].p, v.xl[nl - 1].p, sc);
   sec_end();
   sec_begin(SEC_PROLONG);
   for (int l = nl - 2; l >= 1; --l) {

@@ -15,6 +15,7 @@
 
 #include "topx_kernels.cuh"
 #include "topx_mesh.hpp"
+#include "topx_nd_dev.hpp"
 #include "topx_opt.cuh"
 
 namespace topx {
@@ -169,7 +170,6 @@ class Engine {
   bool pre32() const { return prec != PREC_FP64; }              // FP32 multigrid preconditioner
   bool flt32() const { return prec == PREC_MIXED_F32_FILTER; }  // FP32 PDE-filter CG
   cudaStream_t st = nullptr;
-  GJFlow gf{};  // dataflow inverse of the coarse factorisation: plans, scratch, control words
   int nl = 0;
   std::vector<Grid> G;  // per level
   int64_t Ne = 0, Nn = 0;
@@ -205,14 +205,19 @@ class Engine {
   DevBuf<int32_t> fl_elem, fl_tsel;
   DevBuf<double> fl_F;
   int nflag = 0;
-  SlabInfo si;
-  DevBuf<double> slabA, slabBup, slabSinv, slabL, slabLT, gfScr, gfY;
-  DevBuf<uint32_t> gfTasks[2];  // inverse task plans for one and two matrices
-  DevBuf<unsigned> gfCtrl;      // control words of the inverse (word 0: error flag)
-  DevBuf<float> slabSinv32, slabL32, slabLT32;  // FP32 copies applied by the mixed-precision V-cycle
-  DevBuf<double> slabBS, slabW, slabV, slabXS;  // slab-ordered vectors of one coarse solve
-  DevBuf<CoopBarrier> coopBar;  // barrier of the cooperative coarse solve
-  int coopCtas = 0;             // its CTA count; 0: multi-launch coarse solve
+  // coarsest level: nested-dissection plan, its device copy and the factor tiles
+  NDPlan nd;
+  NDDevice ndd;
+  DevBuf<NDFront> ndFronts;
+  DevBuf<NDTask> ndTasks;
+  DevBuf<NDAsm> ndAsm;
+  DevBuf<int64_t> ndPad;
+  DevBuf<int32_t> ndMap, ndSep, ndUpd, ndSrc0, ndSrc1;
+  DevBuf<double> ndPool, ndScr, ndW, ndPart;
+  DevBuf<unsigned> ndCnt;
+  DevBuf<float> ndPool32;  // FP32 copy applied by the mixed-precision V-cycle
+  DevBuf<CoopBarrier> coopBar;  // grid barrier of the persistent coarse solve
+  int coopCtas = 0;             // its CTA count; 0: one launch per tree level and direction
   void check_coop_barrier();    // waits for the stream; throws if a barrier wait gave up (re-arming it)
   void check_device_waits() const;  // after a stream sync: throws if a bounded device wait gave up
   // workspaces
@@ -233,7 +238,6 @@ class Engine {
   DevBuf<double> dscal;
   PcgScalars* h_sc = nullptr;  // pinned
   CoopBarrier* h_bar = nullptr;  // pinned
-  int* h_gferr = nullptr;        // pinned copy of gfCtrl[0]
   // optimiser state (compact, FP64)
   DevBuf<double> x, xPhys, dc, ce, tmpA, tmpB, xTilde, xhat, dfdx, dxv, volMax;
   DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;

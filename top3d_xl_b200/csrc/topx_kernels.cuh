@@ -106,69 +106,20 @@ void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const ui
 template <typename T>
 void launch_diag_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* present, T* d);
 
-// Slab block-LDL^T of the coarsest level (node grid split into slabs along `axis`)
-struct SlabInfo {
-  int axis = 0;        // 0:y 1:x 2:z
-  int ns = 0;          // number of slabs
-  int nu = 0, nv = 0;  // in-slab node dims (u varies fastest)
-  int m = 0;           // DOFs per slab = 3*nu*nv
-};
-void launch_slab_assemble(cudaStream_t st, Grid g, SlabInfo si, const double* Ks, const uint8_t* present, double* A,
-                          double* Bup);
-// one-time per-device kernel attributes of the coarse factorisation (call outside stream capture)
-void prepare_coarse_kernels();
 // caches the SM count used to shape the K*u launch (call once per device, outside capture)
 void prepare_fem_kernels();
-// Dataflow Gauss-Jordan inverse (topx_gjflow.cu): ticket-ordered task tables for one and two
-// matrices (gf_plan), ring scratch (gf_scratch_doubles) and control words (gf_ctrl_words; word
-// 0 is the error flag, set when a wait gave up, read and cleared by the host).
-struct GJFlow {
-  const uint32_t* tasks[2];
-  unsigned ntasks[2];
-  double* scratch;
-  unsigned* ctrl;
-  int nctas;
-  double* ytmp;  // 2 m x m: the coupling terms of the Schur complements, by rows, before transposition
-};
-// one-time per-device kernel attributes (call outside stream capture)
-void prepare_gj_flow();
-// CTAs of one inverse launch of order m: every SM for an engine alone on the GPU, else a few
-int gj_flow_ctas(bool whole_gpu, int m);
-// in-place inverse of the SPD m x m matrices A0 (and A1 when nset == 2)
-void launch_gj_flow(cudaStream_t st, int m, int nset, double* A0, double* A1, const uint32_t* tasks,
-                    unsigned ntasks, double* scratch, unsigned* ctrl, int nctas);
-// twisted block factorisation of the slab-tridiagonal coarsest matrix: Inv (ns m x m inverses of the
-// Schur complements), X (ns-1 coupling blocks L_s / U_s) and XT (their transposes)
-void launch_slab_factor(cudaStream_t st, const GJFlow& gf, SlabInfo si, const double* A, const double* Bup,
-                        double* Inv, double* X, double* XT);
-// x = K_coarsest^{-1} b; bs, W, V, xs are ns*m FP64 scratch vectors in slab order
-template <typename T, typename TM>
-void launch_slab_solve(cudaStream_t st, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT, const T* b,
-                       double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc);
 
-// State of the grid-wide barrier of the cooperative coarse solve (zeroed before first use;
-// err != 0 after a CTA gave up waiting, and then count must be zeroed again).
+// State of the grid-wide barrier of the persistent coarse solve (zeroed before first use;
+// err != 0 after a CTA gave up waiting, and then the words must be zeroed again).
 struct CoopBarrier {
   unsigned count;
   unsigned gen;
-  int err;  // 0, or the kind of wait that gave up first (kCoopErrBarrier, kCoopErrVector)
+  int err;  // 0, or kCoopErrBarrier once a barrier wait gave up
   int pad;
 };
 constexpr int kCoopErrBarrier = 1;  // a grid barrier wait gave up
-constexpr int kCoopErrVector = 2;   // a wait for an entry of a solve vector gave up
-// Self-test of the coarse solve's bounded waits (which: 0 grid barrier, 1 single entry, 2 vector
-// of entries) against words that nothing writes; `absent` holds 65 doubles of scratch.
-void launch_coop_wait_selftest(cudaStream_t st, int which, CoopBarrier* bar, double* absent);
-// Self-test of the Gauss-Jordan inverse's bounded dependency wait: waits for *word >= 1 where
-// nothing writes `word` (zeroed here); gives up and sets ctrl[0].
-void launch_gf_wait_selftest(cudaStream_t st, unsigned* ctrl, unsigned* word);
-// CTAs of launch_slab_solve_coop on the current device (one per SM), or 0 when cooperative
-// launch is unavailable; sets the kernels' shared-memory limit (call outside stream capture).
-int slab_solve_coop_ctas(int m);
-// the coarse solve above as one cooperative launch (same factors; rows summed in another order)
-template <typename T, typename TM>
-void launch_slab_solve_coop(cudaStream_t st, int nctas, Grid g, SlabInfo si, const TM* Inv, const TM* X, const TM* XT,
-                            const T* b, double* bs, double* W, double* V, double* xs, T* x, const PcgScalars* sc,
-                            CoopBarrier* bar);
+// Self-test of the barrier's bounded wait: a two-CTA grid whose second CTA leaves without
+// arriving, so the first CTA's wait runs into its poll limit (about a second) and sets bar->err.
+void launch_coop_barrier_selftest(cudaStream_t st, CoopBarrier* bar);
 
 }  // namespace topx

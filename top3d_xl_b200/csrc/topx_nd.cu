@@ -1,0 +1,571 @@
+// Device side of the nested-dissection multifrontal factorisation and solve of the coarsest-
+// level matrix (plan and storage in topx_nd.hpp).  Replaces the reference's sparse Cholesky
+// with fill-reducing permutation (chol(K,'lower'), TOP3D_XL.m:1052-1065) and its triangular
+// solves in the V-cycle (TOP3D_XL.m:767): the same exact solve, another elimination order.
+//
+// Factorisation, per tree level from the leaves up: extend-add of the children's Schur
+// complements, then for k = 0 .. T1-1 three launches over all fronts of the level:
+//   pivot   P^-1 of tile (k, k) (register-blocked Gauss-Jordan on the tensor cores), with the
+//           write-back of the previous step's row and column;
+//   panel   R_j = -P^-1 A[k][j] for every tile column j != k (into scratch);
+//   update  A[i][j] += A[i][k] R_j for every stored tile (i >= j), i, j != k;
+// and at the end of a step the new row k is R and the new column k is -R^T.  Only the lower
+// triangle of tiles is stored: an upper tile is the transpose of its mirror, negated when
+// exactly one of its two tile indices has already been swept.
+// Solve, per level: up the tree f = b + children's updates, w1 = F11^-1 f1, u = f2 - X f1;
+// down the tree x1 = w1 - X^T x2.  No kernel waits on another: launches order the steps.
+#include <algorithm>
+#include <mutex>
+
+#include "topx_coop.cuh"
+#include "topx_kernels.cuh"
+#include "topx_nd.hpp"
+#include "topx_nd_dev.hpp"
+#include "topx_tile64.cuh"
+
+namespace topx {
+
+namespace {
+
+constexpr int ND_TILE = ND_T * ND_T;
+constexpr int ND_THREADS = GF_THREADS;  // 256
+constexpr size_t ND_SMEM_SWEEP = size_t(3) * GF_BUF * sizeof(double);
+static_assert(ND_T == GF_T, "tile widths");
+
+__device__ __forceinline__ int64_t nd_tri(int64_t i) { return i * (i + 1) / 2; }
+__device__ __forceinline__ double* nd_tile(double* pool, const NDFront& d, int i, int j) {
+  return pool + (d.tile0 + nd_tri(i) + j) * ND_TILE;
+}
+template <typename TM>
+__device__ __forceinline__ const TM* nd_tile_c(const TM* pool, const NDFront& d, int i, int j) {
+  return pool + (d.tile0 + nd_tri(i) + j) * ND_TILE;
+}
+// the stored element of the symmetric entry (p1, p2) of front d; also its mirror inside a
+// diagonal tile (-1 when there is none)
+__device__ __forceinline__ void nd_entry(const NDFront& d, int p1, int p2, int64_t& at, int64_t& mirror) {
+  const int hi = max(p1, p2), lo = min(p1, p2);
+  const int ti = hi / ND_T, tj = lo / ND_T;
+  const int64_t base = (d.tile0 + nd_tri(ti) + tj) * ND_TILE;
+  at = base + (hi % ND_T) * ND_T + lo % ND_T;
+  mirror = (ti == tj && hi != lo) ? base + (lo % ND_T) * ND_T + hi % ND_T : -1;
+}
+
+// s[t][c] (row stride ld) = sgn * g[c][t] for a contiguous 64 x 64 tile g
+__device__ __forceinline__ void nd_stage_transposed(double* s, const double* g, int ld, double sgn) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) {
+    const int c = e >> 6, t = e & 63;
+    s[t * ld + c] = sgn * __ldcg(g + e);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// assembly of the original matrix into the fronts (writes), and the padding identity
+// ---------------------------------------------------------------------------
+__global__ void k_nd_assemble(Grid g, const NDFront* __restrict__ fronts, const NDAsm* __restrict__ asmb, int64_t n,
+                              const double* __restrict__ Ks, double* __restrict__ pool) {
+  const int nny = g.ny + 1, nnx = g.nx + 1;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x) {
+    const NDAsm e = asmb[t];
+    const NDFront d = fronts[e.f];
+    const int ay = e.a % nny, ax = (e.a / nny) % nnx, az = e.a / (nny * nnx);
+    const int by = e.b % nny, bx = (e.b / nny) % nnx, bz = e.b / (nny * nnx);
+    double blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int la = 0; la < 8; ++la) {  // the hexes around node a that also hold node b
+      const int ey = ay - hex_ly(la), ex = ax - hex_lx(la), ez = az - hex_lz(la);
+      if (ey < 0 || ey >= g.ny || ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+      const int ly = by - ey, lx = bx - ex, lz = bz - ez;
+      if (ly < 0 || ly > 1 || lx < 0 || lx > 1 || lz < 0 || lz > 1) continue;
+      const int lb = hex_local(ly, lx, lz);
+      const double* K = Ks + (ey + int64_t(g.ny) * (ex + int64_t(g.nx) * ez)) * 576;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) blk[i * 3 + j] += K[(3 * la + i) * 24 + 3 * lb + j];
+    }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        int64_t at, mir;
+        nd_entry(d, e.pa + i, e.pb + j, at, mir);
+        pool[at] = blk[i * 3 + j];
+        if (mir >= 0) pool[mir] = blk[i * 3 + j];
+      }
+  }
+}
+
+__global__ void k_nd_pad(const int64_t* __restrict__ at, int64_t n, double* __restrict__ pool) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    pool[at[t]] = 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// extend-add: child tile (i, j) of its update block into the parent front (adds; the map is
+// one to one, so no two threads of a launch touch one entry)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(ND_THREADS) k_nd_extend(const NDFront* __restrict__ fronts,
+                                                          const NDTask* __restrict__ tasks,
+                                                          const int32_t* __restrict__ upd_map,
+                                                          double* __restrict__ pool) {
+  const NDTask tk = tasks[blockIdx.x];
+  const NDFront c = fronts[tk.f];
+  const NDFront d = fronts[c.parent];
+  const double* src = nd_tile(pool, c, tk.i, tk.j);
+  const int P1 = ND_T * c.T1;
+  for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) {
+    const int r = e >> 6, cc = e & 63;
+    const int k1 = ND_T * tk.i + r - P1, k2 = ND_T * tk.j + cc - P1;
+    if (k1 >= c.n2 || k2 >= c.n2 || (tk.i == tk.j && r < cc)) continue;
+    const double v = src[e];
+    int64_t at, mir;
+    nd_entry(d, upd_map[c.map0 + k1], upd_map[c.map0 + k2], at, mir);
+    pool[at] += v;
+    if (mir >= 0) pool[mir] += v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sweep step k
+// ---------------------------------------------------------------------------
+// Blocks [0, npiv): pivot of front f: tile (k, k) <- its inverse, also into scratch slot 0.
+// Blocks [npiv, gridDim.x): write-back of step i = k-1 for tile column j: row i takes R_j
+// (j < i) or column i takes -R_j^T (j > i).
+__global__ void __launch_bounds__(ND_THREADS) k_nd_pivot(const NDFront* __restrict__ fronts,
+                                                         const NDTask* __restrict__ tasks, int npiv,
+                                                         double* __restrict__ pool, double* __restrict__ scr) {
+  extern __shared__ __align__(16) double nd_smem[];
+  const NDTask tk = tasks[blockIdx.x];
+  const NDFront d = fronts[tk.f];
+  if (int(blockIdx.x) < npiv) {
+    double* A = nd_tile(pool, d, tk.i, tk.i);
+    double acc[4][2][2];
+    gf_for_outputs(acc, [&](int r, int c, double& v) { v = __ldcg(A + r * ND_T + c); });
+    double* Pinv = scr + int64_t(d.scr0) * ND_TILE;
+    gf_pivot(acc, nullptr, 0, 0, ND_T, Pinv, *reinterpret_cast<GFPivotSmem*>(nd_smem));
+    gf_for_outputs(acc, [&](int r, int c, double v) { A[r * ND_T + c] = v; });
+    return;
+  }
+  const double* R = scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE;
+  if (tk.j < tk.i) {
+    double* D = nd_tile(pool, d, tk.i, tk.j);
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = __ldcg(R + e);
+  } else {
+    double* D = nd_tile(pool, d, tk.j, tk.i);
+    double* s = nd_smem;  // [64][65]
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) s[(e >> 6) * 65 + (e & 63)] = __ldcg(R + e);
+    __syncthreads();
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = -s[(e & 63) * 65 + (e >> 6)];
+  }
+}
+
+// R_j = -P^-1 A[k][j] into scratch slot 1 + j
+__global__ void __launch_bounds__(ND_THREADS) k_nd_panel(const NDFront* __restrict__ fronts,
+                                                         const NDTask* __restrict__ tasks, int k,
+                                                         const double* __restrict__ pool, double* __restrict__ scr) {
+  extern __shared__ __align__(16) double nd_smem[];
+  double* bufA = nd_smem;
+  double* bufB = nd_smem + GF_BUF;
+  const NDTask tk = tasks[blockIdx.x];
+  const NDFront d = fronts[tk.f];
+  const double* Pinv = scr + int64_t(d.scr0) * ND_TILE;
+  gf_stage_ring(bufA, Pinv, GF_LDA);
+  if (tk.j < k)
+    gf_stage_ring(bufB, nd_tile_c(pool, d, k, tk.j), GF_LD);
+  else
+    nd_stage_transposed(bufB, nd_tile_c(pool, d, tk.j, k), GF_LD, 1.0);
+  gf_cp_wait();
+  __syncthreads();
+  double acc[4][2][2];
+  gf_for_outputs(acc, [&](int, int, double& v) { v = 0.0; });
+  gf_product(bufA, bufB, acc);
+  double* R = scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE;
+  gf_for_outputs(acc, [&](int r, int c, double v) { R[r * ND_T + c] = -v; });
+}
+
+// A[i][j] += A[i][k] R_j for a stored tile (i >= j)
+__global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restrict__ fronts,
+                                                          const NDTask* __restrict__ tasks, int k,
+                                                          double* __restrict__ pool, const double* __restrict__ scr) {
+  extern __shared__ __align__(16) double nd_smem[];
+  double* bufA = nd_smem;
+  double* bufB = nd_smem + GF_BUF;
+  double* bufD = nd_smem + 2 * GF_BUF;
+  const NDTask tk = tasks[blockIdx.x];
+  const NDFront d = fronts[tk.f];
+  if (tk.i > k)
+    gf_stage_ring(bufA, nd_tile_c(pool, d, tk.i, k), GF_LDA);
+  else  // tile column i is swept, k is not: A[i][k] = -A[k][i]^T
+    nd_stage_transposed(bufA, nd_tile_c(pool, d, k, tk.i), GF_LDA, -1.0);
+  gf_stage_ring(bufB, scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE, GF_LD);
+  double* D = nd_tile(pool, d, tk.i, tk.j);
+  gf_stage_ring(bufD, D, GF_LD);
+  gf_cp_wait();
+  __syncthreads();
+  double acc[4][2][2];
+  gf_for_outputs(acc, [&](int r, int c, double& v) { v = bufD[r * GF_LD + c]; });
+  gf_product(bufA, bufB, acc);
+  __syncthreads();
+  gf_for_outputs(acc, [&](int r, int c, double v) { bufD[r * GF_LD + c] = v; });
+  __syncthreads();
+  gf_copy_to_ring(D, bufD, GF_LD);
+}
+
+// ---------------------------------------------------------------------------
+// solve: GEMVs over whole tiles.  A warp streams a tile with coalesced 16-byte loads: lane
+// (h, c) = (lane / 16, lane % 16) reads columns 4c .. 4c + 3 of rows 2 k + h.  Row sums
+// (y = A x) are kept per row and reduced across the 16 lanes of a half by recursive halving,
+// which leaves lane (h, c) the rows 4c + h and 4c + 2 + h; column sums (y = A^T x) are kept
+// per column and the two halves added.  Either way a lane ends with outputs 4c + h, 4c + 2 + h.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void nd_load4(const double* p, double (&v)[4]) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+__device__ __forceinline__ void nd_load4(const float* p, double (&v)[4]) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+
+// acc[k] += tile row (2k + h) (of the 32 rows at t), columns 4c .. 4c + 3, times x[4c ..]
+template <typename TM>
+__device__ __forceinline__ void nd_rows(const TM* t, const double* x, int h, int c, double (&acc)[16]) {
+  const double x0 = x[4 * c], x1 = x[4 * c + 1], x2 = x[4 * c + 2], x3 = x[4 * c + 3];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double v[4];
+    nd_load4(t + (2 * k + h) * ND_T + 4 * c, v);
+    acc[k] = fma(v[0], x0, fma(v[1], x1, fma(v[2], x2, fma(v[3], x3, acc[k]))));
+  }
+}
+// col[e] += sum over the rows (2k + h) of the 32 rows at t of t[row][4c + e] x[row]
+template <typename TM>
+__device__ __forceinline__ void nd_cols(const TM* t, const double* x, int h, int c, double (&col)[4]) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int row = 2 * k + h;
+    double v[4];
+    nd_load4(t + row * ND_T + 4 * c, v);
+    const double xr = x[row];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) col[e] = fma(v[e], xr, col[e]);
+  }
+}
+// recursive halving of 16 row sums over the 16 lanes of a half: lane c ends with the sum of
+// local row k = c, i.e. row 2c + h of the 32 rows
+__device__ __forceinline__ double nd_reduce_rows(double (&acc)[16], int c) {
+#pragma unroll
+  for (int o = 8, n = 16; o >= 1; o >>= 1, n >>= 1) {
+    const bool up = (c & o) != 0;
+#pragma unroll
+    for (int t = 0; t < n / 2; ++t) {
+      const double send = up ? acc[t] : acc[t + n / 2];
+      const double keep = up ? acc[t + n / 2] : acc[t];
+      acc[t] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return acc[0];
+}
+
+// One chunk (up to ND_CHUNK input tiles) of output tile i: warp w takes rows 32 (w & 1) .. + 31
+// of input tile w >> 1 and leaves its part of the 64 outputs in red[w][].  Row sums (y = A x)
+// give each lane the row 2c + h of its 32; column sums (y = A^T x) the columns 4c + h, 4c + 2 + h.
+template <typename TM>
+__device__ __forceinline__ void nd_chunk_rows(const TM* t, const double* x, double* redw, int rh, int h, int c) {
+  double acc[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+  nd_rows(t + 32 * rh * ND_T, x, h, c, acc);
+  redw[32 * rh + 2 * c + h] = nd_reduce_rows(acc, c);
+}
+template <typename TM>
+__device__ __forceinline__ void nd_chunk_cols(const TM* t, const double* x, double* redw, int rh, int h, int c) {
+  double col[4] = {0.0, 0.0, 0.0, 0.0};
+  nd_cols(t + 32 * rh * ND_T, x + 32 * rh, h, c, col);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) col[e] += __shfl_xor_sync(0xffffffffu, col[e], 16);
+  redw[4 * c + h] = h ? col[1] : col[0];
+  redw[4 * c + 2 + h] = h ? col[3] : col[2];
+}
+
+// The 64 sums of a chunk (threads < 64 hold them in s) complete output tile `id`: with one
+// chunk the caller writes at once; else the chunk's partial goes to part[ti] (ti: the task's
+// index in its launch or phase), and the last CTA of the output tile to finish (atomic ticket,
+// no waiting) adds the chunks in order.  Returns true (with s the total) in the threads < 64 of
+// the CTA that writes the output.
+__device__ __forceinline__ bool nd_finish(double& s, int64_t ti, int ch, int nch, unsigned* cnt, int64_t id,
+                                          double* part, bool* last) {
+  if (nch == 1) return threadIdx.x < ND_T;
+  if (threadIdx.x < ND_T) part[ti * ND_T + threadIdx.x] = s;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) *last = atomicAdd(cnt + id, 1u) == unsigned(nch - 1);
+  __syncthreads();
+  if (!*last) return false;
+  __threadfence();
+  if (threadIdx.x == 0) cnt[id] = 0u;  // ready for the next launch
+  if (threadIdx.x < ND_T) {
+    double t = 0.0;
+    for (int q = 0; q < nch; ++q) t += __ldcg(part + (ti - ch + q) * ND_T + threadIdx.x);
+    s = t;
+  }
+  return threadIdx.x < ND_T;
+}
+
+struct NDSolveSmem {
+  double vec[ND_CHUNK * ND_T];  // the chunk's input entries
+  double red[8][ND_T];
+  bool last;
+};
+
+template <typename T, typename TM>
+struct NDSolveArgs {
+  const NDFront* fronts;
+  const NDTask* tasks;
+  const TM* pool;
+  const T* b;
+  T* x;
+  const int32_t *sep_dof, *upd_dof, *src0, *src1;
+  double* w;
+  double* part;
+  unsigned* cnt;
+};
+
+// Forward task: one chunk of the eliminated tiles for output tile i of a front, per level up the
+// tree.  i < T1: w = F11^-1 f1; i >= T1: w = f2 - X f1, where f1 is the eliminated part of the
+// front's right-hand side (b at its DOFs plus what its children's updates put there) and f2
+// what the children's updates put on the update DOFs.
+template <typename T, typename TM>
+__device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
+                                                NDSolveSmem& sm) {
+  const NDFront d = a.fronts[tk.f];
+  const int i = tk.i, ch = tk.j;
+  const int nch = max(1, (d.T1 + ND_CHUNK - 1) / ND_CHUNK);
+  const int j0 = ch * ND_CHUNK, nj = min(ND_CHUNK, d.T1 - j0);
+  auto rhs = [&](int64_t p) {
+    const int32_t g = a.sep_dof[p], s0 = a.src0[p], s1 = a.src1[p];
+    // values written by other CTAs earlier in a persistent launch: loads bypass L1
+    double v = g >= 0 ? double(a.b[g]) : 0.0;
+    if (s0 >= 0) v += __ldcg(a.w + s0);
+    if (s1 >= 0) v += __ldcg(a.w + s1);
+    return v;
+  };
+  __syncthreads();  // the previous task's readers of sm are done
+  for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) sm.vec[p] = rhs(d.pos0 + int64_t(ND_T) * j0 + p);
+  for (int e = threadIdx.x; e < 8 * ND_T; e += ND_THREADS) sm.red[e >> 6][e & 63] = 0.0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
+  const int ts = warp >> 1, rh = warp & 1;
+  if (ts < nj) {
+    const int j = j0 + ts;
+    if (i >= d.T1 || j <= i)
+      nd_chunk_rows(nd_tile_c(a.pool, d, i, j), sm.vec + ND_T * ts, sm.red[warp], rh, h, c);
+    else  // F11^-1 (i, j) = (stored tile (j, i))^T
+      nd_chunk_cols(nd_tile_c(a.pool, d, j, i), sm.vec + ND_T * ts, sm.red[warp], rh, h, c);
+  }
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < ND_T)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += sm.red[q][threadIdx.x];
+  if (nd_finish(s, ti, ch, nch, a.cnt, d.pos0 / ND_T + i, a.part, &sm.last)) {
+    const int64_t p = d.pos0 + ND_T * i + threadIdx.x;
+    a.w[p] = i < d.T1 ? s : rhs(p) - s;
+  }
+}
+
+// Backward task: one chunk of the update tiles for output tile i < T1 of a front, per level
+// down the tree: x1 = w1 - X^T x2, with x2 gathered from the solution at the update DOFs
+// (written by the ancestors' phases); x1 goes to the separator DOFs.
+template <typename T, typename TM>
+__device__ __forceinline__ void nd_backward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
+                                                 NDSolveSmem& sm) {
+  const NDFront d = a.fronts[tk.f];
+  const int i = tk.i, ch = tk.j, P1 = ND_T * d.T1;
+  const int nch = max(1, (d.N - d.T1 + ND_CHUNK - 1) / ND_CHUNK);
+  const int j0 = d.T1 + ch * ND_CHUNK, nj = min(ND_CHUNK, d.N - j0);
+  __syncthreads();
+  for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) {
+    const int u = ND_T * (j0 - d.T1) + p;  // update DOF
+    sm.vec[p] = u < d.n2 ? double(__ldcg(a.x + a.upd_dof[d.pos0 + P1 + u])) : 0.0;
+  }
+  for (int e = threadIdx.x; e < 8 * ND_T; e += ND_THREADS) sm.red[e >> 6][e & 63] = 0.0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
+  const int ts = warp >> 1, rh = warp & 1;
+  if (ts < nj) nd_chunk_cols(nd_tile_c(a.pool, d, j0 + ts, i), sm.vec + ND_T * ts, sm.red[warp], rh, h, c);
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < ND_T)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += sm.red[q][threadIdx.x];
+  if (nd_finish(s, ti, ch, nch, a.cnt, d.pos0 / ND_T + i, a.part, &sm.last)) {
+    const int64_t p = d.pos0 + ND_T * i + threadIdx.x;
+    const int32_t g = a.sep_dof[p];
+    if (g >= 0) a.x[g] = T(__ldcg(a.w + p) - s);
+  }
+}
+
+// one launch per tree level and direction
+template <typename T, typename TM, bool FWD>
+__global__ void __launch_bounds__(ND_THREADS) k_nd_solve_level(NDSolveArgs<T, TM> a, const PcgScalars* sc) {
+  if (sc && sc->done) return;
+  __shared__ NDSolveSmem sm;
+  if (FWD)
+    nd_forward_task(a, a.tasks[blockIdx.x], blockIdx.x, sm);
+  else
+    nd_backward_task(a, a.tasks[blockIdx.x], blockIdx.x, sm);
+}
+
+// The whole solve as one persistent launch (all CTAs resident): the phases (forward levels from
+// the leaves up, then backward levels from the root down) are separated by the bounded grid
+// barrier; within a phase the CTAs take its tasks in turn.
+constexpr int ND_MAX_PHASES = 64;
+struct NDPhases {
+  int64_t begin[ND_MAX_PHASES], end[ND_MAX_PHASES];
+  int n, nfwd;
+};
+
+template <typename T, typename TM>
+__global__ void __launch_bounds__(ND_THREADS) k_nd_solve_coop(NDSolveArgs<T, TM> a, NDPhases ph, const PcgScalars* sc,
+                                                              CoopBarrier* bar) {
+  if (sc && sc->done) return;  // the same for every CTA
+  __shared__ NDSolveSmem sm;
+  unsigned epoch = 0;
+  for (int q = 0; q < ph.n; ++q) {
+    for (int64_t t = ph.begin[q] + blockIdx.x; t < ph.end[q]; t += gridDim.x) {
+      if (q < ph.nfwd)
+        nd_forward_task(a, a.tasks[t], t - ph.begin[q], sm);
+      else
+        nd_backward_task(a, a.tasks[t], t - ph.begin[q], sm);
+    }
+    if (q + 1 < ph.n && !coop_barrier(bar, epoch)) break;
+  }
+  coop_exit(bar);
+}
+
+__global__ void k_coop_barrier_selftest(CoopBarrier* bar) {
+  if (blockIdx.x != 0) return;  // never arrives
+  unsigned epoch = 0;
+  coop_barrier(bar, epoch);
+}
+
+inline unsigned nd_grid(int64_t n, int threads) {
+  return unsigned(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 16)));
+}
+
+}  // namespace
+
+void prepare_nd_kernels() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  TOPX_CUDA_OK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return;
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_nd_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ND_SMEM_SWEEP)));
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_nd_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ND_SMEM_SWEEP)));
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_nd_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ND_SMEM_SWEEP)));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+void NDDevice::factor(cudaStream_t st, const NDPlan& P, Grid g, const double* Ks) const {
+  TOPX_CUDA_OK(cudaMemsetAsync(pool, 0, sizeof(double) * size_t(P.ntiles) * ND_TILE, st));
+  const int64_t na = int64_t(P.asmb.size()), np = int64_t(P.pad_diag.size());
+  (k_nd_assemble<<<nd_grid(na, 256), 256, 0, st>>>(g, fronts, asmb, na, Ks, pool), topx::count_launch());
+  if (np) (k_nd_pad<<<nd_grid(np, 256), 256, 0, st>>>(pad, np, pool), topx::count_launch());
+  for (int l = int(P.levels.size()) - 1; l >= 0; --l) {
+    const NDLevel& L = P.levels[size_t(l)];
+    for (int s = 0; s < 2; ++s) {
+      const int64_t n = L.ext[s + 1] - L.ext[s];
+      if (n) (k_nd_extend<<<unsigned(n), ND_THREADS, 0, st>>>(fronts, tasks + L.ext[s], upd_map, pool), topx::count_launch());
+    }
+    for (int k = 0; k < L.maxT1; ++k) {
+      const int64_t* s = &L.step[size_t(5) * k];
+      const int64_t npiv = s[1] - s[0], nfin = s[2] - s[1], npan = s[3] - s[2], nupd = s[4] - s[3];
+      (k_nd_pivot<<<unsigned(npiv + nfin), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[0], int(npiv), pool, scr),
+       topx::count_launch());
+      if (npan)
+        (k_nd_panel<<<unsigned(npan), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[2], k, pool, scr),
+         topx::count_launch());
+      if (nupd)
+        (k_nd_update<<<unsigned(nupd), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[3], k, pool, scr),
+         topx::count_launch());
+    }
+    const int64_t nfin = L.fin_last[1] - L.fin_last[0];
+    if (nfin)
+      (k_nd_pivot<<<unsigned(nfin), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + L.fin_last[0], 0, pool, scr),
+       topx::count_launch());
+  }
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+template <typename T, typename TM>
+void NDDevice::solve(cudaStream_t st, const NDPlan& P, const TM* tiles, const T* b, T* x, const PcgScalars* sc) const {
+  NDSolveArgs<T, TM> a{fronts, tasks, tiles, b, x, sep_dof, upd_dof, src0, src1, wvec, part, cnt};
+  const int nlev = int(P.levels.size());
+  if (coop_ctas > 0 && 2 * nlev <= ND_MAX_PHASES) {
+    NDPhases ph{};
+    for (int l = nlev - 1; l >= 0; --l) {
+      ph.begin[ph.n] = P.levels[size_t(l)].fwd[0];
+      ph.end[ph.n++] = P.levels[size_t(l)].fwd[1];
+    }
+    ph.nfwd = ph.n;
+    for (int l = 0; l < nlev; ++l) {
+      ph.begin[ph.n] = P.levels[size_t(l)].bwd[0];
+      ph.end[ph.n++] = P.levels[size_t(l)].bwd[1];
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(coop_ctas));
+    cfg.blockDim = dim3(ND_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TOPX_CUDA_OK(cudaLaunchKernelEx(&cfg, k_nd_solve_coop<T, TM>, a, ph, sc, bar));
+    topx::count_launch();
+    return;
+  }
+  for (int l = nlev - 1; l >= 0; --l) {
+    const NDLevel& L = P.levels[size_t(l)];
+    a.tasks = tasks + L.fwd[0];
+    (k_nd_solve_level<T, TM, true><<<unsigned(L.fwd[1] - L.fwd[0]), ND_THREADS, 0, st>>>(a, sc), topx::count_launch());
+  }
+  for (int l = 0; l < nlev; ++l) {
+    const NDLevel& L = P.levels[size_t(l)];
+    a.tasks = tasks + L.bwd[0];
+    if (L.bwd[1] > L.bwd[0])
+      (k_nd_solve_level<T, TM, false><<<unsigned(L.bwd[1] - L.bwd[0]), ND_THREADS, 0, st>>>(a, sc), topx::count_launch());
+  }
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+int nd_solve_coop_ctas() {
+  int dev = 0, coop = 0, nsm = 0, per = 0, per32 = 0;
+  TOPX_CUDA_OK(cudaGetDevice(&dev));
+  TOPX_CUDA_OK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  TOPX_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (!coop) return 0;
+  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_nd_solve_coop<double, double>, ND_THREADS, 0));
+  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_nd_solve_coop<float, float>, ND_THREADS, 0));
+  per = std::min(std::min(per, per32), 2);
+  return per >= 1 ? nsm * per : 0;
+}
+
+void launch_coop_barrier_selftest(cudaStream_t st, CoopBarrier* bar) {
+  (k_coop_barrier_selftest<<<2, 32, 0, st>>>(bar), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
+}
+
+template void NDDevice::solve<double, double>(cudaStream_t, const NDPlan&, const double*, const double*, double*,
+                                             const PcgScalars*) const;
+template void NDDevice::solve<float, float>(cudaStream_t, const NDPlan&, const float*, const float*, float*,
+                                           const PcgScalars*) const;
+
+}  // namespace topx

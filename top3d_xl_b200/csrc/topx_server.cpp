@@ -4,9 +4,8 @@
 // model, estimates its device footprint from the model's grid sizes and waits until that
 // footprint fits the HBM budget; then it creates the job's engine (own stream, own graphs,
 // own scratch), runs the optimisation loop and frees everything.  Jobs on different workers
-// overlap on the device.  Engines here use the multi-launch coarsest solve and ordinary CTAs
-// for the factorisation's side-stream update: a cooperative launch wants every SM at once and
-// SM-reserving CTAs would starve the neighbouring jobs.
+// overlap on the device.  Engines here run the coarsest-level solve level by level rather than
+// as one persistent launch, which would want all of its CTAs resident at once.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -21,7 +20,7 @@
 
 #include "topx.h"
 #include "topx_engine.hpp"
-#include "topx_gjflow.hpp"
+#include "topx_nd.hpp"
 
 namespace {
 
@@ -37,22 +36,25 @@ struct Job {
 };
 
 // Device bytes an engine for this model will hold: dense level-1 grid vectors and element
-// arrays, the coarsest level's slab factors, and fixed scratch.  Calibrated to stay above the
-// bytes the engine's buffers report (see the serving test).
+// arrays, the coarsest level's factor tiles with their plan and solve vectors (planned here for
+// the full box of coarsest nodes, an upper bound for a masked domain), and fixed scratch.
+// Calibrated to stay above the bytes the engine's buffers report (see the serving test).
 int64_t footprint_estimate(const topx_info& in, int precision) {
   const int64_t ny = in.resY[0], nx = in.resX[0], nz = in.resZ[0];
   const int64_t nodes = (ny + 1) * (nx + 1) * (nz + 1), elems = ny * nx * nz;
   const int L = in.numLevels - 1;
-  int64_t d[3] = {in.resY[L] + 1, in.resX[L] + 1, in.resZ[L] + 1};
-  std::sort(d, d + 3);
-  const int64_t ns = d[2], m = 3 * d[0] * d[1];
-  const int64_t slab = (2 * ns + 2 * (ns - 1) + 2) * m * m * 8 + (precision != TOPX_FP64 ? 3 * ns * m * m * 4 : 0);
-  // the Gauss-Jordan inverse's ring scratch, control words and task plans (~nt^3 tasks each)
-  const int64_t nt = topx::gf_tiles(int(m));
-  const int64_t inverse = int64_t(topx::gf_scratch_doubles(int(m))) * 8 + int64_t(topx::gf_ctrl_words(int(m))) * 4 +
-                          3 * nt * (nt * nt + 2 * nt + 1) * 4;
+  const int nny = in.resY[L] + 1, nnx = in.resX[L] + 1, nnz = in.resZ[L] + 1;
+  const std::vector<uint8_t> all(size_t(nny) * nnx * nnz, 1);
+  const int64_t stride = (int64_t(nny) * nnx * nnz + 31) / 32 * 32;
+  const topx::NDPlan P = topx::nd_plan(nny, nnx, nnz, stride, all);
+  const int64_t tile = int64_t(topx::ND_T) * topx::ND_T;
+  const int64_t coarsest = P.ntiles * tile * (precision != TOPX_FP64 ? 12 : 8) + int64_t(P.nscr) * tile * 8 +
+                           P.npos * (8 + 16) + P.nsolve_tasks * topx::ND_T * 8 + P.npos / topx::ND_T * 4 +
+                           int64_t(P.tasks.size()) * 8 + int64_t(P.asmb.size()) * 20 +
+                           int64_t(P.pad_diag.size()) * 8 + int64_t(P.upd_map.size()) * 4 +
+                           int64_t(P.fronts.size()) * int64_t(sizeof(topx::NDFront));
   const int64_t per_node = precision != TOPX_FP64 ? 584 : 544, per_elem = 200;
-  return per_node * nodes + per_elem * elems + slab + inverse + (int64_t(48) << 20);
+  return per_node * nodes + per_elem * elems + coarsest + (int64_t(48) << 20);
 }
 
 }  // namespace
