@@ -176,6 +176,18 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   }
   Ks.resize(nl);
   for (int l = 1; l < nl; ++l) Ks[l].alloc(size_t(G[l].nelems()) * 576);
+  // ---- level-1 K*u: the tiles that own a node of the domain (when voids leave some out) -----
+  {
+    std::vector<uint8_t> pn(size_t(G[0].nnodes()), 0);
+    for (auto k : M.levels[0].nodMapBack) pn[k - 1] = 1;
+    const std::vector<uint32_t> act = ku_active_tiles(G[0], pn);
+    const std::vector<uint8_t> all(pn.size(), 1);
+    const size_t full = ku_active_tiles(G[0], all).size();
+    if (!act.empty() && act.size() < full * 9 / 10) {
+      kuTiles.upload(act.data(), act.size());
+      kut = KuTiles{kuTiles.p, int(act.size())};
+    }
+  }
   // ---- coarsest level: nested-dissection plan and factor storage -----------------
   {
     const Grid& g = G[nl - 1];
@@ -490,7 +502,7 @@ void Engine::vcycle_standard(bool init, PcgScalars* sc) {
   const double om = M.S.weightFactorJacobi;
   sec_begin(SEC_RESTRICT);
   launch_jacobi_pre<double, double, double>(st, G[0], kw.r.p, v.d1.p, present[0].p, kw.z.p, om, sc);
-  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
   launch_residual_inplace<double, double>(st, G[0], kw.r.p, kw.q.p, sc);
   launch_restrict<double, double>(st, M.levels[1].span, kw.q.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
   for (int l = 1; l < nl - 1; ++l) {
@@ -514,7 +526,7 @@ void Engine::vcycle_standard(bool init, PcgScalars* sc) {
   }
   launch_prolong_add<double, double, double>(st, M.levels[1].span, v.xl[1].p, G[1], kw.r.p, v.d1.p, present[0].p,
                                              kw.z.p, G[0], om, sc);
-  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+  launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
   launch_jacobi_correct<double, double, double>(st, G[0], kw.r.p, kw.q.p, v.d1.p, present[0].p, kw.z.p, om, true,
                                                 init, sc, rs1);
   sec_end();
@@ -539,7 +551,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
   std::snprintf(key, sizeof(key), "pcg_init:%p:%p:%d:%.17g:%d", (const void*)b, (const void*)y, int(warm), tol, maxIT);
   run_graph(key, [&]() {
     if (warm)
-      launch_ku<double>(st, KU_PLAIN, g, y, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+      launch_ku<double>(st, KU_PLAIN, g, y, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
     else
       TOPX_CUDA_OK(cudaMemsetAsync(kw.q.p, 0, kw.q.bytes(), st));
     launch_residual_init<double>(st, g, b, kw.q.p, kw.r.p, sc, rs1, tol, maxIT);
@@ -556,7 +568,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
         for (int c = 0; c < CH; ++c) {  // CH is even: every chunk starts from p
           double* pin = (c & 1) ? kw.p2.p : kw.p.p;
           double* pnew = (c & 1) ? kw.p.p : kw.p2.p;
-          launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+          launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
           launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
           vcycle(false, sc);
         }
@@ -570,7 +582,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c], st));
       double* pin = (launched & 1) ? kw.p2.p : kw.p.p;
       double* pnew = (launched & 1) ? kw.p.p : kw.p2.p;
-      launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1);
+      launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
       sec_begin(SEC_UPDATE);
       launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);

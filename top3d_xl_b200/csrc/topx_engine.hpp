@@ -205,6 +205,8 @@ class Engine {
   DevBuf<int32_t> fl_elem, fl_tsel;
   DevBuf<double> fl_F;
   int nflag = 0;
+  DevBuf<uint32_t> kuTiles;  // level-1 K*u tiles that own a node of the domain
+  KuTiles kut;               // their list (null: the whole grid)
   // coarsest level: nested-dissection plan, its device copy and the factor tiles
   NDPlan nd;
   NDDevice ndd;

@@ -5,6 +5,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <type_traits>
+#include <vector>
 
 #include "topx_ke_classes.h"
 #include "topx_kernels.cuh"
@@ -180,11 +181,26 @@ __device__ __forceinline__ void cp_async_el(void* smem, const void* gmem, bool p
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// A tile of the launch: blockIdx, or entry blockIdx.x of a list of the tiles that own a node of
+// the domain (y-tile | x-tile << 10 | z-chunk << 20); tiles of void alone are not launched.
+__device__ __forceinline__ void ku_tile(const uint32_t* __restrict__ active, int& ty, int& tx, int& tz) {
+  if (active) {
+    const uint32_t t = active[blockIdx.x];
+    ty = int(t & 1023u);
+    tx = int((t >> 10) & 1023u);
+    tz = int(t >> 20);
+  } else {
+    ty = blockIdx.x;
+    tx = blockIdx.y;
+    tz = blockIdx.z;
+  }
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __restrict__ in, const T* __restrict__ zin,
                                                   T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
-                                                  PcgScalars* sc, RedScratch rs) {
+                                                  PcgScalars* sc, RedScratch rs, const uint32_t* __restrict__ active) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
   __shared__ T se[3][KX + 1][KY + 1];     // ring of 3 element planes
@@ -192,7 +208,9 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   __shared__ T sb[MODE == KU_PLAIN ? 1 : 3][MODE == KU_PLAIN ? 1 : KU_NP];  // staged p_old (PCG mode)
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
-  const int y0 = blockIdx.x * KY, x0 = blockIdx.y * KX, zc0 = blockIdx.z * zc;
+  int tyi, txi, tzi;
+  ku_tile(active, tyi, txi, tzi);
+  const int y0 = tyi * KY, x0 = txi * KX, zc0 = tzi * zc;
   const int zend = min(zc0 + zc, nnz);
   const int ty = threadIdx.x, tx = threadIdx.y;
   const int tid = ty + KY * tx;
@@ -464,20 +482,56 @@ static int ku_z_chunk(int nny, int nnx, int nnz) {
   return best;
 }
 
+// Tile grid of the level-1 K*u launch: y-tiles (a last node row that would fill a tile on its own
+// goes to k_ku_l1_lastrow instead), x-tiles and z-chunks.
+struct KuGeometry {
+  bool lastrow;
+  int rows, zc;
+  dim3 grd;
+};
+static KuGeometry ku_geometry(Grid g) {
+  KuGeometry k;
+  k.lastrow = g.ny >= KY && g.ny % KY == 0;
+  k.rows = k.lastrow ? g.ny : g.nny();
+  k.zc = ku_z_chunk(k.rows, g.nnx(), g.nnz());
+  k.grd = dim3((k.rows + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + k.zc - 1) / k.zc);
+  return k;
+}
+
+std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present) {
+  const KuGeometry k = ku_geometry(g);
+  const int nny = g.nny(), nnx = g.nnx(), nnz = g.nnz();
+  if (k.grd.x > 1024 || k.grd.y > 1024 || k.grd.z > 4095) return {};
+  std::vector<uint32_t> list;
+  for (unsigned tz = 0; tz < k.grd.z; ++tz)
+    for (unsigned tx = 0; tx < k.grd.y; ++tx)
+      for (unsigned ty = 0; ty < k.grd.x; ++ty) {
+        bool any = false;
+        for (int z = int(tz) * k.zc; z < std::min(nnz, int(tz + 1) * k.zc) && !any; ++z)
+          for (int x = int(tx) * KX; x < std::min(nnx, int(tx + 1) * KX) && !any; ++x)
+            for (int y = int(ty) * KY; y < std::min(k.rows, int(ty + 1) * KY) && !any; ++y)
+              any = present[size_t(y + int64_t(nny) * (x + int64_t(nnx) * z))] != 0;
+        if (any) list.push_back(ty | (tx << 10) | (tz << 20));
+      }
+  return list;
+}
+
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
-               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs) {
-  // y-tiles of the tile kernel; a last node row that would fill a tile on its own goes to
-  // k_ku_l1_lastrow instead
-  const bool lastrow = g.ny >= KY && g.ny % KY == 0;
-  const int rows = lastrow ? g.ny : g.nny();
-  const int zc = ku_z_chunk(rows, g.nnx(), g.nnz());
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles) {
+  const KuGeometry k = ku_geometry(g);
+  const bool lastrow = k.lastrow;
+  const int zc = k.zc;
   dim3 blk(KY, KX, 1);
-  dim3 grd((rows + KY - 1) / KY, (g.nnx() + KX - 1) / KX, (g.nnz() + zc - 1) / zc);
-  if (mode == KU_PLAIN)
-    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+  dim3 grd = tiles.list ? dim3(unsigned(tiles.n)) : k.grd;
+  if (tiles.list && tiles.n == 0) grd = dim3(0);
+  if (grd.x == 0) {
+  } else if (mode == KU_PLAIN)
+    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs, tiles.list),
+     topx::count_launch());
   else
-    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs), topx::count_launch());
+    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs, tiles.list),
+     topx::count_launch());
   if (lastrow) {
     const dim3 nb((g.nnx() + KLX - 1) / KLX, (g.nnz() + KLZ - 1) / KLZ);
     if (mode == KU_PLAIN)
@@ -1036,7 +1090,7 @@ void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int3
 // explicit instantiations
 #define TOPX_INST(T)                                                                                             \
   template void launch_ku<T>(cudaStream_t, KuMode, Grid, const T*, const T*, T*, T*, const T*, const uint8_t*,   \
-                             const T*, PcgScalars*, RedScratch);                                                 \
+                             const T*, PcgScalars*, RedScratch, KuTiles);                                        \
   template void launch_diag_l1<T, T>(cudaStream_t, Grid, const T*, const uint8_t*, const T*, const uint8_t*, T*); \
   template void launch_residual_init<T>(cudaStream_t, Grid, const T*, const T*, T*, PcgScalars*, RedScratch,     \
                                         double, int);                                                            \

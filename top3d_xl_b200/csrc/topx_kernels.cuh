@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <stdexcept>
 #include <string>
 
@@ -42,9 +43,16 @@ enum KuMode { KU_PLAIN = 0, KU_P_UPDATE = 2 };
 void upload_ke(const double* Ke576);
 
 // --- level-1 elasticity --------------------------------------------------
+// Tiles of the level-1 K*u launch that own a node of the domain (ku_active_tiles); a null list
+// launches the whole grid
+struct KuTiles {
+  const uint32_t* list = nullptr;
+  int n = 0;
+};
+std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present);
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
-               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs);
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles = KuTiles{});
 template <typename TE, typename T = TE>
 void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
                     const uint8_t* present, T* d);

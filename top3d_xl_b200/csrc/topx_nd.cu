@@ -554,7 +554,7 @@ int nd_solve_coop_ctas() {
   if (!coop) return 0;
   TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_nd_solve_coop<double, double>, ND_THREADS, 0));
   TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_nd_solve_coop<float, float>, ND_THREADS, 0));
-  per = std::min(std::min(per, per32), 2);
+  per = std::min(std::min(per, per32), 4);
   return per >= 1 ? nsm * per : 0;
 }
 
