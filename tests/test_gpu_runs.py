@@ -138,3 +138,11 @@ def test_config2a_demo_cuboid_global_10_iterations():
     g = np.load(os.path.join(GOLD, "config2a_global_10.npz"))
     cs, hist, x = _run(np.ones((50, 100, 50), bool), "GLOBAL", 0.12, 50, np.sqrt(3), 0.0, 10)
     _check(g, cs, hist, x)
+
+
+def test_config2b_demo_cuboid_local_42_iterations():
+    """The demo size under LOCAL with rHat 6 (TOP3D_XL(true(50,100,50),'LOCAL',0.5,300,sqrt(3),6)):
+    42 iterations, past the beta doubling at loopbeta = 40 (TX:375-379)."""
+    g = np.load(os.path.join(GOLD, "config2b_local_42.npz"))
+    cs, hist, x = _run(np.ones((50, 100, 50), bool), "LOCAL", 0.5, 300, np.sqrt(3), 6.0, 42)
+    _check(g, cs, hist, x)

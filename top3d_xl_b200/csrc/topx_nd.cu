@@ -124,9 +124,35 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_extend(const NDFront* __restr
 // ---------------------------------------------------------------------------
 // sweep step k
 // ---------------------------------------------------------------------------
-// Blocks [0, npiv): pivot of front f: tile (k, k) <- its inverse, also into scratch slot 0.
-// Blocks [npiv, gridDim.x): write-back of step i = k-1 for tile column j: row i takes R_j
-// (j < i) or column i takes -R_j^T (j > i).
+// scratch slot of R_j of step k (R tiles alternate between two sets by the parity of k)
+__device__ __forceinline__ double* nd_rslot(double* scr, const NDFront& d, int k, int j) {
+  return scr + int64_t(d.scr0 + 1 + (k & 1) * d.N + j) * ND_TILE;
+}
+
+// write-back of step i for tile column j: row i takes R_j (j < i), column i takes -R_j^T (j > i)
+__device__ __forceinline__ void nd_finalize_task(const NDFront& d, NDTask tk, double* pool, double* scr, double* s) {
+  const double* R = nd_rslot(scr, d, tk.i, tk.j);
+  if (tk.j < tk.i) {
+    double* D = nd_tile(pool, d, tk.i, tk.j);
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = __ldcg(R + e);
+  } else {
+    double* D = nd_tile(pool, d, tk.j, tk.i);
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) s[(e >> 6) * 65 + (e & 63)] = __ldcg(R + e);  // [64][65]
+    __syncthreads();
+    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = -s[(e & 63) * 65 + (e >> 6)];
+  }
+}
+
+// the inverse of the (symmetric positive definite) tile in acc, into scratch slot 0 and tile A
+__device__ __forceinline__ void nd_pivot_acc(double (&acc)[4][2][2], double* A, double* scr, const NDFront& d,
+                                             double* smem) {
+  double* Pinv = scr + int64_t(d.scr0) * ND_TILE;
+  gf_pivot(acc, nullptr, 0, 0, ND_T, Pinv, *reinterpret_cast<GFPivotSmem*>(smem));
+  gf_for_outputs(acc, [&](int r, int c, double v) { A[r * ND_T + c] = v; });
+}
+
+// Blocks [0, npiv): pivot of step 0 of front f (tile (0, 0) <- its inverse, also into scratch
+// slot 0).  Blocks [npiv, gridDim.x): write-back tasks (the last step of a level).
 __global__ void __launch_bounds__(ND_THREADS) k_nd_pivot(const NDFront* __restrict__ fronts,
                                                          const NDTask* __restrict__ tasks, int npiv,
                                                          double* __restrict__ pool, double* __restrict__ scr) {
@@ -137,36 +163,32 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_pivot(const NDFront* __restri
     double* A = nd_tile(pool, d, tk.i, tk.i);
     double acc[4][2][2];
     gf_for_outputs(acc, [&](int r, int c, double& v) { v = __ldcg(A + r * ND_T + c); });
-    double* Pinv = scr + int64_t(d.scr0) * ND_TILE;
-    gf_pivot(acc, nullptr, 0, 0, ND_T, Pinv, *reinterpret_cast<GFPivotSmem*>(nd_smem));
-    gf_for_outputs(acc, [&](int r, int c, double v) { A[r * ND_T + c] = v; });
+    nd_pivot_acc(acc, A, scr, d, nd_smem);
     return;
   }
-  const double* R = scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE;
-  if (tk.j < tk.i) {
-    double* D = nd_tile(pool, d, tk.i, tk.j);
-    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = __ldcg(R + e);
-  } else {
-    double* D = nd_tile(pool, d, tk.j, tk.i);
-    double* s = nd_smem;  // [64][65]
-    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) s[(e >> 6) * 65 + (e & 63)] = __ldcg(R + e);
-    __syncthreads();
-    for (int e = threadIdx.x; e < ND_TILE; e += ND_THREADS) D[e] = -s[(e & 63) * 65 + (e >> 6)];
-  }
+  nd_finalize_task(d, tk, pool, scr, nd_smem);
 }
 
-// R_j = -P^-1 A[k][j] into scratch slot 1 + j
+// Blocks [0, npan): R_j = -P^-1 A[k][j] of step k into its scratch slot; A[k][k-1] is the column
+// k-1 that step k-1's write-back (blocks [npan, gridDim.x) of the same launch) is storing, so it
+// is taken from step k-1's R_k instead: -R_k^T.
 __global__ void __launch_bounds__(ND_THREADS) k_nd_panel(const NDFront* __restrict__ fronts,
-                                                         const NDTask* __restrict__ tasks, int k,
-                                                         const double* __restrict__ pool, double* __restrict__ scr) {
+                                                         const NDTask* __restrict__ tasks, int npan, int k,
+                                                         double* __restrict__ pool, double* __restrict__ scr) {
   extern __shared__ __align__(16) double nd_smem[];
-  double* bufA = nd_smem;
-  double* bufB = nd_smem + GF_BUF;
   const NDTask tk = tasks[blockIdx.x];
   const NDFront d = fronts[tk.f];
+  if (int(blockIdx.x) >= npan) {
+    nd_finalize_task(d, tk, pool, scr, nd_smem);
+    return;
+  }
+  double* bufA = nd_smem;
+  double* bufB = nd_smem + GF_BUF;
   const double* Pinv = scr + int64_t(d.scr0) * ND_TILE;
   gf_stage_ring(bufA, Pinv, GF_LDA);
-  if (tk.j < k)
+  if (tk.j == k - 1)
+    nd_stage_transposed(bufB, nd_rslot(scr, d, k - 1, k), GF_LD, -1.0);
+  else if (tk.j < k)
     gf_stage_ring(bufB, nd_tile_c(pool, d, k, tk.j), GF_LD);
   else
     nd_stage_transposed(bufB, nd_tile_c(pool, d, tk.j, k), GF_LD, 1.0);
@@ -175,14 +197,15 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_panel(const NDFront* __restri
   double acc[4][2][2];
   gf_for_outputs(acc, [&](int, int, double& v) { v = 0.0; });
   gf_product(bufA, bufB, acc);
-  double* R = scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE;
+  double* R = nd_rslot(scr, d, k, tk.j);
   gf_for_outputs(acc, [&](int r, int c, double v) { R[r * ND_T + c] = -v; });
 }
 
-// A[i][j] += A[i][k] R_j for a stored tile (i >= j)
+// A[i][j] += A[i][k] R_j for a stored tile (i >= j); the CTA of tile (k+1, k+1) then inverts it,
+// the pivot of step k+1
 __global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restrict__ fronts,
                                                           const NDTask* __restrict__ tasks, int k,
-                                                          double* __restrict__ pool, const double* __restrict__ scr) {
+                                                          double* __restrict__ pool, double* __restrict__ scr) {
   extern __shared__ __align__(16) double nd_smem[];
   double* bufA = nd_smem;
   double* bufB = nd_smem + GF_BUF;
@@ -193,7 +216,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restr
     gf_stage_ring(bufA, nd_tile_c(pool, d, tk.i, k), GF_LDA);
   else  // tile column i is swept, k is not: A[i][k] = -A[k][i]^T
     nd_stage_transposed(bufA, nd_tile_c(pool, d, k, tk.i), GF_LDA, -1.0);
-  gf_stage_ring(bufB, scr + int64_t(d.scr0 + 1 + tk.j) * ND_TILE, GF_LD);
+  gf_stage_ring(bufB, nd_rslot(scr, d, k, tk.j), GF_LD);
   double* D = nd_tile(pool, d, tk.i, tk.j);
   gf_stage_ring(bufD, D, GF_LD);
   gf_cp_wait();
@@ -202,6 +225,10 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restr
   gf_for_outputs(acc, [&](int r, int c, double& v) { v = bufD[r * GF_LD + c]; });
   gf_product(bufA, bufB, acc);
   __syncthreads();
+  if (tk.i == k + 1 && tk.j == k + 1 && k + 1 < d.T1) {
+    nd_pivot_acc(acc, D, scr, d, bufA);
+    return;
+  }
   gf_for_outputs(acc, [&](int r, int c, double v) { bufD[r * GF_LD + c] = v; });
   __syncthreads();
   gf_copy_to_ring(D, bufD, GF_LD);
@@ -296,16 +323,21 @@ __device__ __forceinline__ void nd_chunk_cols(const TM* t, const double* x, doub
 // index in its launch or phase), and the last CTA of the output tile to finish (atomic ticket,
 // no waiting) adds the chunks in order.  Returns true (with s the total) in the threads < 64 of
 // the CTA that writes the output.
+__device__ __forceinline__ unsigned nd_ticket(unsigned* p) {
+  // release: the CTA's partial sums (ordered before by the barrier) are visible to whoever
+  // acquires the count; acquire: so are the other chunks' partials to the last CTA
+  unsigned v;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ bool nd_finish(double& s, int64_t ti, int ch, int nch, unsigned* cnt, int64_t id,
                                           double* part, bool* last) {
   if (nch == 1) return threadIdx.x < ND_T;
   if (threadIdx.x < ND_T) part[ti * ND_T + threadIdx.x] = s;
-  __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) *last = atomicAdd(cnt + id, 1u) == unsigned(nch - 1);
+  if (threadIdx.x == 0) *last = nd_ticket(cnt + id) == unsigned(nch - 1);
   __syncthreads();
   if (!*last) return false;
-  __threadfence();
   if (threadIdx.x == 0) cnt[id] = 0u;  // ready for the next launch
   if (threadIdx.x < ND_T) {
     double t = 0.0;
@@ -313,6 +345,10 @@ __device__ __forceinline__ bool nd_finish(double& s, int64_t ti, int ch, int nch
     s = t;
   }
   return threadIdx.x < ND_T;
+}
+
+__device__ __forceinline__ void nd_prefetch_l2(const char* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 struct NDSolveSmem {
@@ -353,6 +389,13 @@ __device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, con
     if (s1 >= 0) v += __ldcg(a.w + s1);
     return v;
   };
+  // the chunk's tiles start on their way to L2 while the right-hand side is gathered
+  for (int e = threadIdx.x; e < nj * (ND_TILE * int(sizeof(TM)) / 128); e += ND_THREADS) {
+    const int t = e / (ND_TILE * int(sizeof(TM)) / 128), off = e % (ND_TILE * int(sizeof(TM)) / 128);
+    const int j = j0 + t;
+    const TM* tile = (i >= d.T1 || j <= i) ? nd_tile_c(a.pool, d, i, j) : nd_tile_c(a.pool, d, j, i);
+    nd_prefetch_l2(reinterpret_cast<const char*>(tile) + 128 * off);
+  }
   __syncthreads();  // the previous task's readers of sm are done
   for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) sm.vec[p] = rhs(d.pos0 + int64_t(ND_T) * j0 + p);
   for (int e = threadIdx.x; e < 8 * ND_T; e += ND_THREADS) sm.red[e >> 6][e & 63] = 0.0;
@@ -387,6 +430,10 @@ __device__ __forceinline__ void nd_backward_task(const NDSolveArgs<T, TM>& a, co
   const int i = tk.i, ch = tk.j, P1 = ND_T * d.T1;
   const int nch = max(1, (d.N - d.T1 + ND_CHUNK - 1) / ND_CHUNK);
   const int j0 = d.T1 + ch * ND_CHUNK, nj = min(ND_CHUNK, d.N - j0);
+  for (int e = threadIdx.x; e < nj * (ND_TILE * int(sizeof(TM)) / 128); e += ND_THREADS) {
+    const int t = e / (ND_TILE * int(sizeof(TM)) / 128), off = e % (ND_TILE * int(sizeof(TM)) / 128);
+    nd_prefetch_l2(reinterpret_cast<const char*>(nd_tile_c(a.pool, d, j0 + t, i)) + 128 * off);
+  }
   __syncthreads();
   for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) {
     const int u = ND_T * (j0 - d.T1) + p;  // update DOF
@@ -483,16 +530,19 @@ void NDDevice::factor(cudaStream_t st, const NDPlan& P, Grid g, const double* Ks
       const int64_t n = L.ext[s + 1] - L.ext[s];
       if (n) (k_nd_extend<<<unsigned(n), ND_THREADS, 0, st>>>(fronts, tasks + L.ext[s], upd_map, pool), topx::count_launch());
     }
-    for (int k = 0; k < L.maxT1; ++k) {
-      const int64_t* s = &L.step[size_t(5) * k];
-      const int64_t npiv = s[1] - s[0], nfin = s[2] - s[1], npan = s[3] - s[2], nupd = s[4] - s[3];
-      (k_nd_pivot<<<unsigned(npiv + nfin), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[0], int(npiv), pool, scr),
+    const int64_t npiv0 = L.piv0[1] - L.piv0[0];
+    if (npiv0)
+      (k_nd_pivot<<<unsigned(npiv0), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + L.piv0[0], int(npiv0), pool, scr),
        topx::count_launch());
-      if (npan)
-        (k_nd_panel<<<unsigned(npan), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[2], k, pool, scr),
+    for (int k = 0; k < L.maxT1; ++k) {
+      const int64_t* s = &L.step[size_t(4) * k];
+      const int64_t npan = s[1] - s[0], nfin = s[2] - s[1], nupd = s[3] - s[2];
+      if (npan + nfin)
+        (k_nd_panel<<<unsigned(npan + nfin), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[0], int(npan), k, pool,
+                                                                             scr),
          topx::count_launch());
       if (nupd)
-        (k_nd_update<<<unsigned(nupd), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[3], k, pool, scr),
+        (k_nd_update<<<unsigned(nupd), ND_THREADS, ND_SMEM_SWEEP, st>>>(fronts, tasks + s[2], k, pool, scr),
          topx::count_launch());
     }
     const int64_t nfin = L.fin_last[1] - L.fin_last[0];

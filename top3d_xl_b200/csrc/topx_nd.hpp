@@ -34,7 +34,8 @@ struct NDFront {
   int N, T1;      // tiles per side; leading tiles of eliminated DOFs
   int n1, n2;     // eliminated and update DOFs
   int parent;     // front index, -1 for a root
-  int scr0;       // first scratch tile (P^-1, then R_0 .. R_{N-1}) while its level is swept
+  int scr0;       // first scratch tile while its level is swept: P^-1, then R_0 .. R_{N-1} of
+                  // even steps and R_0 .. R_{N-1} of odd steps
 };
 
 // A launch task: front f, tile row i, tile column j.
@@ -53,8 +54,11 @@ struct NDLevel {
   std::vector<int> fronts;
   int maxT1 = 0;
   int64_t pos_begin = 0, pos_end = 0;  // positions of its fronts (contiguous)
-  // sweep tasks of step k: pivots [s[5k], s[5k+1]), finalise of step k-1 [s[5k+1], s[5k+2]),
-  // panels [s[5k+2], s[5k+3]), updates [s[5k+3], s[5k+4]); the last step's finalise after
+  // sweep: the pivots of step 0 [piv0[0], piv0[1]); per step k, panels [s[4k], s[4k+1]) with the
+  // write-back of step k-1 [s[4k+1], s[4k+2]) in one launch, then the updates [s[4k+2], s[4k+3])
+  // (the pivot of step k+1 runs inside the update of its diagonal tile); the write-back of the
+  // last step [fin_last[0], fin_last[1])
+  int64_t piv0[2] = {0, 0};
   std::vector<int64_t> step;
   int64_t fin_last[2] = {0, 0};
   // extend-add tasks into this level's fronts, from their children of slot 0 and slot 1

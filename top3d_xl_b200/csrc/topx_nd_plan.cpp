@@ -135,7 +135,7 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
       tiles += tri(d.N);
       pos += int64_t(ND_T) * d.N;
       map += d.n2;
-      scr += d.N + 1;
+      scr += 2 * d.N + 1;
       L.maxT1 = std::max(L.maxT1, d.T1);
       P.max_n1 = std::max(P.max_n1, d.n1);
       P.max_n2 = std::max(P.max_n2, d.n2);
@@ -227,18 +227,11 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
   const double tile_flops = 2.0 * ND_T * ND_T * ND_T;
   for (size_t l = 0; l < P.levels.size(); ++l) {
     NDLevel& L = P.levels[l];
+    L.piv0[0] = int64_t(P.tasks.size());
+    for (int f : L.fronts)
+      if (P.fronts[size_t(f)].T1 > 0) add(f, 0, 0);
+    L.piv0[1] = int64_t(P.tasks.size());
     for (int k = 0; k < L.maxT1; ++k) {
-      L.step.push_back(int64_t(P.tasks.size()));
-      for (int f : L.fronts)
-        if (P.fronts[size_t(f)].T1 > k) add(f, k, k);
-      L.step.push_back(int64_t(P.tasks.size()));
-      if (k > 0)
-        for (int f : L.fronts) {
-          const NDFront& d = P.fronts[size_t(f)];
-          if (d.T1 >= k)
-            for (int j = 0; j < d.N; ++j)
-              if (j != k - 1) add(f, k - 1, j);
-        }
       L.step.push_back(int64_t(P.tasks.size()));
       for (int f : L.fronts) {
         const NDFront& d = P.fronts[size_t(f)];
@@ -249,6 +242,14 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
               P.flops += tile_flops;
             }
       }
+      L.step.push_back(int64_t(P.tasks.size()));
+      if (k > 0)
+        for (int f : L.fronts) {
+          const NDFront& d = P.fronts[size_t(f)];
+          if (d.T1 >= k)
+            for (int j = 0; j < d.N; ++j)
+              if (j != k - 1) add(f, k - 1, j);
+        }
       L.step.push_back(int64_t(P.tasks.size()));
       for (int f : L.fronts) {
         const NDFront& d = P.fronts[size_t(f)];
@@ -334,13 +335,13 @@ void nd_check_plan(const NDPlan& P) {
     if (a.pa < 0 || a.pa + 2 >= d.n1 || a.pb < 0 || a.pb + 2 >= ND_T * d.N) fail("assembly position");
   }
   for (const NDLevel& L : P.levels) {
-    if (int64_t(L.step.size()) != 5 * int64_t(L.maxT1)) fail("step table");
+    if (int64_t(L.step.size()) != 4 * int64_t(L.maxT1)) fail("step table");
     int64_t scr = 0;
     for (int f : L.fronts) {
       const NDFront& d = P.fronts[size_t(f)];
       if (d.pos0 < L.pos_begin || d.pos0 + ND_T * d.N > L.pos_end) fail("level positions");
       if (d.scr0 != scr) fail("scratch offsets");
-      scr += d.N + 1;
+      scr += 2 * d.N + 1;
     }
     if (scr != L.nscr || L.nscr > P.nscr) fail("scratch size");
   }
