@@ -146,3 +146,11 @@ def test_config2b_demo_cuboid_local_42_iterations():
     g = np.load(os.path.join(GOLD, "config2b_local_42.npz"))
     cs, hist, x = _run(np.ones((50, 100, 50), bool), "LOCAL", 0.5, 300, np.sqrt(3), 6.0, 42)
     _check(g, cs, hist, x)
+
+
+def test_config3_large_cuboid_global_2_iterations():
+    """The benchmarked cuboid, TOP3D_XL(true(128,256,128),'GLOBAL',0.12,50,sqrt(3)): 4,194,304
+    elements, cSolid and 2 iterations against the oracle (an oracle iteration takes minutes)."""
+    g = np.load(os.path.join(GOLD, "config3_global_2.npz"))
+    cs, hist, x = _run(np.ones((128, 256, 128), bool), "GLOBAL", 0.12, 50, np.sqrt(3), 0.0, 2)
+    _check(g, cs, hist, x)
