@@ -416,7 +416,14 @@ __device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, con
     for (int q = 0; q < 8; ++q) s += sm.red[q][threadIdx.x];
   if (nd_finish(s, ti, ch, nch, a.cnt, d.pos0 / ND_T + i, a.part, &sm.last)) {
     const int64_t p = d.pos0 + ND_T * i + threadIdx.x;
-    a.w[p] = i < d.T1 ? s : rhs(p) - s;
+    if (i >= d.T1) {
+      a.w[p] = rhs(p) - s;
+    } else if (d.n2 > 0) {
+      a.w[p] = s;
+    } else {  // no update DOFs: x1 = F11^-1 f1 is the solution (no phase on the way down)
+      const int32_t g = a.sep_dof[p];
+      if (g >= 0) a.x[g] = T(s);
+    }
   }
 }
 
@@ -557,19 +564,27 @@ template <typename T, typename TM>
 void NDDevice::solve(cudaStream_t st, const NDPlan& P, const TM* tiles, const T* b, T* x, const PcgScalars* sc) const {
   NDSolveArgs<T, TM> a{fronts, tasks, tiles, b, x, sep_dof, upd_dof, src0, src1, wvec, part, cnt};
   const int nlev = int(P.levels.size());
-  if (coop_ctas > 0 && 2 * nlev <= ND_MAX_PHASES) {
+  if (coop_ctas > 0 && 2 * nlev <= ND_MAX_PHASES && nlev > 0) {
     NDPhases ph{};
+    int64_t most = 1;
     for (int l = nlev - 1; l >= 0; --l) {
-      ph.begin[ph.n] = P.levels[size_t(l)].fwd[0];
-      ph.end[ph.n++] = P.levels[size_t(l)].fwd[1];
+      const NDLevel& L = P.levels[size_t(l)];
+      if (L.fwd[1] == L.fwd[0]) continue;
+      ph.begin[ph.n] = L.fwd[0];
+      ph.end[ph.n++] = L.fwd[1];
+      most = std::max(most, L.fwd[1] - L.fwd[0]);
     }
     ph.nfwd = ph.n;
     for (int l = 0; l < nlev; ++l) {
-      ph.begin[ph.n] = P.levels[size_t(l)].bwd[0];
-      ph.end[ph.n++] = P.levels[size_t(l)].bwd[1];
+      const NDLevel& L = P.levels[size_t(l)];
+      if (L.bwd[1] == L.bwd[0]) continue;
+      ph.begin[ph.n] = L.bwd[0];
+      ph.end[ph.n++] = L.bwd[1];
+      most = std::max(most, L.bwd[1] - L.bwd[0]);
     }
+    // no more CTAs than the largest phase has tasks: fewer arrivals at each barrier
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(unsigned(coop_ctas));
+    cfg.gridDim = dim3(unsigned(std::min<int64_t>(coop_ctas, most)));
     cfg.blockDim = dim3(ND_THREADS);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;

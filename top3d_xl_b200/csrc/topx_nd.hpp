@@ -23,6 +23,7 @@ namespace topx {
 
 constexpr int ND_T = 64;      // tile width
 constexpr int ND_CHUNK = 4;   // tiles a solve CTA streams for one output tile (more: several CTAs)
+constexpr int64_t kNdOneFrontNodes = 320;  // coarsest grids with at most this many nodes: one front
 
 // One front of the elimination tree (device descriptor).  Positions 0 .. n1-1 are the
 // eliminated DOFs (3 per separator node, in node order), n1 .. 64 T1 - 1 padding (identity),

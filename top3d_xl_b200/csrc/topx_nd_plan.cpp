@@ -103,7 +103,11 @@ inline int64_t tri(int64_t i) { return i * (i + 1) / 2; }
 NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint8_t>& present, int leaf_nodes) {
   if (int64_t(present.size()) != int64_t(nny) * nnx * nnz) throw std::invalid_argument("nd_plan: present size");
   if (stride * 3 > int64_t(INT32_MAX)) throw std::invalid_argument("nd_plan: grid too large");
-  Builder B(nny, nnx, nnz, present, std::max(8, leaf_nodes));
+  // a small grid is one front: its solve is then a single GEMV with no dependent phases
+  int64_t npresent = 0;
+  for (uint8_t v : present) npresent += v ? 1 : 0;
+  const int64_t leaf = npresent <= kNdOneFrontNodes ? int64_t(nny) * nnx * nnz : std::max(8, leaf_nodes);
+  Builder B(nny, nnx, nnz, present, int(std::min<int64_t>(leaf, INT32_MAX)));
   Box all{{0, 0, 0}, {nny, nnx, nnz}};
   B.build(all, -1, 0, 0);
   NDPlan P;
@@ -291,10 +295,11 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
         for (int ch = 0; ch < chunks(d.T1); ++ch) add(f, i, ch);
     }
     L.fwd[1] = L.bwd[0] = int64_t(P.tasks.size());
-    for (int f : L.fronts) {
+    for (int f : L.fronts) {  // a front without update DOFs writes its solution going up
       const NDFront& d = P.fronts[size_t(f)];
-      for (int i = 0; i < d.T1; ++i)
-        for (int ch = 0; ch < chunks(d.N - d.T1); ++ch) add(f, i, ch);
+      if (d.n2 > 0)
+        for (int i = 0; i < d.T1; ++i)
+          for (int ch = 0; ch < chunks(d.N - d.T1); ++ch) add(f, i, ch);
     }
     L.bwd[1] = int64_t(P.tasks.size());
     P.nsolve_tasks = std::max(P.nsolve_tasks, std::max(L.fwd[1] - L.fwd[0], L.bwd[1] - L.bwd[0]));
