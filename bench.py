@@ -219,6 +219,25 @@ def run_e2e(wl, precision, steps, warmup, device):
     return dict(value=steps / wall, h2d=8 * ne, d2h=8 * ne)
 
 
+def profile_one_step(wl, precision, device, coop=True):
+    """One warm-up OC iteration, then one OC iteration bracketed by cudaProfilerStart/Stop, so that
+    `ncu --profile-from-start off` captures exactly the kernels of one iteration."""
+    import ctypes
+    from top3d_xl_b200 import Context
+    rt = ctypes.CDLL("libcudart.so")
+    with Context(precision, device=device, **({} if coop else dict(coarse_coop=0))) as ctx:
+        load_workload(ctx, wl)
+        ctx.begin(wl["cons"], wl["V0"], wl["nLoop"], wl["rMin"], wl["rHat"])
+        ctx.step()
+        rt.cudaDeviceSynchronize()
+        rt.cudaProfilerStart()
+        r = ctx.step()
+        rt.cudaDeviceSynchronize()
+        rt.cudaProfilerStop()
+    print(json.dumps({"profiled_step": r["loop"], "pcg_its": r["its"], "c": r["c"]}), flush=True)
+    return 0
+
+
 def cpu_sample(wl, its_per_oc, filter_its_per_oc, budget_s=30.0):
     """Time the FP64 oracle (CPU restatement of TOP3D_XL.m) on a bounded sample of the
     workload and extrapolate one OC iteration from the GPU's measured iteration counts."""
@@ -394,6 +413,11 @@ def main(argv=None):
                     help="reference arm: time spent on timed whole OC iterations (at least one runs)")
     ap.add_argument("--mixed", choices=["mixed", "mixed32"], default="mixed",
                     help="precision of the mixed arm: FP32 preconditioner (mixed), also FP32 filter (mixed32)")
+    ap.add_argument("--profile-one-step", action="store_true",
+                    help="profiling pass: one warm-up OC iteration, then one OC iteration between "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); prints its PCG counts")
+    ap.add_argument("--coarse-levels", action="store_true",
+                    help="with --profile-one-step: run the coarsest solve level by level, not as one persistent launch")
     ap.add_argument("--only", choices=["mixed", "mixed32", "fp64"], default=None,
                     help="run one precision arm only (profiling); prints its timing and exits")
     a = ap.parse_args(argv)
@@ -457,6 +481,8 @@ def main(argv=None):
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
         return 0
+    if a.profile_one_step:
+        return profile_one_step(wl, a.only or "fp64", device, coop=not a.coarse_levels)
     if a.only:
         r = run_native(wl, a.only, a.steps, a.warmup, device, profile_steps=1)
         print(json.dumps({"only": a.only, "ms_per_step": r["ms"] / max(1, a.steps),

@@ -194,7 +194,9 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     const Level& Lc = M.levels[nl - 1];
     std::vector<uint8_t> pc(size_t(g.nnodes()), 0);
     for (auto k : Lc.nodMapBack) pc[k - 1] = 1;
-    nd = nd_plan(g.nny(), g.nnx(), g.nnz(), g.stride, pc);
+    int64_t npc = 0;
+    for (uint8_t v : pc) npc += v;
+    nd = nd_plan(g.nny(), g.nnx(), g.nnz(), g.stride, pc, nd_leaf_nodes(npc));
     ndFronts.upload(nd.fronts.data(), nd.fronts.size());
     ndTasks.upload(nd.tasks.data(), nd.tasks.size());
     ndAsm.upload(nd.asmb.data(), nd.asmb.size());

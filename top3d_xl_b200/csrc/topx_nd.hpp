@@ -24,6 +24,8 @@ namespace topx {
 constexpr int ND_T = 64;      // tile width
 constexpr int ND_CHUNK = 4;   // tiles a solve CTA streams for one output tile (more: several CTAs)
 constexpr int64_t kNdOneFrontNodes = 320;  // coarsest grids with at most this many nodes: one front
+constexpr int64_t ND_MEDIUM_NODES = 2048;  // grids up to this size: leaves of ND_MEDIUM_LEAF nodes
+constexpr int ND_MEDIUM_LEAF = 256, ND_LEAF = 128;
 
 // One front of the elimination tree (device descriptor).  Positions 0 .. n1-1 are the
 // eliminated DOFs (3 per separator node, in node order), n1 .. 64 T1 - 1 padding (identity),
@@ -94,6 +96,10 @@ struct NDPlan {
 // the SoA DOF vectors (component c of node n at n + c * stride).  Leaf boxes hold at most
 // `leaf_nodes` grid nodes.
 NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint8_t>& present, int leaf_nodes = 64);
+
+// Leaf size of the tree for a coarsest grid of `present` nodes: each tree level costs the solve a
+// dependent phase, each larger leaf the factorisation its cube; medium grids take fewer levels.
+inline int nd_leaf_nodes(int64_t present) { return present <= ND_MEDIUM_NODES ? ND_MEDIUM_LEAF : ND_LEAF; }
 
 // Consistency checks of a plan (positions, maps, task ranges); throws on the first violation.
 void nd_check_plan(const NDPlan& p);
