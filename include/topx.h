@@ -215,12 +215,12 @@ topx_status topx_set_density(topx_ctx* ctx, const double* xPhys, size_t ne);
 topx_status topx_get_displacement(topx_ctx* ctx, int lc, double* out, size_t ndof);
 
 /* ---- failure handling (no reference counterpart) ----------------------------- */
-/* Test of the give-up path of the one bounded wait in the library's kernels, the grid barrier of
-   the persistent coarsest-level solve (contexts with topx_params.coarse_coop = 1).  which must be
-   0: a two-CTA grid whose second CTA leaves without arriving, so the first one's wait exhausts
-   its poll limit (about a second) and sets the barrier's error word.  Returns TOPX_ERR_TIMEOUT
-   with a message naming the wait, as a real give-up inside a solve would; the context stays
-   usable. */
+/* Test of the give-up path of the one bounded wait in the library's kernels: in the persistent
+   coarsest-level solve (contexts with topx_params.coarse_coop = 1) a task waits for the tasks of
+   the fronts it reads.  which must be 0: one CTA waits for a counter that nothing raises, so its
+   wait exhausts its poll limit (about a second) and sets the solve's error word.  Returns
+   TOPX_ERR_TIMEOUT with a message naming the wait, as a real give-up inside a solve would; the
+   context stays usable. */
 topx_status topx_selftest_wait(topx_ctx* ctx, int which);
 
 /* ---- measurement (no reference counterpart) --------------------------------- */

@@ -2,9 +2,9 @@
 
 Sizes are chosen so the FP64 oracle finishes in seconds.  Tolerances: the
 native path computes the same FP64 arithmetic in a different summation order
-(node-centric gathers instead of accumarray scatters, slab LDL^T instead of a
-permuted sparse Cholesky), so single operators agree to ~1e-13 relative and
-iterative solves to ~1e-9.
+(node-centric gathers instead of accumarray scatters, a nested-dissection
+factorisation instead of a permuted sparse Cholesky), so single operators agree
+to ~1e-13 relative and iterative solves to ~1e-9.
 """
 import numpy as np
 import pytest
@@ -134,8 +134,8 @@ def test_filter_preserves_constants(setup):
 
 @pytest.mark.parametrize("shape", [(64, 96, 64), (112, 136, 112)])
 def test_vcycle_with_large_coarsest_slabs(shape):
-    # coarsest slabs of m = 243 (4 pivot blocks, the last one 51 wide) and m = 675 (11 blocks,
-    # the last one 35 wide): the Gauss-Jordan inverses run many tile tasks, both chains at once
+    # coarsest grids of 9 x 13 x 9 and 15 x 18 x 15 nodes: elimination trees of several levels,
+    # fronts of several 64-wide tiles (Gauss-Jordan steps over many tile tasks)
     from top3d_xl_b200 import Context
     vox = np.ones(shape, bool)
     m = O.build_model(vox)
@@ -154,6 +154,37 @@ def test_vcycle_with_large_coarsest_slabs(shape):
         ctx.assemble()  # a second factorisation through the same scratch and control words
         r = np.random.default_rng(6).standard_normal(m.levels[0].numDOFs)
         assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
+
+
+@pytest.mark.parametrize("kind", ["cuboid", "irregular"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_coarse_solve_matches_level_launches(kind, precision):
+    # the coarsest solve as one dataflow launch (tasks wait for their children's or parent's
+    # counters) and as one launch per tree level run the same tasks with the same summation
+    # order: the V-cycles agree bit for bit, over repeated solves (the counters are re-armed by
+    # each launch) and after a second factorisation
+    from top3d_xl_b200 import Context
+    if kind == "cuboid":
+        vox = np.ones((64, 128, 64), bool)
+    else:
+        vox = np.random.default_rng(12).random((64, 128, 64)) < 0.8
+        vox[:, 0, :] = True
+        vox[:, -1, :] = True
+    E = 1.0 + np.random.default_rng(11).uniform(0.0, 1.0, int(vox.sum())) ** 3
+    outs = []
+    for coop in (1, 0):
+        with Context(precision, coarse_coop=coop) as ctx:
+            ctx.load_voxels(vox)
+            ctx.set_moduli(E)
+            ctx.assemble()
+            res = []
+            for k, seed in enumerate((21, 22, 23)):
+                if k == 2:
+                    ctx.assemble()
+                res.append(ctx.vcycle(np.random.default_rng(seed).standard_normal(ctx.numDOFs)))
+            outs.append(res)
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("kind", ["cuboid", "irregular"])

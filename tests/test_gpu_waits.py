@@ -1,13 +1,13 @@
-"""Give-up path of the one bounded wait in the kernels, on the GPU, through the C ABI.
+"""Give-up path of the bounded wait in the kernels, on the GPU, through the C ABI.
 
-The coarsest-level solve of an engine alone on the GPU runs as one persistent launch whose tree
-levels are separated by a grid barrier.  The barrier's wait has a poll limit (about a second),
-after which it sets an error word and every CTA returns; the host reads the word after the
-stream synchronises, clears it and raises TOPX_ERR_TIMEOUT.  topx_selftest_wait runs the barrier
-in a two-CTA grid whose second CTA leaves without arriving (no kernel faults, traps or spins
-without a limit), so the limit must run out.  The test then checks the status and message, and
-that the same context still computes the V-cycle and the PCG solve exactly as before and as the
-oracle does.
+The coarsest-level solve of an engine alone on the GPU runs as one persistent dataflow launch:
+a task waits for the tasks of the fronts it reads.  The wait has a poll limit (about a second),
+after which it sets an error word and the CTAs waiting after it return; the host reads the word
+after the stream synchronises, clears it (with the solve's counters) and raises
+TOPX_ERR_TIMEOUT.  topx_selftest_wait has one CTA wait for a counter that nothing raises (no
+kernel faults, traps or spins without a limit), so the limit must run out.  The test then checks
+the status and message, and that the same context still computes the V-cycle and the PCG solve
+exactly as before and as the oracle does.
 """
 import numpy as np
 import pytest
@@ -41,11 +41,11 @@ def setup():
     ctx.close()
 
 
-def test_barrier_wait_gives_up_and_context_stays_usable(setup):
+def test_wait_gives_up_and_context_stays_usable(setup):
     ctx = setup["ctx"]
     st = ctx.lib.topx_selftest_wait(ctx._h, 0)
     assert st == TOPX_ERR_TIMEOUT, (st, ctx.lib.topx_last_error(ctx._h))
-    assert b"grid barrier" in ctx.lib.topx_last_error(ctx._h)
+    assert b"dependency wait" in ctx.lib.topx_last_error(ctx._h)
     # the error word was cleared: the factorisation, the persistent solve and the PCG run as before
     ctx.assemble()
     z = ctx.vcycle(setup["r"])
@@ -58,5 +58,5 @@ def test_barrier_wait_gives_up_and_context_stays_usable(setup):
 
 def test_other_selftest_cases_are_refused(setup):
     ctx = setup["ctx"]
-    for which in (1, 7):
+    for which in (1, 7, -1):
         assert ctx.lib.topx_selftest_wait(ctx._h, which) == -1  # TOPX_ERR_ARG

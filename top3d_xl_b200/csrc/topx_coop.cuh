@@ -1,13 +1,13 @@
-// Grid-wide barrier with a bounded wait, for persistent launches whose CTAs are all resident
-// (cooperative launch).  No kernel spins without a limit: a wait that runs out sets the error
-// word, every CTA then leaves at its next barrier, and the host reads and clears the word.
+// Bounded waits of persistent launches whose CTAs are all resident (cooperative launch).  No
+// kernel spins without a limit: a wait that runs out sets the error word, the CTAs waiting after
+// it give up too, and the host reads and clears the word.
 #pragma once
 
 #include "topx_kernels.cuh"
 
 namespace topx {
 
-// polls of the barrier word before a CTA gives up (about a second in all)
+// polls of a counter before a CTA gives up (about a second in all)
 constexpr unsigned kCoopSpinLimit = 1u << 20;
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
@@ -17,46 +17,21 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 }
 __device__ __forceinline__ int ld_volatile_int(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
-// bar->count only grows within a launch: barrier number i (1, 2, ...) is passed once it reaches
-// i * gridDim.x, so an arrival is one fire-and-forget release add and the wait polls that single
-// word (no reset round trip).  The last CTA to leave the kernel (coop_exit) zeroes the words for
-// the next launch.  Returns false in every thread of the CTA once any CTA has given up; the
-// kernel then returns, so it always ends.
-__device__ __forceinline__ bool coop_barrier(CoopBarrier* bar, unsigned& epoch) {
-  __shared__ int s_ok;
-  __syncthreads();
-  ++epoch;
-  if (threadIdx.x == 0) {
-    int ok = ld_volatile_int(&bar->err) == 0;
-    if (ok) {
-      const unsigned target = epoch * gridDim.x;
-      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&bar->count) : "memory");
-      unsigned it = 0;
-      while (ld_acquire_gpu(&bar->count) < target) {
-        if (++it > kCoopSpinLimit || ld_volatile_int(&bar->err)) {
-          atomicCAS(&bar->err, 0, kCoopErrBarrier);
-          ok = 0;
-          break;
-        }
-      }
+// Thread 0 of a CTA waits until the counter *p has reached `need` (counters only grow within a
+// launch; producers add with release semantics, the poll loads with acquire).  Gives up after
+// kCoopSpinLimit polls, or soon after another CTA gave up, with ctl->err set to kCoopErrWait.
+__device__ __forceinline__ bool coop_wait_count(const unsigned* p, unsigned need, CoopControl* ctl) {
+  unsigned it = 0;
+  while (ld_acquire_gpu(p) < need) {
+    if ((++it & 31u) == 0u && (it > kCoopSpinLimit || ld_volatile_int(&ctl->err))) {
+      atomicCAS(&ctl->err, 0, kCoopErrWait);
+      return false;
     }
-    s_ok = ok;
   }
-  __syncthreads();
-  return s_ok != 0;
+  return true;
 }
-
-// Called once by every CTA on every exit path after its first barrier: the last one out
-// re-arms the barrier words (all other CTAs have left their waits by then).
-__device__ __forceinline__ void coop_exit(CoopBarrier* bar) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&bar->gen, 1u) == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      atomicExch(&bar->gen, 0u);
-    }
-  }
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 }  // namespace topx

@@ -210,7 +210,7 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     ndPool.alloc(size_t(nd.ntiles) * tile, false);
     ndScr.alloc(size_t(nd.nscr) * tile, false);
     ndW.alloc(size_t(nd.npos));
-    ndPart.alloc(size_t(nd.nsolve_tasks) * ND_T, false);
+    ndPart.alloc(size_t(std::max<int64_t>(nd.nsolve_tasks, int64_t(nd.flow.size()))) * ND_T, false);
     ndCnt.alloc(size_t(nd.npos / ND_T));
     if (pre32()) ndPool32.alloc(size_t(nd.ntiles) * tile, false);
     ndd.fronts = ndFronts.p;
@@ -227,13 +227,19 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     ndd.wvec = ndW.p;
     ndd.part = ndPart.p;
     ndd.cnt = ndCnt.p;
-    coopBar.alloc(1);
+    coopCtl.alloc(1);
     // an engine alone on the GPU runs the solve as one persistent launch; engines sharing the
     // GPU (the job server) launch it level by level, since a persistent launch needs all its CTAs
     // resident at once
     coopCtas = coarse_coop ? nd_solve_coop_ctas() : 0;
     ndd.coop_ctas = coopCtas;
-    ndd.bar = coopBar.p;
+    ndd.ctl = coopCtl.p;
+    if (coopCtas) {
+      ndFlow.upload(nd.flow.data(), nd.flow.size());
+      ndDone.alloc(2 * nd.fronts.size());
+      ndd.flow = ndFlow.p;
+      ndd.flow_done = ndDone.p;
+    }
   }
   // ---- workspaces ------------------------------------------------------------
   {
@@ -269,8 +275,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   mmaS.alloc(1);
   dscal.alloc(16);
   TOPX_CUDA_OK(cudaMallocHost(&h_sc, sizeof(PcgScalars)));
-  TOPX_CUDA_OK(cudaMallocHost(&h_bar, sizeof(CoopBarrier)));
-  h_bar->err = 0;
+  TOPX_CUDA_OK(cudaMallocHost(&h_ctl, sizeof(CoopControl)));
+  h_ctl->err = 0;
   // ---- optimiser state -------------------------------------------------------
   for (DevBuf<double>* b : {&x, &xPhys, &dc, &ce, &tmpA, &tmpB, &xTilde, &xhat, &dfdx, &dxv, &volMax})
     b->alloc(size_t(Ne));
@@ -320,7 +326,7 @@ Engine::~Engine() {
     if (e) cudaEventDestroy(e);
   if (ev_legacy) cudaEventDestroy(ev_legacy);
   if (h_sc) cudaFreeHost(h_sc);
-  if (h_bar) cudaFreeHost(h_bar);
+  if (h_ctl) cudaFreeHost(h_ctl);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -355,40 +361,45 @@ void Engine::alloc_fwork(FWork<TF>& f) {
 
 void Engine::read_scalars(PcgScalars& h, const PcgScalars* d) const {
   TOPX_CUDA_OK(cudaMemcpyAsync(h_sc, d, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_ctl, coopCtl.p, sizeof(CoopControl), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   h = *h_sc;
   check_device_waits();
 }
 
-void Engine::check_coop_barrier() {
-  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_bar, coopBar.p, sizeof(CoopBarrier), cudaMemcpyDeviceToHost, st));
+void Engine::check_coop_waits() {
+  if (coopCtas) TOPX_CUDA_OK(cudaMemcpyAsync(h_ctl, coopCtl.p, sizeof(CoopControl), cudaMemcpyDeviceToHost, st));
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
   check_device_waits();
 }
 
-// The persistent coarse solve's grid barrier sets an error word instead of spinning on (its wait
-// is bounded); the word was copied into pinned memory before the caller's stream sync.  A word
+// The persistent coarse solve's dependency waits set an error word instead of spinning on (they
+// are bounded); the word was copied into pinned memory before the caller's stream sync.  A word
 // that is set is cleared (so the engine stays usable) and reported.
 void Engine::check_device_waits() const {
-  if (coopCtas && h_bar->err) {
-    h_bar->err = 0;
-    TOPX_CUDA_OK(cudaMemset(coopBar.p, 0, sizeof(CoopBarrier)));
-    throw DeviceWaitError("coarse solve: a grid barrier wait gave up (persistent launch not co-resident)");
+  if (coopCtas && h_ctl->err) {
+    const int err = h_ctl->err;
+    h_ctl->err = 0;
+    // a launch that gave up may leave chunk tickets and dependency counts behind
+    TOPX_CUDA_OK(cudaMemset(coopCtl.p, 0, sizeof(CoopControl)));
+    TOPX_CUDA_OK(cudaMemset(ndCnt.p, 0, sizeof(unsigned) * ndCnt.n));
+    if (ndDone.p) TOPX_CUDA_OK(cudaMemset(ndDone.p, 0, sizeof(unsigned) * ndDone.n));
+    throw DeviceWaitError(err == kCoopErrWait ? "coarse solve: a dependency wait gave up (persistent launch not co-resident)"
+                                              : "coarse solve: unknown wait error");
   }
 }
 
-// Drives the grid barrier's bounded wait to its poll limit: a two-CTA grid whose second CTA
-// leaves without arriving.  The wait gives up within about a second and the check below throws
-// DeviceWaitError after clearing the error word.
+// Drives the persistent coarse solve's bounded dependency wait to its poll limit: one CTA waits
+// for a counter that nothing raises.  The wait gives up within about a second and the check below
+// throws DeviceWaitError after clearing the words.
 void Engine::selftest_wait(int which) {
-  if (which != 0) throw std::invalid_argument("selftest_wait: which must be 0 (the coarse solve's grid barrier)");
+  if (which != 0) throw std::invalid_argument("selftest_wait: which must be 0 (the coarse solve's dependency wait)");
   if (!coopCtas)
     throw std::invalid_argument("selftest_wait: this context runs the coarse solve without a persistent launch");
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemsetAsync(coopBar.p, 0, sizeof(CoopBarrier), st));
-  launch_coop_barrier_selftest(st, coopBar.p);
-  check_coop_barrier();
+  TOPX_CUDA_OK(cudaMemsetAsync(coopCtl.p, 0, sizeof(CoopControl), st));
+  launch_coop_wait_selftest(st, coopCtl.p);
+  check_coop_waits();
 }
 
 // ---------------------------------------------------------------------------
@@ -708,7 +719,7 @@ void Engine::apply_vcycle(const double* h_r, double* h_z) {
   launch_compact_to_grid_nodes<double>(st, cu.p, kw.r.p, G[0], nodMapBack0.p, Nn);
   vcycle(true, scE.p);
   launch_grid_to_compact_nodes<double>(st, kw.z.p, cu.p, G[0], nodMapBack0.p, Nn);
-  check_coop_barrier();
+  check_coop_waits();
   TOPX_CUDA_OK(cudaMemcpy(h_z, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
 }
 

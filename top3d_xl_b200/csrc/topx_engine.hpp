@@ -217,10 +217,12 @@ class Engine {
   DevBuf<int32_t> ndMap, ndSep, ndUpd, ndSrc0, ndSrc1;
   DevBuf<double> ndPool, ndScr, ndW, ndPart;
   DevBuf<unsigned> ndCnt;
+  DevBuf<NDTask> ndFlow;   // the solve tasks in dependency order (persistent dataflow solve)
+  DevBuf<unsigned> ndDone; // its per-front counters
   DevBuf<float> ndPool32;  // FP32 copy applied by the mixed-precision V-cycle
-  DevBuf<CoopBarrier> coopBar;  // grid barrier of the persistent coarse solve
+  DevBuf<CoopControl> coopCtl;  // control words of the persistent coarse solve
   int coopCtas = 0;             // its CTA count; 0: one launch per tree level and direction
-  void check_coop_barrier();    // waits for the stream; throws if a barrier wait gave up (re-arming it)
+  void check_coop_waits();      // waits for the stream; throws if a wait gave up (re-arming the words)
   void check_device_waits() const;  // after a stream sync: throws if a bounded device wait gave up
   // workspaces
   KrylovWork kw;
@@ -239,7 +241,7 @@ class Engine {
   DevBuf<MmaState> mmaS;
   DevBuf<double> dscal;
   PcgScalars* h_sc = nullptr;  // pinned
-  CoopBarrier* h_bar = nullptr;  // pinned
+  CoopControl* h_ctl = nullptr;  // pinned
   // optimiser state (compact, FP64)
   DevBuf<double> x, xPhys, dc, ce, tmpA, tmpB, xTilde, xhat, dfdx, dxv, volMax;
   DevBuf<double> xold1, xold2, low, upp, alpha, beta, p0, q0, pij, qij, xmma, xmin, xmax;

@@ -117,17 +117,17 @@ void launch_diag_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t
 // caches the SM count used to shape the K*u launch (call once per device, outside capture)
 void prepare_fem_kernels();
 
-// State of the grid-wide barrier of the persistent coarse solve (zeroed before first use;
-// err != 0 after a CTA gave up waiting, and then the words must be zeroed again).
-struct CoopBarrier {
-  unsigned count;
-  unsigned gen;
-  int err;  // 0, or kCoopErrBarrier once a barrier wait gave up
+// Control words of the persistent coarse solve (zeroed before first use; err != 0 after a CTA
+// gave up waiting, and then the words, and the solve's counters, must be zeroed again).
+struct CoopControl {
+  unsigned idle;   // a counter that nothing raises (the wait self-test); zero
+  unsigned exits;  // CTAs that left the launch (the last one re-arms the counters); zero between launches
+  int err;         // 0, or kCoopErrWait once a wait gave up
   int pad;
 };
-constexpr int kCoopErrBarrier = 1;  // a grid barrier wait gave up
-// Self-test of the barrier's bounded wait: a two-CTA grid whose second CTA leaves without
-// arriving, so the first CTA's wait runs into its poll limit (about a second) and sets bar->err.
-void launch_coop_barrier_selftest(cudaStream_t st, CoopBarrier* bar);
+constexpr int kCoopErrWait = 1;  // a wait for another CTA's tasks (dataflow solve) gave up
+// Self-test of the dataflow solve's bounded dependency wait: one CTA waits for a counter that
+// nothing raises, gives up within about a second and sets ctl->err to kCoopErrWait.
+void launch_coop_wait_selftest(cudaStream_t st, CoopControl* ctl);
 
 }  // namespace topx

@@ -351,10 +351,20 @@ __device__ __forceinline__ void nd_prefetch_l2(const char* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+static_assert(ND_CHUNK * ND_T <= ND_THREADS, "a solve task gathers one input entry per thread");
 struct NDSolveSmem {
   double vec[ND_CHUNK * ND_T];  // the chunk's input entries
   double red[8][ND_T];
   bool last;
+  int ok;  // dataflow launch: the task's inputs are complete (0: a wait gave up)
+};
+
+// Dataflow launch: per front, output tiles completed by its children on the way up, and output
+// tiles of its own solution (zero between launches)
+struct NDFlow {
+  unsigned* fwd_done;
+  unsigned* bwd_done;
+  CoopControl* ctl;  // error word and exit count
 };
 
 template <typename T, typename TM>
@@ -374,21 +384,13 @@ struct NDSolveArgs {
 // tree.  i < T1: w = F11^-1 f1; i >= T1: w = f2 - X f1, where f1 is the eliminated part of the
 // front's right-hand side (b at its DOFs plus what its children's updates put there) and f2
 // what the children's updates put on the update DOFs.
-template <typename T, typename TM>
-__device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
-                                                NDSolveSmem& sm) {
+template <typename T, typename TM, bool FLOW>
+__device__ __forceinline__ bool nd_forward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
+                                                NDSolveSmem& sm, const NDFlow* fl) {
   const NDFront d = a.fronts[tk.f];
   const int i = tk.i, ch = tk.j;
   const int nch = max(1, (d.T1 + ND_CHUNK - 1) / ND_CHUNK);
   const int j0 = ch * ND_CHUNK, nj = min(ND_CHUNK, d.T1 - j0);
-  auto rhs = [&](int64_t p) {
-    const int32_t g = a.sep_dof[p], s0 = a.src0[p], s1 = a.src1[p];
-    // values written by other CTAs earlier in a persistent launch: loads bypass L1
-    double v = g >= 0 ? double(a.b[g]) : 0.0;
-    if (s0 >= 0) v += __ldcg(a.w + s0);
-    if (s1 >= 0) v += __ldcg(a.w + s1);
-    return v;
-  };
   // the chunk's tiles start on their way to L2 while the right-hand side is gathered
   for (int e = threadIdx.x; e < nj * (ND_TILE * int(sizeof(TM)) / 128); e += ND_THREADS) {
     const int t = e / (ND_TILE * int(sizeof(TM)) / 128), off = e % (ND_TILE * int(sizeof(TM)) / 128);
@@ -396,8 +398,40 @@ __device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, con
     const TM* tile = (i >= d.T1 || j <= i) ? nd_tile_c(a.pool, d, i, j) : nd_tile_c(a.pool, d, j, i);
     nd_prefetch_l2(reinterpret_cast<const char*>(tile) + 128 * off);
   }
+  // Right-hand side at position p: b at its grid DOF (eliminated DOFs) plus the children's
+  // update entries that land there.  The indices and b come before the wait, the children's
+  // entries (written by other CTAs of the launch: loads bypass L1) after it.  Thread k gathers
+  // input entry k of the chunk; threads < 64 also the entry at their output position.
+  const bool has_in = threadIdx.x < nj * ND_T;
+  const int64_t pin = d.pos0 + int64_t(ND_T) * j0 + threadIdx.x;
+  const int64_t pout = d.pos0 + int64_t(ND_T) * i + threadIdx.x;
+  int32_t s0 = -1, s1 = -1, o0 = -1, o1 = -1, og = -1;
+  double v = 0.0, ov = 0.0;
+  if (has_in) {
+    const int32_t g = a.sep_dof[pin];
+    s0 = a.src0[pin];
+    s1 = a.src1[pin];
+    if (g >= 0) v = double(a.b[g]);
+  }
+  if (threadIdx.x < ND_T) {
+    og = a.sep_dof[pout];
+    if (i >= d.T1) {  // an update position: no grid DOF of this front, so no b
+      o0 = a.src0[pout];
+      o1 = a.src1[pout];
+    }
+  }
+  // dataflow: the children's update vectors (all their output tiles) are complete
+  if (FLOW && threadIdx.x == 0)
+    sm.ok = d.fwd_need == 0 || coop_wait_count(fl->fwd_done + tk.f, unsigned(d.fwd_need), fl->ctl);
   __syncthreads();  // the previous task's readers of sm are done
-  for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) sm.vec[p] = rhs(d.pos0 + int64_t(ND_T) * j0 + p);
+  if (FLOW && !sm.ok) return false;
+  if (has_in) {
+    if (s0 >= 0) v += __ldcg(a.w + s0);
+    if (s1 >= 0) v += __ldcg(a.w + s1);
+    sm.vec[threadIdx.x] = v;
+  }
+  if (o0 >= 0) ov += __ldcg(a.w + o0);
+  if (o1 >= 0) ov += __ldcg(a.w + o1);
   for (int e = threadIdx.x; e < 8 * ND_T; e += ND_THREADS) sm.red[e >> 6][e & 63] = 0.0;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
@@ -415,24 +449,29 @@ __device__ __forceinline__ void nd_forward_task(const NDSolveArgs<T, TM>& a, con
 #pragma unroll
     for (int q = 0; q < 8; ++q) s += sm.red[q][threadIdx.x];
   if (nd_finish(s, ti, ch, nch, a.cnt, d.pos0 / ND_T + i, a.part, &sm.last)) {
-    const int64_t p = d.pos0 + ND_T * i + threadIdx.x;
-    if (i >= d.T1) {
-      a.w[p] = rhs(p) - s;
-    } else if (d.n2 > 0) {
-      a.w[p] = s;
-    } else {  // no update DOFs: x1 = F11^-1 f1 is the solution (no phase on the way down)
-      const int32_t g = a.sep_dof[p];
-      if (g >= 0) a.x[g] = T(s);
+    if (i >= d.T1)
+      a.w[pout] = ov - s;
+    else if (d.n2 > 0)
+      a.w[pout] = s;
+    else if (og >= 0)  // no update DOFs: x1 = F11^-1 f1 is the solution (no phase on the way down)
+      a.x[og] = T(s);
+  }
+  if (FLOW && (nch == 1 || sm.last)) {  // this CTA wrote output tile i: count it (release)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (d.parent >= 0) red_release_add(fl->fwd_done + d.parent, 1u);
+      if (d.n2 == 0) red_release_add(fl->bwd_done + tk.f, 1u);
     }
   }
+  return true;
 }
 
 // Backward task: one chunk of the update tiles for output tile i < T1 of a front, per level
 // down the tree: x1 = w1 - X^T x2, with x2 gathered from the solution at the update DOFs
 // (written by the ancestors' phases); x1 goes to the separator DOFs.
-template <typename T, typename TM>
-__device__ __forceinline__ void nd_backward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
-                                                 NDSolveSmem& sm) {
+template <typename T, typename TM, bool FLOW>
+__device__ __forceinline__ bool nd_backward_task(const NDSolveArgs<T, TM>& a, const NDTask tk, int64_t ti,
+                                                 NDSolveSmem& sm, const NDFlow* fl) {
   const NDFront d = a.fronts[tk.f];
   const int i = tk.i, ch = tk.j, P1 = ND_T * d.T1;
   const int nch = max(1, (d.N - d.T1 + ND_CHUNK - 1) / ND_CHUNK);
@@ -441,11 +480,20 @@ __device__ __forceinline__ void nd_backward_task(const NDSolveArgs<T, TM>& a, co
     const int t = e / (ND_TILE * int(sizeof(TM)) / 128), off = e % (ND_TILE * int(sizeof(TM)) / 128);
     nd_prefetch_l2(reinterpret_cast<const char*>(nd_tile_c(a.pool, d, j0 + t, i)) + 128 * off);
   }
+  // thread k gathers the solution at update DOF k of the chunk (index before the wait, value
+  // after it); threads < 64 also w1 at their output position, after the wait
+  const int u = ND_T * (j0 - d.T1) + int(threadIdx.x);
+  const bool has_in = threadIdx.x < nj * ND_T;
+  const int64_t pout = d.pos0 + int64_t(ND_T) * i + threadIdx.x;
+  const int32_t gi = has_in && u < d.n2 ? a.upd_dof[d.pos0 + P1 + u] : -1;
+  const int32_t og = threadIdx.x < ND_T ? a.sep_dof[pout] : -1;
+  // dataflow: the parent's solution is complete (and with it every ancestor's)
+  if (FLOW && threadIdx.x == 0)
+    sm.ok = d.bwd_need == 0 || coop_wait_count(fl->bwd_done + d.parent, unsigned(d.bwd_need), fl->ctl);
   __syncthreads();
-  for (int p = threadIdx.x; p < nj * ND_T; p += ND_THREADS) {
-    const int u = ND_T * (j0 - d.T1) + p;  // update DOF
-    sm.vec[p] = u < d.n2 ? double(__ldcg(a.x + a.upd_dof[d.pos0 + P1 + u])) : 0.0;
-  }
+  if (FLOW && !sm.ok) return false;
+  if (has_in) sm.vec[threadIdx.x] = gi >= 0 ? double(__ldcg(a.x + gi)) : 0.0;
+  const double wv = og >= 0 ? __ldcg(a.w + pout) : 0.0;
   for (int e = threadIdx.x; e < 8 * ND_T; e += ND_THREADS) sm.red[e >> 6][e & 63] = 0.0;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
@@ -457,10 +505,13 @@ __device__ __forceinline__ void nd_backward_task(const NDSolveArgs<T, TM>& a, co
 #pragma unroll
     for (int q = 0; q < 8; ++q) s += sm.red[q][threadIdx.x];
   if (nd_finish(s, ti, ch, nch, a.cnt, d.pos0 / ND_T + i, a.part, &sm.last)) {
-    const int64_t p = d.pos0 + ND_T * i + threadIdx.x;
-    const int32_t g = a.sep_dof[p];
-    if (g >= 0) a.x[g] = T(__ldcg(a.w + p) - s);
+    if (og >= 0) a.x[og] = T(wv - s);
   }
+  if (FLOW && (nch == 1 || sm.last)) {
+    __syncthreads();
+    if (threadIdx.x == 0) red_release_add(fl->bwd_done + tk.f, 1u);
+  }
+  return true;
 }
 
 // one launch per tree level and direction
@@ -469,42 +520,48 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_solve_level(NDSolveArgs<T, TM
   if (sc && sc->done) return;
   __shared__ NDSolveSmem sm;
   if (FWD)
-    nd_forward_task(a, a.tasks[blockIdx.x], blockIdx.x, sm);
+    nd_forward_task<T, TM, false>(a, a.tasks[blockIdx.x], blockIdx.x, sm, nullptr);
   else
-    nd_backward_task(a, a.tasks[blockIdx.x], blockIdx.x, sm);
+    nd_backward_task<T, TM, false>(a, a.tasks[blockIdx.x], blockIdx.x, sm, nullptr);
 }
 
-// The whole solve as one persistent launch (all CTAs resident): the phases (forward levels from
-// the leaves up, then backward levels from the root down) are separated by the bounded grid
-// barrier; within a phase the CTAs take its tasks in turn.
-constexpr int ND_MAX_PHASES = 64;
-struct NDPhases {
-  int64_t begin[ND_MAX_PHASES], end[ND_MAX_PHASES];
-  int n, nfwd;
-};
-
+// The whole solve as one dataflow launch (all CTAs resident): the tasks in dependency order
+// (a.tasks: the forward tasks from the leaves up, the first nfwd, then the backward tasks from the
+// root down), CTA b taking tasks b, b + grid, ...  A task waits only for the fronts it reads:
+// a forward task for its children's update vectors, a backward task for its parent's solution.
+// Every dependency points to an earlier task, and each CTA takes its tasks in order, so the
+// earliest unfinished task always has its inputs and its CTA is running it: the launch cannot
+// deadlock, and every wait is bounded all the same.
 template <typename T, typename TM>
-__global__ void __launch_bounds__(ND_THREADS) k_nd_solve_coop(NDSolveArgs<T, TM> a, NDPhases ph, const PcgScalars* sc,
-                                                              CoopBarrier* bar) {
+__global__ void __launch_bounds__(ND_THREADS) k_nd_solve_flow(NDSolveArgs<T, TM> a, int64_t nfwd, int64_t ntot,
+                                                              NDFlow fl, int nfronts, const PcgScalars* sc) {
   if (sc && sc->done) return;  // the same for every CTA
   __shared__ NDSolveSmem sm;
-  unsigned epoch = 0;
-  for (int q = 0; q < ph.n; ++q) {
-    for (int64_t t = ph.begin[q] + blockIdx.x; t < ph.end[q]; t += gridDim.x) {
-      if (q < ph.nfwd)
-        nd_forward_task(a, a.tasks[t], t - ph.begin[q], sm);
-      else
-        nd_backward_task(a, a.tasks[t], t - ph.begin[q], sm);
-    }
-    if (q + 1 < ph.n && !coop_barrier(bar, epoch)) break;
+  for (int64_t t = blockIdx.x; t < ntot; t += gridDim.x) {
+    const bool ok = t < nfwd ? nd_forward_task<T, TM, true>(a, a.tasks[t], t, sm, &fl)
+                             : nd_backward_task<T, TM, true>(a, a.tasks[t], t, sm, &fl);
+    if (!ok) break;  // a wait gave up (ctl->err is set): the CTAs after it give up too
   }
-  coop_exit(bar);
+  // the last CTA out zeroes the counters for the next launch (every other CTA is past its tasks)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    sm.last = atomicAdd(&fl.ctl->exits, 1u) == gridDim.x - 1;
+    __threadfence();
+  }
+  __syncthreads();
+  if (sm.last) {
+    for (int f = threadIdx.x; f < nfronts; f += ND_THREADS) {
+      fl.fwd_done[f] = 0u;
+      fl.bwd_done[f] = 0u;
+    }
+    if (threadIdx.x == 0) fl.ctl->exits = 0u;
+  }
 }
 
-__global__ void k_coop_barrier_selftest(CoopBarrier* bar) {
-  if (blockIdx.x != 0) return;  // never arrives
-  unsigned epoch = 0;
-  coop_barrier(bar, epoch);
+// one CTA waits for a counter that nothing raises
+__global__ void k_coop_wait_selftest(CoopControl* ctl) {
+  if (threadIdx.x == 0) coop_wait_count(&ctl->idle, 1u, ctl);
 }
 
 inline unsigned nd_grid(int64_t n, int threads) {
@@ -564,25 +621,13 @@ template <typename T, typename TM>
 void NDDevice::solve(cudaStream_t st, const NDPlan& P, const TM* tiles, const T* b, T* x, const PcgScalars* sc) const {
   NDSolveArgs<T, TM> a{fronts, tasks, tiles, b, x, sep_dof, upd_dof, src0, src1, wvec, part, cnt};
   const int nlev = int(P.levels.size());
-  if (coop_ctas > 0 && 2 * nlev <= ND_MAX_PHASES && nlev > 0) {
-    NDPhases ph{};
+  if (coop_ctas > 0 && nlev > 0) {
     int64_t most = 1;
-    for (int l = nlev - 1; l >= 0; --l) {
-      const NDLevel& L = P.levels[size_t(l)];
-      if (L.fwd[1] == L.fwd[0]) continue;
-      ph.begin[ph.n] = L.fwd[0];
-      ph.end[ph.n++] = L.fwd[1];
-      most = std::max(most, L.fwd[1] - L.fwd[0]);
-    }
-    ph.nfwd = ph.n;
-    for (int l = 0; l < nlev; ++l) {
-      const NDLevel& L = P.levels[size_t(l)];
-      if (L.bwd[1] == L.bwd[0]) continue;
-      ph.begin[ph.n] = L.bwd[0];
-      ph.end[ph.n++] = L.bwd[1];
-      most = std::max(most, L.bwd[1] - L.bwd[0]);
-    }
-    // no more CTAs than the largest phase has tasks: fewer arrivals at each barrier
+    for (const NDLevel& L : P.levels) most = std::max(most, std::max(L.fwd[1] - L.fwd[0], L.bwd[1] - L.bwd[0]));
+    NDSolveArgs<T, TM> af = a;
+    af.tasks = flow;
+    NDFlow fl{flow_done, flow_done + P.fronts.size(), ctl};
+    const int64_t ntot = int64_t(P.flow.size());
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(std::min<int64_t>(coop_ctas, most)));
     cfg.blockDim = dim3(ND_THREADS);
@@ -593,7 +638,7 @@ void NDDevice::solve(cudaStream_t st, const NDPlan& P, const TM* tiles, const T*
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TOPX_CUDA_OK(cudaLaunchKernelEx(&cfg, k_nd_solve_coop<T, TM>, a, ph, sc, bar));
+    TOPX_CUDA_OK(cudaLaunchKernelEx(&cfg, k_nd_solve_flow<T, TM>, af, P.flow_fwd, ntot, fl, int(P.fronts.size()), sc));
     topx::count_launch();
     return;
   }
@@ -617,14 +662,14 @@ int nd_solve_coop_ctas() {
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   if (!coop) return 0;
-  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_nd_solve_coop<double, double>, ND_THREADS, 0));
-  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_nd_solve_coop<float, float>, ND_THREADS, 0));
+  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_nd_solve_flow<double, double>, ND_THREADS, 0));
+  TOPX_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_nd_solve_flow<float, float>, ND_THREADS, 0));
   per = std::min(std::min(per, per32), 4);
   return per >= 1 ? nsm * per : 0;
 }
 
-void launch_coop_barrier_selftest(cudaStream_t st, CoopBarrier* bar) {
-  (k_coop_barrier_selftest<<<2, 32, 0, st>>>(bar), topx::count_launch());
+void launch_coop_wait_selftest(cudaStream_t st, CoopControl* ctl) {
+  (k_coop_wait_selftest<<<1, 32, 0, st>>>(ctl), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

@@ -39,6 +39,10 @@ struct NDFront {
   int parent;     // front index, -1 for a root
   int scr0;       // first scratch tile while its level is swept: P^-1, then R_0 .. R_{N-1} of
                   // even steps and R_0 .. R_{N-1} of odd steps
+  // dataflow solve: output tiles its children complete on the way up before its forward tasks
+  // may start (the sum of their N), and output tiles of its parent's solution (the parent's T1,
+  // 0 for a root) before its backward tasks may start
+  int fwd_need, bwd_need;
 };
 
 // A launch task: front f, tile row i, tile column j.
@@ -84,6 +88,11 @@ struct NDPlan {
   std::vector<int32_t> src[2];          // per position: solve-vector index of child slot 0 / 1's update
                                         // entry that lands here, else -1
   std::vector<NDTask> tasks;
+  // the solve's tasks in dependency order for a dataflow launch: the forward tasks level by level
+  // from the leaves up (the first flow_fwd entries), then the backward tasks from the root down;
+  // a task depends only on tasks before it
+  std::vector<NDTask> flow;
+  int64_t flow_fwd = 0;
   int64_t ntiles = 0, npos = 0;
   int64_t nsolve_tasks = 0;             // upper bound of the solve tasks of one launch (partial sums)
   int nscr = 0;                         // scratch tiles (max over levels)

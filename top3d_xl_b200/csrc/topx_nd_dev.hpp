@@ -24,8 +24,12 @@ struct NDDevice {
   double* wvec = nullptr;   // per position: F11^-1 f1 and the update vectors
   double* part = nullptr;   // per solve task: partial sums of its chunk (64)
   unsigned* cnt = nullptr;  // per output tile: chunks done (zero between launches)
-  int coop_ctas = 0;        // > 0: the solve runs as one persistent launch of this many CTAs
-  CoopBarrier* bar = nullptr;  // its grid barrier
+  // coop_ctas > 0: the solve runs as one persistent dataflow launch of this many CTAs, over the
+  // tasks in dependency order (NDPlan::flow) with 2 x fronts counters and the control words
+  int coop_ctas = 0;
+  const NDTask* flow = nullptr;
+  unsigned* flow_done = nullptr;
+  CoopControl* ctl = nullptr;
   // assembly, extend-add and the sweep of every front: pool <- the factor of the coarsest
   // matrix whose element operators (576 per dense element of grid g) are Ks
   void factor(cudaStream_t st, const NDPlan& P, Grid g, const double* Ks) const;

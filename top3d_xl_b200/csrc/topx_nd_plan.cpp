@@ -146,6 +146,8 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
       P.max_t1 = std::max(P.max_t1, d.T1);
       P.max_t2 = std::max(P.max_t2, d.N - d.T1);
       P.child_slot[size_t(f)] = h.slot;
+      d.fwd_need = 0;
+      d.bwd_need = 0;
     }
     L.pos_end = pos;
     L.nscr = scr;
@@ -153,6 +155,13 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
   }
   P.ntiles = tiles;
   P.npos = pos;
+  for (int f = 0; f < nf; ++f) {
+    NDFront& d = P.fronts[size_t(f)];
+    if (d.parent >= 0) {
+      P.fronts[size_t(d.parent)].fwd_need += d.N;
+      d.bwd_need = P.fronts[size_t(d.parent)].T1;
+    }
+  }
   P.upd_map.assign(size_t(map), -1);
   P.sep_dof.assign(size_t(pos), -1);
   P.upd_dof.assign(size_t(pos), -1);
@@ -304,6 +313,12 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
     L.bwd[1] = int64_t(P.tasks.size());
     P.nsolve_tasks = std::max(P.nsolve_tasks, std::max(L.fwd[1] - L.fwd[0], L.bwd[1] - L.bwd[0]));
   }
+  for (int l = int(P.levels.size()) - 1; l >= 0; --l) {
+    const NDLevel& L = P.levels[size_t(l)];
+    P.flow.insert(P.flow.end(), P.tasks.begin() + L.fwd[0], P.tasks.begin() + L.fwd[1]);
+  }
+  P.flow_fwd = int64_t(P.flow.size());
+  for (const NDLevel& L : P.levels) P.flow.insert(P.flow.end(), P.tasks.begin() + L.bwd[0], P.tasks.begin() + L.bwd[1]);
   nd_check_plan(P);
   return P;
 }
@@ -355,6 +370,33 @@ void nd_check_plan(const NDPlan& P) {
       const int32_t s = P.src[sl][size_t(p)];
       if (s < -1 || s >= P.npos) fail("solve source index");
     }
+  // dataflow order: every front's forward tasks after all of its children's, its backward tasks
+  // after all of its parent's, every forward task before every backward task
+  std::vector<int64_t> fwd_first(size_t(nf), -1), fwd_last(size_t(nf), -1), bwd_first(size_t(nf), -1),
+      bwd_last(size_t(nf), -1);
+  int64_t nsolve = 0;
+  for (const NDLevel& L : P.levels) nsolve += (L.fwd[1] - L.fwd[0]) + (L.bwd[1] - L.bwd[0]);
+  if (int64_t(P.flow.size()) != nsolve || P.flow_fwd < 0 || P.flow_fwd > nsolve) fail("flow size");
+  std::vector<int> need(size_t(nf), 0);
+  for (int64_t t = 0; t < nsolve; ++t) {
+    const NDTask& k = P.flow[size_t(t)];
+    if (k.f < 0 || k.f >= nf) fail("flow task front");
+    auto& first = t < P.flow_fwd ? fwd_first : bwd_first;
+    auto& last = t < P.flow_fwd ? fwd_last : bwd_last;
+    if (first[size_t(k.f)] < 0) first[size_t(k.f)] = t;
+    last[size_t(k.f)] = t;
+  }
+  for (int f = 0; f < nf; ++f) {
+    const NDFront& d = P.fronts[size_t(f)];
+    if (d.parent >= 0) need[size_t(d.parent)] += d.N;
+    if (d.bwd_need != (d.parent >= 0 ? P.fronts[size_t(d.parent)].T1 : 0)) fail("backward need of front " + std::to_string(f));
+    if (d.parent < 0 || fwd_first[size_t(d.parent)] < 0) continue;
+    if (fwd_last[size_t(f)] >= fwd_first[size_t(d.parent)]) fail("flow: a forward task before its child's");
+    if (bwd_first[size_t(f)] >= 0 && bwd_last[size_t(d.parent)] >= bwd_first[size_t(f)])
+      fail("flow: a backward task before its parent's");
+  }
+  for (int f = 0; f < nf; ++f)
+    if (P.fronts[size_t(f)].fwd_need != need[size_t(f)]) fail("forward need of front " + std::to_string(f));
 }
 
 }  // namespace topx

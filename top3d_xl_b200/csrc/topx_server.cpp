@@ -46,10 +46,10 @@ int64_t footprint_estimate(const topx_info& in, int precision) {
   const int nny = in.resY[L] + 1, nnx = in.resX[L] + 1, nnz = in.resZ[L] + 1;
   const std::vector<uint8_t> all(size_t(nny) * nnx * nnz, 1);
   const int64_t stride = (int64_t(nny) * nnx * nnz + 31) / 32 * 32;
-  const topx::NDPlan P = topx::nd_plan(nny, nnx, nnz, stride, all);
+  const topx::NDPlan P = topx::nd_plan(nny, nnx, nnz, stride, all, topx::nd_leaf_nodes(int64_t(all.size())));
   const int64_t tile = int64_t(topx::ND_T) * topx::ND_T;
   const int64_t coarsest = P.ntiles * tile * (precision != TOPX_FP64 ? 12 : 8) + int64_t(P.nscr) * tile * 8 +
-                           P.npos * (8 + 16) + P.nsolve_tasks * topx::ND_T * 8 + P.npos / topx::ND_T * 4 +
+                           P.npos * (8 + 16) + std::max<int64_t>(P.nsolve_tasks, int64_t(P.flow.size())) * topx::ND_T * 8 + P.npos / topx::ND_T * 4 +
                            int64_t(P.tasks.size()) * 8 + int64_t(P.asmb.size()) * 20 +
                            int64_t(P.pad_diag.size()) * 8 + int64_t(P.upd_map.size()) * 4 +
                            int64_t(P.fronts.size()) * int64_t(sizeof(topx::NDFront));
