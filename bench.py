@@ -511,12 +511,13 @@ def main(argv=None):
     relerr = float(np.max(relerrs))
     # roofline of the dominant kernel: level-1 K*u in PCG mode (FP64 in both arms; the tile
     # kernel and its last-row kernel).  Per launch it reads p_old and z and writes q and the new
-    # direction p (3 doubles per node each), reads the moduli (1 double per element) and the
-    # free-DOF bits (1 byte per node): 97 B/node + 8 B/element; per node 8 hexes x 3 rows x 24
-    # DOFs + 24 scalings = 600 FMA.
+    # direction p, and reads and writes the solution y for the previous iteration's step (3
+    # doubles per node each), reads the moduli (1 double per element) and the free-DOF bits (1
+    # byte per node): 145 B/node + 8 B/element; per node 8 hexes x 3 rows x 24 DOFs + 24
+    # scalings = 600 FMA.
     prof = fp64["prof"]
     nn = fp64["nnodes"]
-    alg_bytes = 97 * nn + 8 * fp64["ne"]
+    alg_bytes = 145 * nn + 8 * fp64["ne"]
     flop = 2 * 600 * nn
     ku_ms = prof["ku_ms"] / max(1, prof["ku_launches"])
     achieved = alg_bytes / (ku_ms * 1e-3) / 1e9

@@ -34,6 +34,8 @@ struct PcgScalars {
   double rr;       // r'r
   double resnorm;  // ||r|| / ||b||
   double beta;     // x2 / x1
+  double lam;      // x1 / pq of the last update: its step y += lam p is applied by the next K*u
+                   // (or, after the last iteration, by launch_pcg_flush)
   double tol;
   int its;
   int maxIT;

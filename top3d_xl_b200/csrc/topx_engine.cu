@@ -581,7 +581,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
         for (int c = 0; c < CH; ++c) {  // CH is even: every chunk starts from p
           double* pin = (c & 1) ? kw.p2.p : kw.p.p;
           double* pnew = (c & 1) ? kw.p.p : kw.p2.p;
-          launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
+          launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut, y);
           launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
           vcycle(false, sc);
         }
@@ -595,7 +595,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c], st));
       double* pin = (launched & 1) ? kw.p2.p : kw.p.p;
       double* pnew = (launched & 1) ? kw.p.p : kw.p2.p;
-      launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
+      launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut, y);
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
       sec_begin(SEC_UPDATE);
       launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
@@ -618,6 +618,9 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
     if (h.done) break;
   }
   read_scalars(h, sc);
+  // the last iteration's solution step (each K*u applied the one before it); iteration k wrote
+  // its direction into p2 (k even) or p (k odd)
+  if (h.its > 0) launch_pcg_flush(st, g, y, ((h.its - 1) & 1) ? kw.p.p : kw.p2.p, sc);
   if (prof_) prof_pcg_its += h.its;
   return h.its;
 }

@@ -196,16 +196,43 @@ __device__ __forceinline__ void ku_tile(const uint32_t* __restrict__ active, int
   }
 }
 
+// In PCG mode with yacc given, each node also takes the previous iteration's solution step
+// y += lam p_in (p_in: that iteration's direction; none on the first step).
+template <typename T>
+__device__ __forceinline__ void ku_solution_step(double* __restrict__ yacc, const T* __restrict__ in, int64_t n,
+                                                 int64_t S, double lam) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) yacc[n + c * S] = fma(lam, double(in[n + c * S]), yacc[n + c * S]);
+}
+
+// Shared memory of the tile kernel (dynamic: above the 48 KB of static shared memory in PCG mode)
+template <typename T, int MODE>
+struct KuSmem {
+  T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
+  T se[3][KX + 1][KY + 1];     // ring of 3 element planes
+  T sa[3][KU_NP];              // staged raw plane: u (plain) or z (PCG mode)
+  T sb[MODE == KU_PLAIN ? 1 : 3][MODE == KU_PLAIN ? 1 : KU_NP];  // staged p_old (PCG mode)
+  // PCG mode with the solution step: y at the thread's own node of the staged plane, and the
+  // step length of the previous iteration (read where used: no register across the plane loop)
+  double sy[MODE == KU_PLAIN ? 1 : 3][MODE == KU_PLAIN ? 1 : KNT];
+  double s_lam;
+};
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __restrict__ in, const T* __restrict__ zin,
                                                   T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
-                                                  PcgScalars* sc, RedScratch rs, const uint32_t* __restrict__ active) {
+                                                  PcgScalars* sc, RedScratch rs, const uint32_t* __restrict__ active,
+                                                  double* __restrict__ yacc) {
   if (MODE != KU_PLAIN && sc->done) return;
-  __shared__ T su[3][3][KX + 2][KY + 2];  // ring of 3 node planes: [slot][comp][x][y], masked by the free mask
-  __shared__ T se[3][KX + 1][KY + 1];     // ring of 3 element planes
-  __shared__ T sa[3][KU_NP];              // staged raw plane: u (plain) or z (PCG mode)
-  __shared__ T sb[MODE == KU_PLAIN ? 1 : 3][MODE == KU_PLAIN ? 1 : KU_NP];  // staged p_old (PCG mode)
+  extern __shared__ __align__(16) unsigned char ku_dyn_smem[];
+  KuSmem<T, MODE>& sm = *reinterpret_cast<KuSmem<T, MODE>*>(ku_dyn_smem);
+  auto& su = sm.su;
+  auto& se = sm.se;
+  auto& sa = sm.sa;
+  auto& sb = sm.sb;
+  auto& sy = sm.sy;
+  double& s_lam = sm.s_lam;
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
   const int64_t S = g.stride;
   int tyi, txi, tzi;
@@ -218,6 +245,9 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
   const T* const araw = MODE == KU_PLAIN ? in : zin;
   uint8_t fbs[2];
+  const bool ystep = MODE != KU_PLAIN && yacc && !first;
+  const bool yown = y0 + ty < nny && x0 + tx < nnx;
+  if (ystep && tid == 0) s_lam = sc->lam;
 
   // issue the copies of node plane zp into the staging area (and its free bits into fbs)
   auto issue_nodes = [&](int zp) {
@@ -252,6 +282,25 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
       }
     }
   };
+  // The previous iteration's solution step y += lam p_in rides with the plane copies: y at the
+  // thread's own node of plane zp is copied beside the staged plane, and when that plane is
+  // formed the thread adds lam times the staged p_in there and stores y.
+  auto issue_y = [&](int zp) {
+    if (ystep && yown && zp >= zc0 && zp < zend) {
+      const int64_t n = (y0 + ty) + int64_t(nny) * ((x0 + tx) + int64_t(nnx) * zp);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cp_async_el<8>(&sy[c][tid], yacc + n + c * S, true);
+    }
+  };
+  auto step_y = [&](int zp) {
+    if (ystep && yown && zp >= zc0 && zp < zend) {
+      const int64_t n = (y0 + ty) + int64_t(nny) * ((x0 + tx) + int64_t(nnx) * zp);
+      const int io = (ty + 1) + (KY + 2) * (tx + 1);  // the own node's staging position
+      const double lam = s_lam;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) yacc[n + c * S] = fma(lam, double(sb[c][io]), sy[c][tid]);
+    }
+  };
   // masked values of the staged plane into node slot `slot`
   auto form_nodes = [&](int slot) {
 #pragma unroll
@@ -277,14 +326,17 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   form_nodes(0);
   __syncthreads();
   issue_nodes(zc0);
+  issue_y(zc0);
   cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
   form_nodes(1);
+  step_y(zc0);
   __syncthreads();
   issue_elems(zc0 - 1, 0);
   issue_elems(zc0, 1);
   issue_nodes(zc0 + 1);
+  issue_y(zc0 + 1);
   cp_async_commit();
   const int gy = y0 + ty, gx = x0 + tx;
   const bool own = gy < nny && gx < nnx;
@@ -294,9 +346,11 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
     cp_async_wait_all();
     __syncthreads();
     form_nodes((k + 2) % 3);
+    step_y(z + 1);
     __syncthreads();
     if (z + 1 < zend) {
       issue_nodes(z + 2);
+      issue_y(z + 2);
       issue_elems(z + 1, (k + 2) % 3);
       cp_async_commit();
     }
@@ -364,7 +418,8 @@ template <typename T, int MODE>
 __global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __restrict__ in, const T* __restrict__ zin,
                                                              T* __restrict__ pout, T* __restrict__ out,
                                                              const T* __restrict__ E, const uint8_t* __restrict__ fixbits,
-                                                             const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs) {
+                                                             const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs,
+                                                             double* __restrict__ yacc) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T sp[3][KLZ + 2][KLX + 2][2];  // masked values, [comp][z][x][row y = ny - 1, ny]
   __shared__ T se[KLZ + 1][KLX + 1];        // moduli of element row ny - 1
@@ -373,6 +428,8 @@ __global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __
   const int64_t S = g.stride;
   const bool first = (MODE != KU_PLAIN) && sc->first;
   const T beta = (MODE != KU_PLAIN) ? T(sc->beta) : T(0);
+  const bool ystep = MODE != KU_PLAIN && yacc && !first;
+  const double lam = ystep ? sc->lam : 0.0;
   const int Y = nny - 1;
   const int x0 = blockIdx.x * KLX, z0 = blockIdx.y * KLZ;
   const int tid = threadIdx.x;
@@ -435,6 +492,7 @@ __global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __
     out[n] = y[0];
     out[n + S] = y[1];
     out[n + 2 * S] = y[2];
+    if (ystep) ku_solution_step(yacc, in, n, S, lam);
     if (MODE != KU_PLAIN) {
       if (pout) {
         pout[n] = p[0];
@@ -462,6 +520,14 @@ void prepare_fem_kernels() {
   int n = 0;
   TOPX_CUDA_OK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
   if (n > 0) g_num_sms = n;
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_ku_l1<double, KU_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(sizeof(KuSmem<double, KU_PLAIN>))));
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_ku_l1<double, KU_P_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(sizeof(KuSmem<double, KU_P_UPDATE>))));
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_ku_l1<float, KU_PLAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(sizeof(KuSmem<float, KU_PLAIN>))));
+  TOPX_CUDA_OK(cudaFuncSetAttribute(k_ku_l1<float, KU_P_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(sizeof(KuSmem<float, KU_P_UPDATE>))));
   if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
@@ -518,7 +584,8 @@ std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& presen
 
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
-               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles) {
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles, double* yacc) {
+  if (mode == KU_PLAIN) yacc = nullptr;
   const KuGeometry k = ku_geometry(g);
   const bool lastrow = k.lastrow;
   const int zc = k.zc;
@@ -527,18 +594,20 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
   if (tiles.list && tiles.n == 0) grd = dim3(0);
   if (grd.x == 0) {
   } else if (mode == KU_PLAIN)
-    (k_ku_l1<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs, tiles.list),
+    (k_ku_l1<T, KU_PLAIN><<<grd, blk, sizeof(KuSmem<T, KU_PLAIN>), st>>>(g, zc, in, z, pout, out, E, fixbits, cfix,
+                                                                       sc, rs, tiles.list, yacc),
      topx::count_launch());
   else
-    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, in, z, pout, out, E, fixbits, cfix, sc, rs, tiles.list),
+    (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, sizeof(KuSmem<T, KU_P_UPDATE>), st>>>(g, zc, in, z, pout, out, E, fixbits,
+                                                                             cfix, sc, rs, tiles.list, yacc),
      topx::count_launch());
   if (lastrow) {
     const dim3 nb((g.nnx() + KLX - 1) / KLX, (g.nnz() + KLZ - 1) / KLZ);
     if (mode == KU_PLAIN)
-      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
+      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc),
        topx::count_launch());
     else
-      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs),
+      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc),
        topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
@@ -625,7 +694,9 @@ struct Vec2<float> {
   using type = float2;
 };
 
-// PGIVEN: p already holds the new direction (written by K*u), z is not read and p not written
+// PGIVEN: p already holds the new direction (written by K*u), z is not read and p not written,
+// and the solution step y += lambda p is left to the next K*u (which reads this p as its p_in) or
+// to launch_pcg_flush after the last iteration: lambda goes to sc->lam and y is not touched here
 template <typename T, typename TY, bool PGIVEN>
 __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z, T* __restrict__ p,
                              T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs) {
@@ -651,10 +722,12 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
         pv.y = first ? zv.y : zv.y + beta * pv.y;
         *reinterpret_cast<V2*>(p + k) = pv;
       }
-      Y2 yv = *reinterpret_cast<const Y2*>(y + k);
-      yv.x = yv.x + lamY * TY(pv.x);
-      yv.y = yv.y + lamY * TY(pv.y);
-      *reinterpret_cast<Y2*>(y + k) = yv;
+      if (!PGIVEN) {
+        Y2 yv = *reinterpret_cast<const Y2*>(y + k);
+        yv.x = fma(lamY, TY(pv.x), yv.x);
+        yv.y = fma(lamY, TY(pv.y), yv.y);
+        *reinterpret_cast<Y2*>(y + k) = yv;
+      }
       const V2 qv = *reinterpret_cast<const V2*>(q + k);
       V2 rv = *reinterpret_cast<const V2*>(r + k);
       rv.x = rv.x - lamT * qv.x;
@@ -665,6 +738,7 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
   }
   double v[1] = {rr}, tot[1];
   if (reduce_publish<1>(v, rs, tot) && threadIdx.x == 0) {
+    sc->lam = lam;
     sc->rr = tot[0];
     sc->resnorm = sqrt(tot[0]) / sc->normB;
     sc->its += 1;
@@ -674,6 +748,30 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
     else if (sc->its >= sc->maxIT)
       sc->done = 2;
   }
+}
+
+// y += sc->lam * p over every node: the solution step of the last PCG iteration (PGIVEN updates
+// leave it to the next K*u)
+__global__ void k_pcg_flush(Grid g, double* __restrict__ y, const double* __restrict__ p, const PcgScalars* sc) {
+  const double lam = sc->lam;
+  const int64_t S = g.stride;
+  const int64_t npair = (g.nnodes() + 1) / 2;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npair; i += int64_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = 2 * i + c * S;
+      const double2 pv = *reinterpret_cast<const double2*>(p + k);
+      double2 yv = *reinterpret_cast<const double2*>(y + k);
+      yv.x = fma(lam, pv.x, yv.x);
+      yv.y = fma(lam, pv.y, yv.y);
+      *reinterpret_cast<double2*>(y + k) = yv;
+    }
+  }
+}
+
+void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc) {
+  (k_pcg_flush<<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, sc), topx::count_launch());
+  TOPX_CUDA_OK(cudaGetLastError());
 }
 
 template <typename T, typename TY>
@@ -1090,7 +1188,7 @@ void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int3
 // explicit instantiations
 #define TOPX_INST(T)                                                                                             \
   template void launch_ku<T>(cudaStream_t, KuMode, Grid, const T*, const T*, T*, T*, const T*, const uint8_t*,   \
-                             const T*, PcgScalars*, RedScratch, KuTiles);                                        \
+                             const T*, PcgScalars*, RedScratch, KuTiles, double*);                               \
   template void launch_diag_l1<T, T>(cudaStream_t, Grid, const T*, const uint8_t*, const T*, const uint8_t*, T*); \
   template void launch_residual_init<T>(cudaStream_t, Grid, const T*, const T*, T*, PcgScalars*, RedScratch,     \
                                         double, int);                                                            \

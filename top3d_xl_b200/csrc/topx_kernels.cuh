@@ -36,7 +36,8 @@ struct Grid {
 };
 
 // KU_PLAIN: out = K in.  KU_P_UPDATE: p = z (first PCG step) or z + beta*p_in,
-// out = K p, p'q reduced into sc->pq, and p stored into pout when given (a buffer other than in).
+// out = K p, p'q reduced into sc->pq, and p stored into pout when given (a buffer other than in);
+// with yacc given (PCG mode only), also the previous step's y += sc->lam * p_in (not on the first step).
 enum KuMode { KU_PLAIN = 0, KU_P_UPDATE = 2 };
 
 // element matrices in constant memory
@@ -52,15 +53,19 @@ struct KuTiles {
 std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present);
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
-               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles = KuTiles{});
+               const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles = KuTiles{},
+               double* yacc = nullptr);
 template <typename TE, typename T = TE>
 void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits, const TE* cfix,
                     const uint8_t* present, T* d);
 // p = z (+ beta p); y += lambda p; r -= lambda q; ||r|| stop test into sc.  z null: p already holds
-// the new direction (K*u in PCG mode wrote it through pout) and is only read
+// the new direction (K*u in PCG mode wrote it through pout) and is only read, and y is not touched:
+// lambda goes to sc->lam, for the next K*u (yacc) or launch_pcg_flush to apply
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
                        RedScratch rs);
+// y += sc->lam * p: the solution step of the last PCG iteration
+void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc);
 template <typename T>
 void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r, PcgScalars* sc, RedScratch rs,
                           double tol, int maxIT);
