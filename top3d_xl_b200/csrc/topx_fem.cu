@@ -857,15 +857,16 @@ template <typename TX, typename T, typename TD, int S, bool DOT, bool SMOOTH = t
 __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ xc, Grid gc, const T* __restrict__ r,
                                                         const TD* __restrict__ dinv,
                                                         const uint8_t* __restrict__ present, T* __restrict__ x,
-                                                        Grid gf, T omega, PcgScalars* sc, RedScratch rs, int init) {
+                                                        Grid gf, FastDiv dny, FastDiv dnx, T omega, PcgScalars* sc,
+                                                        RedScratch rs, int init) {
   if ((DOT || !SMOOTH) && sc->done) return;
-  const int fny = gf.nny(), fnx = gf.nnx();
-  const int64_t nn = gf.nnodes();
+  const uint32_t fny = uint32_t(gf.nny()), fnx = uint32_t(gf.nnx());
+  const uint32_t nn = uint32_t(gf.nnodes());  // < 2^32 (checked at launch)
   const int cny = gc.nny(), cnx = gc.nnx();
   double zr = 0.0;
   // grid-stride over the flattened fine grid: no idle lanes on odd extents, and one
   // reduction tail per CTA instead of one per 256 nodes
-  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < nn; n += int64_t(gridDim.x) * blockDim.x) {
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += gridDim.x * blockDim.x) {
     T rv[3], di[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -874,10 +875,11 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
     }
     T v[3] = {T(0), T(0), T(0)};
     if (present[n]) {
-      const int64_t q = n / fny;
+      const uint32_t q = dny.div(n);
       const int fy = int(n - q * fny);
-      const int fz = int(q / fnx);
-      const int fx = int(q - int64_t(fz) * fnx);
+      const uint32_t fzu = dnx.div(q);
+      const int fz = int(fzu);
+      const int fx = int(q - fzu * fnx);
       const int Y = fy / S, X = fx / S, Z = fz / S;
       const int ty = fy - S * Y, tx = fx - S * X, tz = fz - S * Z;
       T pc[3] = {T(0), T(0), T(0)};
@@ -923,18 +925,24 @@ template <typename TX, typename T, typename TD>
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
                            PcgScalars* sc, RedScratch rs) {
+  if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
   const unsigned nb = grid1d(gf.nnodes(), 256, 148 * 8);
   const T w = T(omega);
+  const FastDiv dny{uint32_t(gf.nny())}, dnx{uint32_t(gf.nnx())};
   if (span == 4) {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+       topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+       topx::count_launch());
   } else {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+       topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, rs, init), topx::count_launch());
+      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+       topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -945,11 +953,15 @@ void launch_prolong_add(cudaStream_t st, int span, const TX* xc, Grid gc, const 
   const unsigned nb = grid1d(gf.nnodes(), 256, 148 * 8);
   const T w = T(omega);
   RedScratch none{nullptr, nullptr};
+  if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
+  const FastDiv dny{uint32_t(gf.nny())}, dnx{uint32_t(gf.nnx())};
   if (span == 4)
-    (k_prolong_smooth<TX, T, TD, 4, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, none, 0),
+    (k_prolong_smooth<TX, T, TD, 4, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc,
+                                                                      none, 0),
      topx::count_launch());
   else
-    (k_prolong_smooth<TX, T, TD, 2, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, w, sc, none, 0),
+    (k_prolong_smooth<TX, T, TD, 2, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc,
+                                                                      none, 0),
      topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -1156,11 +1168,12 @@ void launch_simp_scatter(cudaStream_t st, const double* xPhys, const int32_t* el
 // TopOpti_ComputeUnitCompliance (TOP3D_XL.m:579-598): ce_e = u_e^T Ke u_e with the
 // unmodified Ke, one thread per element (compact order), FP64.
 __global__ void k_unit_compliance(Grid g, const double* __restrict__ U, const int32_t* __restrict__ emb0,
-                                  int64_t Ne, double w, int acc, double* __restrict__ ce) {
+                                  int64_t Ne, FastDiv dy, FastDiv dx, double w, int acc, double* __restrict__ ce) {
   const int nny = g.ny + 1, nnx = g.nx + 1;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < Ne; e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t id = emb0[e];
-    const int ey = int(id % g.ny), ex = int((id / g.ny) % g.nx), ez = int(id / (int64_t(g.ny) * g.nx));
+    const uint32_t id = uint32_t(emb0[e]);  // element id on the full box, < 2^31
+    const uint32_t q = dy.div(id), ez = dx.div(q);
+    const int ey = int(id - q * uint32_t(g.ny)), ex = int(q - ez * uint32_t(g.nx));
     double u[24];
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
@@ -1181,7 +1194,9 @@ __global__ void k_unit_compliance(Grid g, const double* __restrict__ U, const in
 }
 void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int32_t* eleMapBack0, int64_t Ne,
                             double weight, bool accumulate, double* ce) {
-  (k_unit_compliance<<<grid1d(Ne, 128), 128, 0, st>>>(g, U, eleMapBack0, Ne, weight, accumulate ? 1 : 0, ce), topx::count_launch());
+  const FastDiv dy{uint32_t(g.ny)}, dx{uint32_t(g.nx)};
+  (k_unit_compliance<<<grid1d(Ne, 128), 128, 0, st>>>(g, U, eleMapBack0, Ne, dy, dx, weight, accumulate ? 1 : 0, ce),
+   topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
