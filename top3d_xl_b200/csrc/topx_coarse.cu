@@ -112,48 +112,63 @@ void launch_galerkin_l2_flagged(cudaStream_t st, Grid gc, const double* Efine, i
 // Span-2 Galerkin operators of levels >= 3 (TOP3D_XL.m:979-995):
 // Ks_J = sum_{c<8} P_c^T Ks_child(c) P_c.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_galerkin_span2(Grid gc, const double* __restrict__ Ksf,
-                                                        const uint8_t* __restrict__ cpresent,
-                                                        const double* __restrict__ P8, double* __restrict__ Ks) {
-  __shared__ double sK[576], sP[576], sT[576];
+// The child prolongators are P_c = W_c (x) I_3 (DOFs interleaved, 3 a + i): W_c[a'][b] is the
+// weight of coarse node b at child node a'.  So Ks_J = sum_c (W_c^T (x) I) K_c (W_c (x) I) costs
+// 2 x 24 x 24 x 8 FMA per child instead of 2 x 24^3, and it sums the same nonzero products in the
+// same order as the dense 24 x 24 products (the skipped terms are exact zeros).
+constexpr int GS2_THREADS = 192;
+constexpr int GS2_PER_THREAD = 8 * 576 / GS2_THREADS;  // 24 outputs of the first product
+__global__ void __launch_bounds__(GS2_THREADS) k_galerkin_span2(Grid gc, const double* __restrict__ Ksf,
+                                                                const uint8_t* __restrict__ cpresent,
+                                                                const double* __restrict__ W8, double* __restrict__ Ks) {
+  __shared__ double sK[8 * 576];  // the 8 children's operators, then T_c = K_c (W_c (x) I) in place
+  __shared__ double sW[8 * 64];   // W_c[a'][b] at c * 64 + 8 a' + b
   const int64_t J = blockIdx.x;
   const int tid = threadIdx.x;
-  double acc[3] = {0.0, 0.0, 0.0};
-  if (cpresent[J]) {
-    const int gy = int(J % gc.ny), gx = int((J / gc.ny) % gc.nx), gz = int(J / (int64_t(gc.ny) * gc.nx));
-    const int fny = 2 * gc.ny, fnx = 2 * gc.nx;
-    for (int c = 0; c < 8; ++c) {
-      const int cy = c & 1, cx = (c >> 1) & 1, cz = c >> 2;
-      const int64_t f = (2 * gy + cy) + int64_t(fny) * ((2 * gx + cx) + int64_t(fnx) * (2 * gz + cz));
-      for (int k = tid; k < 576; k += 256) {
-        sK[k] = Ksf[f * 576 + k];
-        sP[k] = P8[c * 576 + k];
-      }
-      __syncthreads();
-      for (int k = tid; k < 576; k += 256) {
-        const int i = k / 24, jj = k % 24;
-        double s = 0.0;
-        for (int q = 0; q < 24; ++q) s = fma(sK[i * 24 + q], sP[q * 24 + jj], s);
-        sT[k] = s;
-      }
-      __syncthreads();
-      int m = 0;
-      for (int k = tid; k < 576; k += 256, ++m) {
-        const int i = k / 24, jj = k % 24;
-        double s = acc[m];
-        for (int q = 0; q < 24; ++q) s = fma(sP[q * 24 + i], sT[q * 24 + jj], s);
-        acc[m] = s;
-      }
-      __syncthreads();
-    }
+  if (!cpresent[J]) {  // the same for the whole CTA
+    for (int k = tid; k < 576; k += GS2_THREADS) Ks[J * 576 + k] = 0.0;
+    return;
   }
-  int m = 0;
-  for (int k = tid; k < 576; k += 256, ++m) Ks[J * 576 + k] = acc[m];
+  const int gy = int(J % gc.ny), gx = int((J / gc.ny) % gc.nx), gz = int(J / (int64_t(gc.ny) * gc.nx));
+  const int fny = 2 * gc.ny, fnx = 2 * gc.nx;
+  for (int c = 0; c < 8; ++c) {
+    const int cy = c & 1, cx = (c >> 1) & 1, cz = c >> 2;
+    const int64_t f = (2 * gy + cy) + int64_t(fny) * ((2 * gx + cx) + int64_t(fnx) * (2 * gz + cz));
+    for (int k = tid; k < 576; k += GS2_THREADS) sK[c * 576 + k] = Ksf[f * 576 + k];
+  }
+  for (int k = tid; k < 8 * 64; k += GS2_THREADS) sW[k] = W8[k];
+  __syncthreads();
+  // T_c[r][3b + j] = sum_a' K_c[r][3a' + j] W_c[a'][b]
+  double t[GS2_PER_THREAD];
+#pragma unroll
+  for (int m = 0; m < GS2_PER_THREAD; ++m) {
+    const int o = tid + m * GS2_THREADS;
+    const int c = o / 576, rem = o - 576 * c, r = rem / 24, col = rem - 24 * r, b = col / 3, j = col - 3 * b;
+    const double* Kr = sK + c * 576 + r * 24 + j;
+    const double* Wc = sW + c * 64 + b;
+    double s = 0.0;
+#pragma unroll
+    for (int ap = 0; ap < 8; ++ap) s = fma(Kr[3 * ap], Wc[8 * ap], s);
+    t[m] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < GS2_PER_THREAD; ++m) sK[tid + m * GS2_THREADS] = t[m];
+  __syncthreads();
+  // Ks_J[3a + i][col] = sum_c sum_a' W_c[a'][a] T_c[3a' + i][col]
+  for (int o = tid; o < 576; o += GS2_THREADS) {
+    const int row = o / 24, col = o - 24 * row, a = row / 3, i = row - 3 * a;
+    double s = 0.0;
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+      for (int ap = 0; ap < 8; ++ap) s = fma(sW[c * 64 + 8 * ap + a], sK[c * 576 + (3 * ap + i) * 24 + col], s);
+    Ks[J * 576 + o] = s;
+  }
 }
 
-void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* P8,
+void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* W8,
                            double* Ks) {
-  (k_galerkin_span2<<<unsigned(gc.nelems()), 256, 0, st>>>(gc, Ksf, cpresent, P8, Ks), topx::count_launch());
+  (k_galerkin_span2<<<unsigned(gc.nelems()), GS2_THREADS, 0, st>>>(gc, Ksf, cpresent, W8, Ks), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 

@@ -171,8 +171,13 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
       fl_tsel.upload(ts.data(), ts.size());
       fl_F.upload(ff.data(), ff.size());
     }
+    // span-2 child prolongators P_c = W_c (x) I_3: their node weights
     const std::vector<double> P2 = child_prolongators(2);
-    P8.upload(P2.data(), P2.size());
+    std::vector<double> w8(8 * 64);
+    for (int c = 0; c < 8; ++c)
+      for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b) w8[size_t(c) * 64 + 8 * a + b] = P2[size_t(c) * 576 + (3 * a) * 24 + 3 * b];
+    W8.upload(w8.data(), w8.size());
   }
   Ks.resize(nl);
   for (int l = 1; l < nl; ++l) Ks[l].alloc(size_t(G[l].nelems()) * 576);
@@ -458,7 +463,7 @@ void Engine::assemble_launches() {
   launch_galerkin_l2_flagged(st, G[1], E64.p, nflag, fl_elem.p, fl_tsel.p, fl_F.p, Tall.p, Ks[1].p);
   sec_end();
   sec_begin(SEC_GALERKIN3);
-  for (int l = 2; l < nl; ++l) launch_galerkin_span2(st, G[l], Ks[l - 1].p, epresent[l].p, P8.p, Ks[l].p);
+  for (int l = 2; l < nl; ++l) launch_galerkin_span2(st, G[l], Ks[l - 1].p, epresent[l].p, W8.p, Ks[l].p);
   sec_end();
   sec_begin(SEC_DIAG);
   for (int l = 1; l < nl - 1; ++l) {

@@ -201,7 +201,7 @@ class Engine {
   std::vector<DevBuf<double>> F, U;  // per load case, dense SoA FP64
   // coarse operators
   std::vector<DevBuf<double>> Ks;  // per level (index = level-1), dense elements x 576
-  DevBuf<double> Tall, P8;
+  DevBuf<double> Tall, W8;
   DevBuf<int32_t> fl_elem, fl_tsel;
   DevBuf<double> fl_F;
   int nflag = 0;

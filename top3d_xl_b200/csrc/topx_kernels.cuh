@@ -114,7 +114,8 @@ void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int3
 void launch_galerkin_l2(cudaStream_t st, Grid gc, const double* Efine, const double* Tm, double* Ks);
 void launch_galerkin_l2_flagged(cudaStream_t st, Grid gc, const double* Efine, int nflag, const int32_t* fl_elem,
                                 const int32_t* fl_tsel, const double* fl_F, const double* Tall, double* Ks);
-void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* P8,
+// W8: the child prolongation weights W_c[a'][b] (child c, child node a', coarse node b) at c * 64 + 8 a' + b
+void launch_galerkin_span2(cudaStream_t st, Grid gc, const double* Ksf, const uint8_t* cpresent, const double* W8,
                            double* Ks);
 template <typename T>
 void launch_diag_coarse(cudaStream_t st, Grid g, const double* Ks, const uint8_t* present, T* d);
