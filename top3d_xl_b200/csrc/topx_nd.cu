@@ -29,7 +29,8 @@ namespace {
 
 constexpr int ND_TILE = ND_T * ND_T;
 constexpr int ND_THREADS = GF_THREADS;  // 256
-constexpr size_t ND_SMEM_SWEEP = size_t(3) * GF_BUF * sizeof(double);
+// two staging buffers per sweep CTA (three CTAs per SM)
+constexpr size_t ND_SMEM_SWEEP = size_t(2) * GF_BUF * sizeof(double);
 static_assert(ND_T == GF_T, "tile widths");
 
 __device__ __forceinline__ int64_t nd_tri(int64_t i) { return i * (i + 1) / 2; }
@@ -209,7 +210,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restr
   extern __shared__ __align__(16) double nd_smem[];
   double* bufA = nd_smem;
   double* bufB = nd_smem + GF_BUF;
-  double* bufD = nd_smem + 2 * GF_BUF;
   const NDTask tk = tasks[blockIdx.x];
   const NDFront d = fronts[tk.f];
   if (tk.i > k)
@@ -218,20 +218,17 @@ __global__ void __launch_bounds__(ND_THREADS) k_nd_update(const NDFront* __restr
     nd_stage_transposed(bufA, nd_tile_c(pool, d, k, tk.i), GF_LDA, -1.0);
   gf_stage_ring(bufB, nd_rslot(scr, d, k, tk.j), GF_LD);
   double* D = nd_tile(pool, d, tk.i, tk.j);
-  gf_stage_ring(bufD, D, GF_LD);
+  double acc[4][2][2];
+  gf_load_acc(acc, D);  // the tile goes straight into the accumulators while the operands land
   gf_cp_wait();
   __syncthreads();
-  double acc[4][2][2];
-  gf_for_outputs(acc, [&](int r, int c, double& v) { v = bufD[r * GF_LD + c]; });
   gf_product(bufA, bufB, acc);
-  __syncthreads();
   if (tk.i == k + 1 && tk.j == k + 1 && k + 1 < d.T1) {
+    __syncthreads();  // bufA becomes the pivot's workspace
     nd_pivot_acc(acc, D, scr, d, bufA);
     return;
   }
-  gf_for_outputs(acc, [&](int r, int c, double v) { bufD[r * GF_LD + c] = v; });
-  __syncthreads();
-  gf_copy_to_ring(D, bufD, GF_LD);
+  gf_store_acc(D, acc);
 }
 
 // ---------------------------------------------------------------------------

@@ -87,6 +87,31 @@ __device__ __forceinline__ void gf_for_outputs(double (&acc)[4][2][2], F&& f) {
       for (int h = 0; h < 2; ++h) f(rb + 8 * fr + g, cb + 8 * fc + 2 * q + h, acc[fr][fc][h]);
 }
 
+// This thread's accumulators from / to a contiguous 64 x 64 tile in global memory (16-byte
+// accesses; loads through L2 only, since earlier launches wrote the tile)
+__device__ __forceinline__ void gf_load_acc(double (&acc)[4][2][2], const double* __restrict__ g) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gi = lane >> 2, q = lane & 3;
+  const int rb = (warp >> 2) * 32, cb = (warp & 3) * 16;
+#pragma unroll
+  for (int fr = 0; fr < 4; ++fr)
+#pragma unroll
+    for (int fc = 0; fc < 2; ++fc) {
+      const double2 v = __ldcg(reinterpret_cast<const double2*>(g + (rb + 8 * fr + gi) * GF_T + cb + 8 * fc + 2 * q));
+      acc[fr][fc][0] = v.x;
+      acc[fr][fc][1] = v.y;
+    }
+}
+__device__ __forceinline__ void gf_store_acc(double* __restrict__ g, const double (&acc)[4][2][2]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gi = lane >> 2, q = lane & 3;
+  const int rb = (warp >> 2) * 32, cb = (warp & 3) * 16;
+#pragma unroll
+  for (int fr = 0; fr < 4; ++fr)
+#pragma unroll
+    for (int fc = 0; fc < 2; ++fc)
+      *reinterpret_cast<double2*>(g + (rb + 8 * fr + gi) * GF_T + cb + 8 * fc + 2 * q) =
+          make_double2(acc[fr][fc][0], acc[fr][fc][1]);
+}
+
 // PIV works in the last staging buffer of the CTA's dynamic shared memory
 struct GFPivotSmem {
   double rowS[2][8][72];   // pivot row block (old values), double-buffered by step
