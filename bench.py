@@ -69,9 +69,9 @@ def load_workload(ctx, wl):
 METRIC = "OC iterations/s (GLOBAL, FP64; mixed precision beside it)"
 # DRAM bytes (read + write) per grid node of one K*u launch in PCG mode (tile kernel + last-row
 # kernel), from an ncu capture of the 128x256x128 cuboid: dram__bytes_read.sum +
-# dram__bytes_write.sum of two launches, 470.53 MB and 465.26 MB, over 4,276,737 nodes; the
-# traffic of a launch scales with its node count.
-KU_TRAFFIC_PER_NODE = 467.89e6 / 4276737
+# dram__bytes_write.sum of the tile kernel (637.2 MB) and the last-row kernel (52.9 MB) over
+# 4,276,737 nodes; the traffic of a launch scales with its node count.
+KU_TRAFFIC_PER_NODE = 690.1e6 / 4276737
 # Nominal FP64 rate of a B200 on CUDA cores: 148 SMs x 64 FMA/clk x 2 flop x 1.965 GHz.
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
