@@ -156,20 +156,27 @@ def test_vcycle_with_large_coarsest_slabs(shape):
         assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-10
 
 
-@pytest.mark.parametrize("kind", ["cuboid", "irregular"])
+@pytest.mark.parametrize("kind", ["cuboid", "irregular", "u_shape"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_persistent_coarse_solve_matches_level_launches(kind, precision):
-    # the coarsest solve as one dataflow launch (tasks wait for their children's or parent's
+    # the coarsest solve as one dataflow launch (tasks wait for their children's or an ancestor's
     # counters) and as one launch per tree level run the same tasks with the same summation
     # order: the V-cycles agree bit for bit, over repeated solves (the counters are re-armed by
-    # each launch) and after a second factorisation
+    # each launch) and after a second factorisation.  The U-shaped domain's tree has fronts whose
+    # separator holds no present node (nothing eliminated, update DOFs around it): their
+    # children's solves up and down must wait past them, for the nearest eliminating ancestor.
     from top3d_xl_b200 import Context
     if kind == "cuboid":
         vox = np.ones((64, 128, 64), bool)
-    else:
+    elif kind == "irregular":
         vox = np.random.default_rng(12).random((64, 128, 64)) < 0.8
         vox[:, 0, :] = True
         vox[:, -1, :] = True
+    else:
+        vox = np.zeros((64, 160, 64), bool)
+        vox[:, :8, :] = True
+        vox[:, -8:, :] = True
+        vox[:, :, :8] = True
     E = 1.0 + np.random.default_rng(11).uniform(0.0, 1.0, int(vox.sum())) ** 3
     outs = []
     for coop in (1, 0):

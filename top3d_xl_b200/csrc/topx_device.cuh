@@ -183,6 +183,14 @@ __device__ __forceinline__ bool reduce_publish_max(double v, RedScratch rs, doub
 // 1994): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
 //   q = (t + ((n - t) >> 1)) >> (l - 1),  t = mulhi(m, n)    (l >= 1; d = 1 returns n)
 // exact for every n < 2^32.
+// Chunk mask of a node grid on an irregular domain: bit c of word c / 32 is set when nodes
+// [32 c, 32 c + 32) of the dense grid hold a present node.  Nodes outside every present chunk are
+// zero in every vector and stay so, so elementwise passes skip their chunks (a warp's 32
+// consecutive nodes share one bit).  A null mask means every chunk is present.
+__device__ __forceinline__ bool chunk_active(const uint32_t* __restrict__ act, int64_t n) {
+  return !act || ((__ldg(act + (n >> 10)) >> ((n >> 5) & 31)) & 1u) != 0u;
+}
+
 struct FastDiv {
   uint32_t d = 1, m = 0;
   int l = 0;

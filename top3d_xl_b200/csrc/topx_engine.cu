@@ -192,6 +192,27 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
       kuTiles.upload(act.data(), act.size());
       kut = KuTiles{kuTiles.p, int(act.size())};
     }
+    const std::vector<uint32_t> fact = filter_active_tiles(G[0], pn);
+    if (!fact.empty() && fact.size() < filter_active_tiles(G[0], all).size() * 9 / 10) {
+      filterTiles.upload(fact.data(), fact.size());
+      fut = KuTiles{filterTiles.p, int(fact.size())};
+    }
+    // elementwise level-1 passes skip the 32-node chunks without a present node
+    const size_t nchunk = (pn.size() + 31) / 32;
+    std::vector<uint32_t> mask((nchunk + 31) / 32, 0u);
+    size_t nact = 0;
+    for (size_t c = 0; c < nchunk; ++c) {
+      bool any = false;
+      for (size_t k = 32 * c; k < std::min(pn.size(), 32 * c + 32) && !any; ++k) any = pn[k] != 0;
+      if (any) {
+        mask[c / 32] |= 1u << (c % 32);
+        ++nact;
+      }
+    }
+    if (nact < nchunk * 9 / 10) {
+      act1Mask.upload(mask.data(), mask.size());
+      act1 = act1Mask.p;
+    }
   }
   // ---- coarsest level: nested-dissection plan and factor storage -----------------
   {
@@ -378,6 +399,11 @@ void Engine::check_coop_waits() {
   check_device_waits();
 }
 
+void Engine::copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) const {
+  TOPX_CUDA_OK(cudaMemcpyAsync(dst, src, bytes, kind, st));
+  TOPX_CUDA_OK(cudaStreamSynchronize(st));
+}
+
 // The persistent coarse solve's dependency waits set an error word instead of spinning on (they
 // are bounded); the word was copied into pinned memory before the caller's stream sync.  A word
 // that is set is cleared (so the engine stays usable) and reported.
@@ -386,9 +412,10 @@ void Engine::check_device_waits() const {
     const int err = h_ctl->err;
     h_ctl->err = 0;
     // a launch that gave up may leave chunk tickets and dependency counts behind
-    TOPX_CUDA_OK(cudaMemset(coopCtl.p, 0, sizeof(CoopControl)));
-    TOPX_CUDA_OK(cudaMemset(ndCnt.p, 0, sizeof(unsigned) * ndCnt.n));
-    if (ndDone.p) TOPX_CUDA_OK(cudaMemset(ndDone.p, 0, sizeof(unsigned) * ndDone.n));
+    TOPX_CUDA_OK(cudaMemsetAsync(coopCtl.p, 0, sizeof(CoopControl), st));
+    TOPX_CUDA_OK(cudaMemsetAsync(ndCnt.p, 0, sizeof(unsigned) * ndCnt.n, st));
+    if (ndDone.p) TOPX_CUDA_OK(cudaMemsetAsync(ndDone.p, 0, sizeof(unsigned) * ndDone.n, st));
+    TOPX_CUDA_OK(cudaStreamSynchronize(st));
     throw DeviceWaitError(err == kCoopErrWait ? "coarse solve: a dependency wait gave up (persistent launch not co-resident)"
                                               : "coarse solve: unknown wait error");
   }
@@ -412,11 +439,11 @@ void Engine::selftest_wait(int which) {
 // ---------------------------------------------------------------------------
 void Engine::set_xphys(const double* h) {
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(xPhys.p, h, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  copy_sync(xPhys.p, h, sizeof(double) * Ne, cudaMemcpyHostToDevice);
 }
 void Engine::get_xphys(double* h) const {
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(h, xPhys.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+  copy_sync(h, xPhys.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost);
 }
 void Engine::get_U(int lc, double* h) const {
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
@@ -424,7 +451,7 @@ void Engine::get_U(int lc, double* h) const {
   tmp.alloc(size_t(Nn) * 3);
   launch_grid_to_compact_nodes<double>(st, U[lc].p, tmp.p, G[0], nodMapBack0.p, Nn);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(h, tmp.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+  copy_sync(h, tmp.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost);
 }
 void Engine::set_U(int lc, const double* h) {
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
@@ -505,7 +532,7 @@ void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
     launch_prolong_smooth<TC, TC, TC>(st, M.levels[l + 1].span, v.xl[l + 1].p, G[l + 1], v.rl[l].p, v.dl[l].p,
                                       present[l].p, v.xl[l].p, G[l], om, false, false, sc, rs1);
   launch_prolong_smooth<TC, double, TC>(st, M.levels[1].span, v.xl[1].p, G[1], kw.r.p, v.d1.p, present[0].p,
-                                        kw.z.p, G[0], om, true, init, sc, rs1);
+                                        kw.z.p, G[0], om, true, init, sc, rs1, act1);
   sec_end();
 }
 
@@ -587,7 +614,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
           double* pin = (c & 1) ? kw.p2.p : kw.p.p;
           double* pnew = (c & 1) ? kw.p.p : kw.p2.p;
           launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut, y);
-          launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
+          launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1, act1);
           vcycle(false, sc);
         }
       });
@@ -603,7 +630,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
       launch_ku<double>(st, KU_P_UPDATE, g, pin, kw.z.p, pnew, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut, y);
       if (prof_) TOPX_CUDA_OK(cudaEventRecord(pev[2 * c + 1], st));
       sec_begin(SEC_UPDATE);
-      launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1);
+      launch_pcg_update<double, double>(st, g, y, nullptr, pnew, kw.r.p, kw.q.p, sc, rs1, act1);
       sec_end();
       vcycle(false, sc);
     }
@@ -625,7 +652,7 @@ int Engine::pcg(const double* b, double* y, bool warm, double tol, int maxIT) {
   read_scalars(h, sc);
   // the last iteration's solution step (each K*u applied the one before it); iteration k wrote
   // its direction into p2 (k even) or p (k odd)
-  if (h.its > 0) launch_pcg_flush(st, g, y, ((h.its - 1) & 1) ? kw.p.p : kw.p2.p, sc);
+  if (h.its > 0) launch_pcg_flush(st, g, y, ((h.its - 1) & 1) ? kw.p.p : kw.p2.p, sc, act1);
   if (prof_) prof_pcg_its += h.its;
   return h.its;
 }
@@ -665,9 +692,9 @@ int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) 
   const Grid& g = G[0];
   PcgScalars* sc = scF.p;
   launch_scatter_elems_t<T>(st, d_src, eleMapBack0.p, Ne, w.fsrc.p);
-  launch_filter_e2n<T>(st, g, w.fsrc.p, w.fb.p);
+  launch_filter_e2n<T>(st, g, w.fsrc.p, w.fb.p, act1);
   launch_filter_residual_init<T>(st, g, w.fb.p, w.fdp[slot].p, w.fr.p, w.fz.p, w.fy.p, sc, rs1, M.S.tol / 10,
-                                 M.S.maxIT);
+                                 M.S.maxIT, act1);
   const int CH = 8;
   PcgScalars h{};
   int launched = 0;
@@ -679,8 +706,8 @@ int Engine::filter_t(FWork<T>& w, int slot, const double* d_src, double* d_out) 
     const int n = std::min(CH, M.S.maxIT - launched);
     auto body = [&]() {
       for (int c = 0; c < n; ++c) {
-        launch_filter_ku<T>(st, KU_P_UPDATE, g, kf, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1);
-        launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1);
+        launch_filter_ku<T>(st, KU_P_UPDATE, g, kf, w.fp.p, w.fz.p, nullptr, w.fq.p, solid1.p, sc, rs1, fut);
+        launch_filter_update<T>(st, g, w.fy.p, w.fp.p, w.fr.p, w.fq.p, w.fdp[slot].p, w.fz.p, sc, rs1, act1);
       }
     };
     if (n == CH)
@@ -713,7 +740,7 @@ void Engine::apply_K(const double* h_u, double* h_y) {
   launch_ku<double>(st, KU_PLAIN, G[0], du.p, nullptr, nullptr, dy.p, E64.p, fixbits.p, cfix64.p, nullptr, rs1);
   launch_grid_to_compact_nodes<double>(st, dy.p, cu.p, G[0], nodMapBack0.p, Nn);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(h_y, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+  copy_sync(h_y, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost);
 }
 
 void Engine::apply_vcycle(const double* h_r, double* h_z) {
@@ -722,13 +749,13 @@ void Engine::apply_vcycle(const double* h_r, double* h_z) {
   cu.upload(h_r, size_t(Nn) * 3);
   PcgScalars z{};
   z.done = 0;
-  TOPX_CUDA_OK(cudaMemcpy(scE.p, &z, sizeof(z), cudaMemcpyHostToDevice));
+  copy_sync(scE.p, &z, sizeof(z), cudaMemcpyHostToDevice);
   TOPX_CUDA_OK(cudaMemsetAsync(kw.r.p, 0, kw.r.bytes(), st));
   launch_compact_to_grid_nodes<double>(st, cu.p, kw.r.p, G[0], nodMapBack0.p, Nn);
   vcycle(true, scE.p);
   launch_grid_to_compact_nodes<double>(st, kw.z.p, cu.p, G[0], nodMapBack0.p, Nn);
   check_coop_waits();
-  TOPX_CUDA_OK(cudaMemcpy(h_z, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost));
+  copy_sync(h_z, cu.p, sizeof(double) * Nn * 3, cudaMemcpyDeviceToHost);
 }
 
 void Engine::timer_start() { TOPX_CUDA_OK(cudaEventRecord(tev[0], st)); }
@@ -815,7 +842,7 @@ void Engine::sec_harvest() {
 
 void Engine::set_moduli_host(const double* h_E) {
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_E, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  copy_sync(tmpA.p, h_E, sizeof(double) * Ne, cudaMemcpyHostToDevice);
   launch_scatter_elems_t<double>(st, tmpA.p, eleMapBack0.p, Ne, E64.p);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
 }
@@ -830,10 +857,10 @@ int Engine::pcg_host(int lc, double* h_u) {
 int Engine::filter_host(double rmin, const double* h_src, double* h_out) {
   setup_filter(0, rmin);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(tmpA.p, h_src, sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  copy_sync(tmpA.p, h_src, sizeof(double) * Ne, cudaMemcpyHostToDevice);
   const int its = filter(0, tmpA.p, tmpB.p);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(h_out, tmpB.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+  copy_sync(h_out, tmpB.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost);
   return its;
 }
 
@@ -841,7 +868,7 @@ void Engine::compliance_host(const double* h_U, double* h_ce) {
   for (size_t lc = 0; lc < U.size(); ++lc) set_U(int(lc), h_U + lc * size_t(Nn) * 3);
   compliance(ce.p);
   TOPX_CUDA_OK(cudaStreamSynchronize(st));
-  TOPX_CUDA_OK(cudaMemcpy(h_ce, ce.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost));
+  copy_sync(h_ce, ce.p, sizeof(double) * Ne, cudaMemcpyDeviceToHost);
 }
 
 void Engine::get_diag(int level, double* h_d) const {
@@ -852,12 +879,12 @@ void Engine::get_diag(int level, double* h_d) const {
   if (!pre32()) {
     const double* src = level == 1 ? v64.d1.p : v64.dl[level - 1].p;
     TOPX_CUDA_OK(cudaStreamSynchronize(st));
-    TOPX_CUDA_OK(cudaMemcpy(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost));
+    copy_sync(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost);
   } else {
     std::vector<float> f(dense.size());
     const float* src = level == 1 ? v32.d1.p : v32.dl[level - 1].p;
     TOPX_CUDA_OK(cudaStreamSynchronize(st));
-    TOPX_CUDA_OK(cudaMemcpy(f.data(), src, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+    copy_sync(f.data(), src, sizeof(float) * f.size(), cudaMemcpyDeviceToHost);
     for (size_t i = 0; i < f.size(); ++i) dense[i] = f[i];
   }
   // the engine stores reciprocal diagonals
@@ -883,7 +910,7 @@ void Engine::begin(int consType, double V0, int nLoop, double rMin, double rHat)
   setup_filter(0, rMin);
   if (consType == 1) setup_filter(1, rHat);
   std::vector<double> h(size_t(Ne), V0);
-  for (DevBuf<double>* b : {&x, &xPhys, &xTilde, &volMax}) TOPX_CUDA_OK(cudaMemcpy(b->p, h.data(), sizeof(double) * Ne, cudaMemcpyHostToDevice));
+  for (DevBuf<double>* b : {&x, &xPhys, &xTilde, &volMax}) copy_sync(b->p, h.data(), sizeof(double) * Ne, cudaMemcpyHostToDevice);
   for (auto& u : U) TOPX_CUDA_OK(cudaMemsetAsync(u.p, 0, u.bytes(), st));
   // compliance of the fully solid domain (TOP3D_XL.m:94-104)
   update_moduli(nullptr, true);

@@ -55,12 +55,20 @@ struct DevBuf {
       TOPX_CUDA_OK(cudaMalloc(&p, sizeof(T) * count));
       n = count;
       devbuf_bytes() += int64_t(sizeof(T) * count);
-      if (zero) TOPX_CUDA_OK(cudaMemset(p, 0, sizeof(T) * count));
+      // the default stream's work does not order the engine's non-blocking stream: the zeroing
+      // (asynchronous to the host) must be complete before any engine kernel may touch the buffer
+      if (zero) {
+        TOPX_CUDA_OK(cudaMemsetAsync(p, 0, sizeof(T) * count, 0));
+        TOPX_CUDA_OK(cudaStreamSynchronize(0));
+      }
     }
   }
   void upload(const T* h, size_t count) {
     alloc(count, false);
-    if (count) TOPX_CUDA_OK(cudaMemcpy(p, h, sizeof(T) * count, cudaMemcpyHostToDevice));
+    if (count) {  // a copy from pageable memory may still be in flight when cudaMemcpy returns
+      TOPX_CUDA_OK(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, 0));
+      TOPX_CUDA_OK(cudaStreamSynchronize(0));
+    }
   }
   void release() {
     if (p) {
@@ -207,6 +215,10 @@ class Engine {
   int nflag = 0;
   DevBuf<uint32_t> kuTiles;  // level-1 K*u tiles that own a node of the domain
   KuTiles kut;               // their list (null: the whole grid)
+  DevBuf<uint32_t> filterTiles;  // the same for the filter's K*u (its own z-chunks)
+  KuTiles fut;
+  DevBuf<uint32_t> act1Mask;     // level-1 chunk mask (chunk_active) of an irregular domain
+  const uint32_t* act1 = nullptr;  // null: every chunk holds a present node
   // coarsest level: nested-dissection plan, its device copy and the factor tiles
   NDPlan nd;
   NDDevice ndd;
@@ -224,6 +236,8 @@ class Engine {
   int coopCtas = 0;             // its CTA count; 0: one launch per tree level and direction
   void check_coop_waits();      // waits for the stream; throws if a wait gave up (re-arming the words)
   void check_device_waits() const;  // after a stream sync: throws if a bounded device wait gave up
+  // a copy between host and device ordered on the engine's stream, complete when it returns
+  void copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) const;
   // workspaces
   KrylovWork kw;
   VWork<double> v64;

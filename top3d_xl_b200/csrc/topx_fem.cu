@@ -699,7 +699,8 @@ struct Vec2<float> {
 // to launch_pcg_flush after the last iteration: lambda goes to sc->lam and y is not touched here
 template <typename T, typename TY, bool PGIVEN>
 __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z, T* __restrict__ p,
-                             T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs) {
+                             T* __restrict__ r, const T* __restrict__ q, PcgScalars* sc, RedScratch rs,
+                             const uint32_t* __restrict__ act) {
   if (sc->done) return;
   const bool first = sc->first;
   const T beta = T(sc->beta);
@@ -712,6 +713,7 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
   using V2 = typename Vec2<T>::type;
   using Y2 = typename Vec2<TY>::type;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npair; i += int64_t(gridDim.x) * blockDim.x) {
+    if (!chunk_active(act, 2 * i)) continue;  // both nodes of the pair lie in one chunk
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t k = 2 * i + c * S;
@@ -752,11 +754,13 @@ __global__ void k_pcg_update(Grid g, TY* __restrict__ y, const T* __restrict__ z
 
 // y += sc->lam * p over every node: the solution step of the last PCG iteration (PGIVEN updates
 // leave it to the next K*u)
-__global__ void k_pcg_flush(Grid g, double* __restrict__ y, const double* __restrict__ p, const PcgScalars* sc) {
+__global__ void k_pcg_flush(Grid g, double* __restrict__ y, const double* __restrict__ p, const PcgScalars* sc,
+                            const uint32_t* __restrict__ act) {
   const double lam = sc->lam;
   const int64_t S = g.stride;
   const int64_t npair = (g.nnodes() + 1) / 2;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npair; i += int64_t(gridDim.x) * blockDim.x) {
+    if (!chunk_active(act, 2 * i)) continue;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t k = 2 * i + c * S;
@@ -769,18 +773,21 @@ __global__ void k_pcg_flush(Grid g, double* __restrict__ y, const double* __rest
   }
 }
 
-void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc) {
-  (k_pcg_flush<<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, sc), topx::count_launch());
+void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc,
+                      const uint32_t* act) {
+  (k_pcg_flush<<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, sc, act), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
-                       RedScratch rs) {
+                       RedScratch rs, const uint32_t* act) {
   if (z)
-    (k_pcg_update<T, TY, false><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
+    (k_pcg_update<T, TY, false><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs, act),
+     topx::count_launch());
   else
-    (k_pcg_update<T, TY, true><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs), topx::count_launch());
+    (k_pcg_update<T, TY, true><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, z, p, r, q, sc, rs, act),
+     topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -858,7 +865,7 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
                                                         const TD* __restrict__ dinv,
                                                         const uint8_t* __restrict__ present, T* __restrict__ x,
                                                         Grid gf, FastDiv dny, FastDiv dnx, T omega, PcgScalars* sc,
-                                                        RedScratch rs, int init) {
+                                                        RedScratch rs, int init, const uint32_t* __restrict__ act) {
   if ((DOT || !SMOOTH) && sc->done) return;
   const uint32_t fny = uint32_t(gf.nny()), fnx = uint32_t(gf.nnx());
   const uint32_t nn = uint32_t(gf.nnodes());  // < 2^32 (checked at launch)
@@ -867,6 +874,7 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
   // grid-stride over the flattened fine grid: no idle lanes on odd extents, and one
   // reduction tail per CTA instead of one per 256 nodes
   for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += gridDim.x * blockDim.x) {
+    if (!chunk_active(act, n)) continue;  // x is zero there and stays so
     T rv[3], di[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -924,24 +932,24 @@ __global__ void __launch_bounds__(256) k_prolong_smooth(const TX* __restrict__ x
 template <typename TX, typename T, typename TD>
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
-                           PcgScalars* sc, RedScratch rs) {
+                           PcgScalars* sc, RedScratch rs, const uint32_t* act) {
   if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
   const unsigned nb = grid1d(gf.nnodes(), 256, 148 * 8);
   const T w = T(omega);
   const FastDiv dny{uint32_t(gf.nny())}, dnx{uint32_t(gf.nnx())};
   if (span == 4) {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+      (k_prolong_smooth<TX, T, TD, 4, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init, act),
        topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+      (k_prolong_smooth<TX, T, TD, 4, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init, act),
        topx::count_launch());
   } else {
     if (dot)
-      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+      (k_prolong_smooth<TX, T, TD, 2, true><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init, act),
        topx::count_launch());
     else
-      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init),
+      (k_prolong_smooth<TX, T, TD, 2, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc, rs, init, act),
        topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
@@ -957,11 +965,11 @@ void launch_prolong_add(cudaStream_t st, int span, const TX* xc, Grid gc, const 
   const FastDiv dny{uint32_t(gf.nny())}, dnx{uint32_t(gf.nnx())};
   if (span == 4)
     (k_prolong_smooth<TX, T, TD, 4, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc,
-                                                                      none, 0),
+                                                                      none, 0, nullptr),
      topx::count_launch());
   else
     (k_prolong_smooth<TX, T, TD, 2, false, false><<<nb, 256, 0, st>>>(xc, gc, r, d, present, x, gf, dny, dnx, w, sc,
-                                                                      none, 0),
+                                                                      none, 0, nullptr),
      topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -1210,21 +1218,21 @@ void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int3
   template void launch_restrict<T, T>(cudaStream_t, int, const T*, Grid, T*, T*, T*, Grid);                      \
   template void launch_prolong_smooth<T, T, T>(cudaStream_t, int, const T*, Grid, const T*, const T*,            \
                                                const uint8_t*, T*, Grid, double, bool, bool, PcgScalars*,        \
-                                               RedScratch);                                                      \
+                                               RedScratch, const uint32_t*);                                     \
   template void launch_compact_to_grid_nodes<T>(cudaStream_t, const double*, T*, Grid, const int32_t*, int64_t); \
   template void launch_grid_to_compact_nodes<T>(cudaStream_t, const T*, double*, Grid, const int32_t*, int64_t);
 TOPX_INST(double)
 TOPX_INST(float)
 template void launch_pcg_update<double, double>(cudaStream_t, Grid, double*, const double*, double*, double*,
-                                                const double*, PcgScalars*, RedScratch);
+                                                const double*, PcgScalars*, RedScratch, const uint32_t*);
 template void launch_pcg_update<float, float>(cudaStream_t, Grid, float*, const float*, float*, float*, const float*,
-                                              PcgScalars*, RedScratch);
+                                              PcgScalars*, RedScratch, const uint32_t*);
 template void launch_diag_l1<double, float>(cudaStream_t, Grid, const double*, const uint8_t*, const double*,
                                            const uint8_t*, float*);
 template void launch_restrict<double, float>(cudaStream_t, int, const double*, Grid, float*, float*, float*, Grid);
 template void launch_prolong_smooth<float, double, float>(cudaStream_t, int, const float*, Grid, const double*,
                                                           const float*, const uint8_t*, double*, Grid, double, bool,
-                                                          bool, PcgScalars*, RedScratch);
+                                                          bool, PcgScalars*, RedScratch, const uint32_t*);
 template void launch_prolong_add<double, double, double>(cudaStream_t, int, const double*, Grid, const double*,
                                                         const double*, const uint8_t*, double*, Grid, double,
                                                         PcgScalars*);

@@ -63,9 +63,10 @@ void launch_diag_l1(cudaStream_t st, Grid g, const TE* E, const uint8_t* fixbits
 // lambda goes to sc->lam, for the next K*u (yacc) or launch_pcg_flush to apply
 template <typename T, typename TY>
 void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, const T* q, PcgScalars* sc,
-                       RedScratch rs);
+                       RedScratch rs, const uint32_t* act = nullptr);
 // y += sc->lam * p: the solution step of the last PCG iteration
-void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc);
+void launch_pcg_flush(cudaStream_t st, Grid g, double* y, const double* p, const PcgScalars* sc,
+                      const uint32_t* act = nullptr);
 template <typename T>
 void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r, PcgScalars* sc, RedScratch rs,
                           double tol, int maxIT);
@@ -75,9 +76,10 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
 // x = omega*(r/d) + P(xc) + (omega*r)/d on present fine nodes; with dot: z.r
 // into sc (init: x1 = z.r; else beta = z.r/x1, x1 = z.r)
 template <typename TX, typename T, typename TD>
+// act: the fine grid's chunk mask (chunk_active), or null
 void launch_prolong_smooth(cudaStream_t st, int span, const TX* xc, Grid gc, const T* r, const TD* d,
                            const uint8_t* present, T* x, Grid gf, double omega, bool dot, bool init,
-                           PcgScalars* sc, RedScratch rs);
+                           PcgScalars* sc, RedScratch rs, const uint32_t* act = nullptr);
 // 'Standard' V-cycle (TX:758-763, 772-777): x = omega*(r/d) + P(xc) without the smoothing term;
 // x = omega*(r/d); q = r - q; x += omega*(r - q)/d (with dot: z.r into sc as above); coarse-level
 // K*u with the stored Galerkin matrices Ks (dense elements x 576).  All skip once sc->done.

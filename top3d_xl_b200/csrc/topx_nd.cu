@@ -484,9 +484,9 @@ __device__ __forceinline__ bool nd_backward_task(const NDSolveArgs<T, TM>& a, co
   const int64_t pout = d.pos0 + int64_t(ND_T) * i + threadIdx.x;
   const int32_t gi = has_in && u < d.n2 ? a.upd_dof[d.pos0 + P1 + u] : -1;
   const int32_t og = threadIdx.x < ND_T ? a.sep_dof[pout] : -1;
-  // dataflow: the parent's solution is complete (and with it every ancestor's)
+  // dataflow: the nearest eliminating ancestor's solution is complete (and with it every ancestor's)
   if (FLOW && threadIdx.x == 0)
-    sm.ok = d.bwd_need == 0 || coop_wait_count(fl->bwd_done + d.parent, unsigned(d.bwd_need), fl->ctl);
+    sm.ok = d.bwd_need == 0 || coop_wait_count(fl->bwd_done + d.bwd_front, unsigned(d.bwd_need), fl->ctl);
   __syncthreads();
   if (FLOW && !sm.ok) return false;
   if (has_in) sm.vec[threadIdx.x] = gi >= 0 ? double(__ldcg(a.x + gi)) : 0.0;

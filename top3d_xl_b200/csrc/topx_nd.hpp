@@ -40,9 +40,10 @@ struct NDFront {
   int scr0;       // first scratch tile while its level is swept: P^-1, then R_0 .. R_{N-1} of
                   // even steps and R_0 .. R_{N-1} of odd steps
   // dataflow solve: output tiles its children complete on the way up before its forward tasks
-  // may start (the sum of their N), and output tiles of its parent's solution (the parent's T1,
-  // 0 for a root) before its backward tasks may start
-  int fwd_need, bwd_need;
+  // may start (the sum of their N); and before its backward tasks may start, the solution tiles
+  // (bwd_need = its T1) of bwd_front, the nearest ancestor that eliminates DOFs (-1: none, need 0).
+  // Fronts between the two eliminate nothing, so that ancestor's solution implies all of theirs.
+  int fwd_need, bwd_need, bwd_front;
 };
 
 // A launch task: front f, tile row i, tile column j.

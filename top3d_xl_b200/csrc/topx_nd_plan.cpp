@@ -148,6 +148,7 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
       P.child_slot[size_t(f)] = h.slot;
       d.fwd_need = 0;
       d.bwd_need = 0;
+      d.bwd_front = -1;
     }
     L.pos_end = pos;
     L.nscr = scr;
@@ -157,10 +158,11 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
   P.npos = pos;
   for (int f = 0; f < nf; ++f) {
     NDFront& d = P.fronts[size_t(f)];
-    if (d.parent >= 0) {
-      P.fronts[size_t(d.parent)].fwd_need += d.N;
-      d.bwd_need = P.fronts[size_t(d.parent)].T1;
-    }
+    if (d.parent >= 0) P.fronts[size_t(d.parent)].fwd_need += d.N;
+    int a = d.parent;
+    while (a >= 0 && P.fronts[size_t(a)].T1 == 0) a = P.fronts[size_t(a)].parent;
+    d.bwd_front = a;
+    d.bwd_need = a >= 0 ? P.fronts[size_t(a)].T1 : 0;
   }
   P.upd_map.assign(size_t(map), -1);
   P.sep_dof.assign(size_t(pos), -1);
@@ -389,7 +391,12 @@ void nd_check_plan(const NDPlan& P) {
   for (int f = 0; f < nf; ++f) {
     const NDFront& d = P.fronts[size_t(f)];
     if (d.parent >= 0) need[size_t(d.parent)] += d.N;
-    if (d.bwd_need != (d.parent >= 0 ? P.fronts[size_t(d.parent)].T1 : 0)) fail("backward need of front " + std::to_string(f));
+    int a = d.parent;
+    while (a >= 0 && P.fronts[size_t(a)].T1 == 0) a = P.fronts[size_t(a)].parent;
+    if (d.bwd_front != a || d.bwd_need != (a >= 0 ? P.fronts[size_t(a)].T1 : 0))
+      fail("backward wait of front " + std::to_string(f));
+    if (a >= 0 && bwd_first[size_t(f)] >= 0 && P.fronts[size_t(a)].n2 > 0 && bwd_last[size_t(a)] >= bwd_first[size_t(f)])
+      fail("flow: a backward task before its ancestor's");
     if (d.parent < 0 || fwd_first[size_t(d.parent)] < 0) continue;
     if (fwd_last[size_t(f)] >= fwd_first[size_t(d.parent)]) fail("flow: a forward task before its child's");
     if (bwd_first[size_t(f)] >= 0 && bwd_last[size_t(d.parent)] >= bwd_first[size_t(f)])

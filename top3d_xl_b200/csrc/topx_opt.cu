@@ -30,11 +30,14 @@ template FilterKe<float> filter_ke<float>(const double*);
 
 // element -> node: node = sum over its hexes (local-node order) of src_e*(1/8)  (TOP3D_XL.m:880-886)
 template <typename T>
-__global__ void k_filter_e2n(Grid g, const T* __restrict__ srcE, T* __restrict__ node) {
-  const int64_t N = g.nnodes();
-  const int nny = g.ny + 1, nnx = g.nx + 1;
-  for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
-    const int gy = int(n % nny), gx = int((n / nny) % nnx), gz = int(n / (int64_t(nny) * nnx));
+__global__ void k_filter_e2n(Grid g, const T* __restrict__ srcE, T* __restrict__ node, FastDiv dny, FastDiv dnx,
+                             const uint32_t* __restrict__ act) {
+  const uint32_t N = uint32_t(g.nnodes());  // < 2^32 (checked at launch)
+  const uint32_t nny = uint32_t(g.ny + 1), nnx = uint32_t(g.nx + 1);
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    if (!chunk_active(act, n)) continue;  // no solid element around these nodes: zero
+    const uint32_t q = dny.div(n), qz = dnx.div(q);
+    const int gy = int(n - q * nny), gx = int(q - qz * nnx), gz = int(qz);
     T s = T(0);
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
@@ -46,8 +49,10 @@ __global__ void k_filter_e2n(Grid g, const T* __restrict__ srcE, T* __restrict__
   }
 }
 template <typename T>
-void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node) {
-  (k_filter_e2n<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, srcE, node), topx::count_launch());
+void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node, const uint32_t* act) {
+  if (g.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
+  const FastDiv dny{uint32_t(g.ny + 1)}, dnx{uint32_t(g.nx + 1)};
+  (k_filter_e2n<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, srcE, node, dny, dnx, act), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -82,12 +87,22 @@ constexpr int FKY = 32, FKX = 8, FNT = FKY * FKX;
 template <typename T, int MODE>
 __global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int zc, const FilterKe<T> kf, const T* __restrict__ in,
                                                     const T* __restrict__ zin, T* __restrict__ out,
-                                                    const uint8_t* __restrict__ solid, PcgScalars* sc, RedScratch rs) {
+                                                    const uint8_t* __restrict__ solid, PcgScalars* sc, RedScratch rs,
+                                                    const uint32_t* __restrict__ active) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T su[3][FKX + 2][FKY + 2];
   __shared__ T ss[2][FKX + 1][FKY + 1];
   const int nny = g.ny + 1, nnx = g.nx + 1, nnz = g.nz + 1;
-  const int y0 = blockIdx.x * FKY, x0 = blockIdx.y * FKX, zc0 = blockIdx.z * zc;
+  // the CTA's tile: blockIdx, or entry blockIdx.x of the list of tiles that own a node of the
+  // domain (y-tile | x-tile << 10 | z-chunk << 20)
+  int tyi = blockIdx.x, txi = blockIdx.y, tzi = blockIdx.z;
+  if (active) {
+    const uint32_t t = active[blockIdx.x];
+    tyi = int(t & 1023u);
+    txi = int((t >> 10) & 1023u);
+    tzi = int(t >> 20);
+  }
+  const int y0 = tyi * FKY, x0 = txi * FKX, zc0 = tzi * zc;
   const int ty = threadIdx.x, tx = threadIdx.y;
   const int tid = ty + FKY * tx;
   const bool first = (MODE != KU_PLAIN) && sc->first;
@@ -170,19 +185,52 @@ __global__ void __launch_bounds__(FNT) k_filter_ku(Grid g, int zc, const FilterK
   }
 }
 
+// tiles of 32 x 8 nodes, each a z-chunk of zc planes (aim at four CTAs per SM)
+struct FilterGeometry {
+  dim3 grd;
+  int zc;
+};
+static FilterGeometry filter_geometry(Grid g) {
+  const int tiles = ((g.nny() + FKY - 1) / FKY) * ((g.nnx() + FKX - 1) / FKX);
+  const int chunks = (148 * 4 + tiles - 1) / tiles;
+  FilterGeometry f;
+  f.zc = std::max(2, std::min(16, (g.nnz() + chunks - 1) / chunks));
+  f.grd = dim3((g.nny() + FKY - 1) / FKY, (g.nnx() + FKX - 1) / FKX, (g.nnz() + f.zc - 1) / f.zc);
+  return f;
+}
+
+std::vector<uint32_t> filter_active_tiles(Grid g, const std::vector<uint8_t>& present) {
+  const FilterGeometry f = filter_geometry(g);
+  const int nny = g.nny(), nnx = g.nnx(), nnz = g.nnz();
+  if (f.grd.x > 1024 || f.grd.y > 1024 || f.grd.z > 4095) return {};
+  std::vector<uint32_t> list;
+  for (unsigned tz = 0; tz < f.grd.z; ++tz)
+    for (unsigned tx = 0; tx < f.grd.y; ++tx)
+      for (unsigned ty = 0; ty < f.grd.x; ++ty) {
+        bool any = false;
+        for (int z = int(tz) * f.zc; z < std::min(nnz, int(tz + 1) * f.zc) && !any; ++z)
+          for (int x = int(tx) * FKX; x < std::min(nnx, int(tx + 1) * FKX) && !any; ++x)
+            for (int y = int(ty) * FKY; y < std::min(nny, int(ty + 1) * FKY) && !any; ++y)
+              any = present[size_t(y + int64_t(nny) * (x + int64_t(nnx) * z))] != 0;
+        if (any) list.push_back(ty | (tx << 10) | (tz << 20));
+      }
+  return list;
+}
+
 template <typename T>
 void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& kf, const T* in, const T* z, T* pout, T* out,
-                      const uint8_t* solid, PcgScalars* sc, RedScratch rs) {
+                      const uint8_t* solid, PcgScalars* sc, RedScratch rs, KuTiles tiles) {
   (void)pout;
-  const int tiles = ((g.nny() + FKY - 1) / FKY) * ((g.nnx() + FKX - 1) / FKX);
-  const int chunks = (148 * 4 + tiles - 1) / tiles;  // aim at four CTAs per SM
-  const int zc = std::max(2, std::min(16, (g.nnz() + chunks - 1) / chunks));
+  const FilterGeometry f = filter_geometry(g);
   dim3 blk(FKY, FKX, 1);
-  dim3 grd((g.nny() + FKY - 1) / FKY, (g.nnx() + FKX - 1) / FKX, (g.nnz() + zc - 1) / zc);
+  const dim3 grd = tiles.list ? dim3(unsigned(tiles.n)) : f.grd;
+  if (grd.x == 0) return;
   if (mode == KU_PLAIN)
-    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, zc, kf, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_PLAIN><<<grd, blk, 0, st>>>(g, f.zc, kf, in, z, out, solid, sc, rs, tiles.list),
+     topx::count_launch());
   else
-    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, zc, kf, in, z, out, solid, sc, rs), topx::count_launch());
+    (k_filter_ku<T, KU_P_UPDATE><<<grd, blk, 0, st>>>(g, f.zc, kf, in, z, out, solid, sc, rs, tiles.list),
+     topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -190,10 +238,11 @@ void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& k
 template <typename T>
 __global__ void k_filter_init(Grid g, const T* __restrict__ b, const T* __restrict__ dp, T* __restrict__ r,
                               T* __restrict__ z, T* __restrict__ y, PcgScalars* sc, RedScratch rs, double tol,
-                              int maxIT) {
+                              int maxIT, const uint32_t* __restrict__ act) {
   const int64_t N = g.nnodes();
   double bb = 0.0, zr = 0.0;
   for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    if (!chunk_active(act, n)) continue;  // zero there and stays so
     const T bv = b[n];
     const T zv = dp[n] * bv;
     r[n] = bv;
@@ -216,8 +265,9 @@ __global__ void k_filter_init(Grid g, const T* __restrict__ b, const T* __restri
 }
 template <typename T>
 void launch_filter_residual_init(cudaStream_t st, Grid g, const T* b, const T* dp, T* r, T* z, T* y, PcgScalars* sc,
-                                 RedScratch rs, double tol, int maxIT) {
-  (k_filter_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, dp, r, z, y, sc, rs, tol, maxIT), topx::count_launch());
+                                 RedScratch rs, double tol, int maxIT, const uint32_t* act) {
+  (k_filter_init<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, b, dp, r, z, y, sc, rs, tol, maxIT, act),
+   topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -225,7 +275,7 @@ void launch_filter_residual_init(cudaStream_t st, Grid g, const T* b, const T* d
 template <typename T>
 __global__ void k_filter_update(Grid g, T* __restrict__ y, T* __restrict__ p, T* __restrict__ r,
                                 const T* __restrict__ q, const T* __restrict__ dp, T* __restrict__ z, PcgScalars* sc,
-                                RedScratch rs) {
+                                RedScratch rs, const uint32_t* __restrict__ act) {
   if (sc->done) return;
   const bool first = sc->first;
   const T beta = T(sc->beta);
@@ -234,6 +284,7 @@ __global__ void k_filter_update(Grid g, T* __restrict__ y, T* __restrict__ p, T*
   const int64_t N = g.nnodes();
   double rr = 0.0, zr = 0.0;
   for (int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; n < N; n += int64_t(gridDim.x) * blockDim.x) {
+    if (!chunk_active(act, n)) continue;  // zero there and stays so
     const T pv = first ? z[n] : z[n] + beta * p[n];
     p[n] = pv;
     y[n] = y[n] + lamT * pv;
@@ -262,8 +313,8 @@ __global__ void k_filter_update(Grid g, T* __restrict__ y, T* __restrict__ p, T*
 }
 template <typename T>
 void launch_filter_update(cudaStream_t st, Grid g, T* y, T* p, T* r, const T* q, const T* dp, T* z, PcgScalars* sc,
-                          RedScratch rs) {
-  (k_filter_update<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, r, q, dp, z, sc, rs), topx::count_launch());
+                          RedScratch rs, const uint32_t* act) {
+  (k_filter_update<T><<<grid1d(g.nnodes(), 256), 256, 0, st>>>(g, y, p, r, q, dp, z, sc, rs, act), topx::count_launch());
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
@@ -507,22 +558,22 @@ void launch_oc_final(cudaStream_t st, int64_t Ne, double* x, const double* w, co
   TOPX_CUDA_OK(cudaGetLastError());
 }
 
-template void launch_filter_e2n<double>(cudaStream_t, Grid, const double*, double*);
-template void launch_filter_e2n<float>(cudaStream_t, Grid, const float*, float*);
+template void launch_filter_e2n<double>(cudaStream_t, Grid, const double*, double*, const uint32_t*);
+template void launch_filter_e2n<float>(cudaStream_t, Grid, const float*, float*, const uint32_t*);
 template void launch_filter_diag<double>(cudaStream_t, Grid, const uint8_t*, const FilterKe<double>&, double*);
 template void launch_filter_diag<float>(cudaStream_t, Grid, const uint8_t*, const FilterKe<double>&, float*);
 template void launch_filter_ku<double>(cudaStream_t, KuMode, Grid, const FilterKe<double>&, const double*, const double*, double*, double*,
-                                       const uint8_t*, PcgScalars*, RedScratch);
+                                       const uint8_t*, PcgScalars*, RedScratch, KuTiles);
 template void launch_filter_ku<float>(cudaStream_t, KuMode, Grid, const FilterKe<float>&, const float*, const float*, float*, float*,
-                                      const uint8_t*, PcgScalars*, RedScratch);
+                                      const uint8_t*, PcgScalars*, RedScratch, KuTiles);
 template void launch_filter_residual_init<double>(cudaStream_t, Grid, const double*, const double*, double*, double*,
-                                                  double*, PcgScalars*, RedScratch, double, int);
+                                                  double*, PcgScalars*, RedScratch, double, int, const uint32_t*);
 template void launch_filter_residual_init<float>(cudaStream_t, Grid, const float*, const float*, float*, float*,
-                                                 float*, PcgScalars*, RedScratch, double, int);
+                                                 float*, PcgScalars*, RedScratch, double, int, const uint32_t*);
 template void launch_filter_update<double>(cudaStream_t, Grid, double*, double*, double*, const double*,
-                                           const double*, double*, PcgScalars*, RedScratch);
+                                           const double*, double*, PcgScalars*, RedScratch, const uint32_t*);
 template void launch_filter_update<float>(cudaStream_t, Grid, float*, float*, float*, const float*, const float*,
-                                          float*, PcgScalars*, RedScratch);
+                                          float*, PcgScalars*, RedScratch, const uint32_t*);
 template void launch_filter_n2e<double>(cudaStream_t, Grid, const double*, const int32_t*, int64_t, double*);
 template void launch_filter_n2e<float>(cudaStream_t, Grid, const float*, const int32_t*, int64_t, double*);
 template void launch_scatter_elems_t<double>(cudaStream_t, const double*, const int32_t*, int64_t, double*);

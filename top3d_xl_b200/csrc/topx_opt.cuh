@@ -28,18 +28,20 @@ struct FilterKe {
 template <typename T>
 FilterKe<T> filter_ke(const double* KF64);
 template <typename T>
-void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node);
+void launch_filter_e2n(cudaStream_t st, Grid g, const T* srcE, T* node, const uint32_t* act = nullptr);
 template <typename T>
 void launch_filter_diag(cudaStream_t st, Grid g, const uint8_t* solid, const FilterKe<double>& kf, T* dp);
 template <typename T>
 void launch_filter_ku(cudaStream_t st, KuMode mode, Grid g, const FilterKe<T>& kf, const T* in, const T* z, T* pout,
-                      T* out, const uint8_t* solid, PcgScalars* sc, RedScratch rs);
+                      T* out, const uint8_t* solid, PcgScalars* sc, RedScratch rs, KuTiles tiles = KuTiles{});
+// tiles of the filter's K*u launch that own a node of the domain (a null list launches them all)
+std::vector<uint32_t> filter_active_tiles(Grid g, const std::vector<uint8_t>& present);
 template <typename T>
 void launch_filter_residual_init(cudaStream_t st, Grid g, const T* b, const T* dp, T* r, T* z, T* y, PcgScalars* sc,
-                                 RedScratch rs, double tol, int maxIT);
+                                 RedScratch rs, double tol, int maxIT, const uint32_t* act = nullptr);
 template <typename T>
 void launch_filter_update(cudaStream_t st, Grid g, T* y, T* p, T* r, const T* q, const T* dp, T* z, PcgScalars* sc,
-                          RedScratch rs);
+                          RedScratch rs, const uint32_t* act = nullptr);
 template <typename T>
 void launch_filter_n2e(cudaStream_t st, Grid g, const T* node, const int32_t* eleMapBack0, int64_t Ne, double* out);
 template <typename T>
