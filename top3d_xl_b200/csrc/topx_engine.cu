@@ -190,7 +190,10 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     const size_t full = ku_active_tiles(G[0], all).size();
     if (!act.empty() && act.size() < full * 9 / 10) {
       kuTiles.upload(act.data(), act.size());
-      kut = KuTiles{kuTiles.p, int(act.size())};
+      // an empty row list (no present node on the row y = ny) launches no last-row kernel
+      const std::vector<uint32_t> rows = ku_active_row_tiles(G[0], pn);
+      if (!rows.empty()) kuRows.upload(rows.data(), rows.size());
+      kut = KuTiles{kuTiles.p, int(act.size()), rows.empty() ? kuTiles.p : kuRows.p, int(rows.size())};
     }
     const std::vector<uint32_t> fact = filter_active_tiles(G[0], pn);
     if (!fact.empty() && fact.size() < filter_active_tiles(G[0], all).size() * 9 / 10) {
@@ -212,6 +215,22 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
     if (nact < nchunk * 9 / 10) {
       act1Mask.upload(mask.data(), mask.size());
       act1 = act1Mask.p;
+    }
+    // the level-1 restriction's y pass skips (x, z) columns without a present node
+    const int64_t ncol = int64_t(G[0].nnx()) * G[0].nnz(), nny1 = G[0].nny();
+    std::vector<uint32_t> cm(size_t((ncol + 31) / 32), 0u);
+    int64_t ncact = 0;
+    for (int64_t q = 0; q < ncol; ++q) {
+      bool any = false;
+      for (int64_t y = 0; y < nny1 && !any; ++y) any = pn[size_t(y + nny1 * q)] != 0;
+      if (any) {
+        cm[size_t(q / 32)] |= 1u << (q % 32);
+        ++ncact;
+      }
+    }
+    if (ncact < ncol * 9 / 10) {
+      cols1Mask.upload(cm.data(), cm.size());
+      cols1 = cols1Mask.p;
     }
   }
   // ---- coarsest level: nested-dissection plan and factor storage -----------------
@@ -516,7 +535,7 @@ void Engine::factor_coarsest() {
 template <typename TC>
 void Engine::vcycle_t(VWork<TC>& v, bool init, PcgScalars* sc) {
   sec_begin(SEC_RESTRICT);
-  launch_restrict<double, TC>(st, M.levels[1].span, kw.r.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
+  launch_restrict<double, TC>(st, M.levels[1].span, kw.r.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1], cols1);
   for (int l = 2; l < nl; ++l)
     launch_restrict<TC, TC>(st, M.levels[l].span, v.rl[l - 1].p, G[l - 1], v.tmp1.p, v.tmp2.p, v.rl[l].p, G[l]);
   sec_end();
@@ -549,7 +568,7 @@ void Engine::vcycle_standard(bool init, PcgScalars* sc) {
   launch_jacobi_pre<double, double, double>(st, G[0], kw.r.p, v.d1.p, present[0].p, kw.z.p, om, sc);
   launch_ku<double>(st, KU_PLAIN, G[0], kw.z.p, nullptr, nullptr, kw.q.p, E64.p, fixbits.p, cfix64.p, sc, rs1, kut);
   launch_residual_inplace<double, double>(st, G[0], kw.r.p, kw.q.p, sc);
-  launch_restrict<double, double>(st, M.levels[1].span, kw.q.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1]);
+  launch_restrict<double, double>(st, M.levels[1].span, kw.q.p, G[0], v.tmp1.p, v.tmp2.p, v.rl[1].p, G[1], cols1);
   for (int l = 1; l < nl - 1; ++l) {
     launch_jacobi_pre<double, double, double>(st, G[l], v.rl[l].p, v.dl[l].p, present[l].p, v.xl[l].p, om, sc);
     launch_ku_coarse(st, G[l], Ks[l].p, epresent[l].p, present[l].p, v.xl[l].p, vq[l].p, sc);

@@ -214,11 +214,14 @@ class Engine {
   DevBuf<double> fl_F;
   int nflag = 0;
   DevBuf<uint32_t> kuTiles;  // level-1 K*u tiles that own a node of the domain
+  DevBuf<uint32_t> kuRows;   // and the last-row kernel's tiles that hold one of the row y = ny
   KuTiles kut;               // their list (null: the whole grid)
   DevBuf<uint32_t> filterTiles;  // the same for the filter's K*u (its own z-chunks)
   KuTiles fut;
   DevBuf<uint32_t> act1Mask;     // level-1 chunk mask (chunk_active) of an irregular domain
   const uint32_t* act1 = nullptr;  // null: every chunk holds a present node
+  DevBuf<uint32_t> cols1Mask;      // level-1 (x, z) columns that hold a present node
+  const uint32_t* cols1 = nullptr;
   // coarsest level: nested-dissection plan, its device copy and the factor tiles
   NDPlan nd;
   NDDevice ndd;

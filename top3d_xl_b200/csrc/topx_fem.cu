@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __
                                                              T* __restrict__ pout, T* __restrict__ out,
                                                              const T* __restrict__ E, const uint8_t* __restrict__ fixbits,
                                                              const T* __restrict__ cfix, PcgScalars* sc, RedScratch rs,
-                                                             double* __restrict__ yacc) {
+                                                             double* __restrict__ yacc, const uint32_t* __restrict__ rows) {
   if (MODE != KU_PLAIN && sc->done) return;
   __shared__ T sp[3][KLZ + 2][KLX + 2][2];  // masked values, [comp][z][x][row y = ny - 1, ny]
   __shared__ T se[KLZ + 1][KLX + 1];        // moduli of element row ny - 1
@@ -431,7 +431,12 @@ __global__ void __launch_bounds__(KLX * KLZ) k_ku_l1_lastrow(Grid g, const T* __
   const bool ystep = MODE != KU_PLAIN && yacc && !first;
   const double lam = ystep ? sc->lam : 0.0;
   const int Y = nny - 1;
-  const int x0 = blockIdx.x * KLX, z0 = blockIdx.y * KLZ;
+  int bx = blockIdx.x, bz = blockIdx.y;
+  if (rows) {  // entry blockIdx.x of the tiles that hold a present node of the row
+    bx = int(rows[blockIdx.x] & 0xffffu);
+    bz = int(rows[blockIdx.x] >> 16);
+  }
+  const int x0 = bx * KLX, z0 = bz * KLZ;
   const int tid = threadIdx.x;
   // stage: position i -> row (i & 1), halo x and z; the two rows of one (x, z) are adjacent in memory
   constexpr int NPOS = 2 * (KLX + 2) * (KLZ + 2);
@@ -582,6 +587,22 @@ std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& presen
   return list;
 }
 
+std::vector<uint32_t> ku_active_row_tiles(Grid g, const std::vector<uint8_t>& present) {
+  const KuGeometry k = ku_geometry(g);
+  std::vector<uint32_t> list;
+  if (!k.lastrow) return list;
+  const int nny = g.nny(), nnx = g.nnx(), nnz = g.nnz(), Y = nny - 1;
+  for (int bz = 0; bz < (nnz + KLZ - 1) / KLZ; ++bz)
+    for (int bx = 0; bx < (nnx + KLX - 1) / KLX; ++bx) {
+      bool any = false;
+      for (int z = bz * KLZ; z < std::min(nnz, (bz + 1) * KLZ) && !any; ++z)
+        for (int x = bx * KLX; x < std::min(nnx, (bx + 1) * KLX) && !any; ++x)
+          any = present[size_t(Y + int64_t(nny) * (x + int64_t(nnx) * z))] != 0;
+      if (any) list.push_back(uint32_t(bx) | (uint32_t(bz) << 16));
+    }
+  return list;
+}
+
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles, double* yacc) {
@@ -601,13 +622,14 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
     (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, sizeof(KuSmem<T, KU_P_UPDATE>), st>>>(g, zc, in, z, pout, out, E, fixbits,
                                                                              cfix, sc, rs, tiles.list, yacc),
      topx::count_launch());
-  if (lastrow) {
-    const dim3 nb((g.nnx() + KLX - 1) / KLX, (g.nnz() + KLZ - 1) / KLZ);
+  if (lastrow && !(tiles.list && tiles.rows && tiles.nrows == 0)) {
+    const uint32_t* rows = tiles.list ? tiles.rows : nullptr;
+    const dim3 nb = rows ? dim3(unsigned(tiles.nrows)) : dim3((g.nnx() + KLX - 1) / KLX, (g.nnz() + KLZ - 1) / KLZ);
     if (mode == KU_PLAIN)
-      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc),
+      (k_ku_l1_lastrow<T, KU_PLAIN><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc, rows),
        topx::count_launch());
     else
-      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc),
+      (k_ku_l1_lastrow<T, KU_P_UPDATE><<<nb, KLX * KLZ, 0, st>>>(g, in, z, pout, out, E, fixbits, cfix, sc, rs, yacc, rows),
        topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
@@ -799,12 +821,19 @@ void launch_pcg_update(cudaStream_t st, Grid g, TY* y, const T* z, T* p, T* r, c
 template <typename TI, typename T, int S, int AXIS>
 __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny, int inx, int inz,
                                 T* __restrict__ out, int64_t ostr, int ony, int onx, int onz, FastDiv fdy,
-                                FastDiv fdx) {
+                                FastDiv fdx, const uint32_t* __restrict__ cols) {
   const uint32_t N = uint32_t(ony) * onx * onz;
   for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
     const uint32_t q = fdy.div(n), oz = fdx.div(q);
     const int oy = int(n - q * uint32_t(ony)), ox = int(q - oz * uint32_t(onx));
     T acc[3] = {T(0), T(0), T(0)};
+    // y pass with a column mask: an input (x, z) column without a present node is zero, and so
+    // is the output (written without reading the column)
+    if (AXIS == 0 && cols && ((__ldg(cols + (q >> 5)) >> (q & 31)) & 1u) == 0u) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) out[n + c * ostr] = T(0);
+      continue;
+    }
 #pragma unroll
     for (int d = -(S - 1); d <= S - 1; ++d) {
       int iy = oy, ix = ox, iz = int(oz);
@@ -832,22 +861,23 @@ __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny
 }
 
 template <typename TI, typename T>
-void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc) {
+void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc,
+                     const uint32_t* cols) {
   const int fy = gf.nny(), fx = gf.nnx(), fz = gf.nnz();
   const int cy = gc.nny(), cx = gc.nnx(), cz = gc.nnz();
   const int64_t s1 = int64_t(cy) * fx * fz, s2 = int64_t(cy) * cx * fz;
   if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
   const FastDiv dcy{uint32_t(cy)}, dfx{uint32_t(fx)}, dcx{uint32_t(cx)};
   if (span == 4) {
-    (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx), topx::count_launch());
-    (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx), topx::count_launch());
+    (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx, cols), topx::count_launch());
+    (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
     (k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz, dcy, dcx), topx::count_launch());
+                                                                             cx, cz, dcy, dcx, nullptr), topx::count_launch());
   } else {
-    (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx), topx::count_launch());
-    (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx), topx::count_launch());
+    (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx, cols), topx::count_launch());
+    (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
     (k_restrict_axis<T, T, 2, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
-                                                                             cx, cz, dcy, dcx), topx::count_launch());
+                                                                             cx, cz, dcy, dcx, nullptr), topx::count_launch());
   }
   TOPX_CUDA_OK(cudaGetLastError());
 }
@@ -1215,7 +1245,7 @@ void launch_unit_compliance(cudaStream_t st, Grid g, const double* U, const int3
   template void launch_diag_l1<T, T>(cudaStream_t, Grid, const T*, const uint8_t*, const T*, const uint8_t*, T*); \
   template void launch_residual_init<T>(cudaStream_t, Grid, const T*, const T*, T*, PcgScalars*, RedScratch,     \
                                         double, int);                                                            \
-  template void launch_restrict<T, T>(cudaStream_t, int, const T*, Grid, T*, T*, T*, Grid);                      \
+  template void launch_restrict<T, T>(cudaStream_t, int, const T*, Grid, T*, T*, T*, Grid, const uint32_t*);     \
   template void launch_prolong_smooth<T, T, T>(cudaStream_t, int, const T*, Grid, const T*, const T*,            \
                                                const uint8_t*, T*, Grid, double, bool, bool, PcgScalars*,        \
                                                RedScratch, const uint32_t*);                                     \
@@ -1229,7 +1259,8 @@ template void launch_pcg_update<float, float>(cudaStream_t, Grid, float*, const 
                                               PcgScalars*, RedScratch, const uint32_t*);
 template void launch_diag_l1<double, float>(cudaStream_t, Grid, const double*, const uint8_t*, const double*,
                                            const uint8_t*, float*);
-template void launch_restrict<double, float>(cudaStream_t, int, const double*, Grid, float*, float*, float*, Grid);
+template void launch_restrict<double, float>(cudaStream_t, int, const double*, Grid, float*, float*, float*, Grid,
+                                             const uint32_t*);
 template void launch_prolong_smooth<float, double, float>(cudaStream_t, int, const float*, Grid, const double*,
                                                           const float*, const uint8_t*, double*, Grid, double, bool,
                                                           bool, PcgScalars*, RedScratch, const uint32_t*);

@@ -49,8 +49,13 @@ void upload_ke(const double* Ke576);
 struct KuTiles {
   const uint32_t* list = nullptr;
   int n = 0;
+  // the last-row kernel's (x, z) tiles that hold a present node of the row y = ny (x | z << 16);
+  // used when list is given (non-null with nrows = 0: no last-row launch)
+  const uint32_t* rows = nullptr;
+  int nrows = 0;
 };
 std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present);
+std::vector<uint32_t> ku_active_row_tiles(Grid g, const std::vector<uint8_t>& present);
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
                const uint8_t* fixbits, const T* cfix, PcgScalars* sc, RedScratch rs, KuTiles tiles = KuTiles{},
@@ -72,7 +77,9 @@ void launch_residual_init(cudaStream_t st, Grid g, const T* b, const T* Ay, T* r
                           double tol, int maxIT);
 // --- transfers -----------------------------------------------------------
 template <typename TI, typename T>
-void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc);
+// cols: bit q set when the fine grid's (x, z) column q = x + nnx z holds a present node (null: all)
+void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc,
+                     const uint32_t* cols = nullptr);
 // x = omega*(r/d) + P(xc) + (omega*r)/d on present fine nodes; with dot: z.r
 // into sc (init: x1 = z.r; else beta = z.r/x1, x1 = z.r)
 template <typename TX, typename T, typename TD>
