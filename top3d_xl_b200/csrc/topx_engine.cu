@@ -185,7 +185,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
   {
     std::vector<uint8_t> pn(size_t(G[0].nnodes()), 0);
     for (auto k : M.levels[0].nodMapBack) pn[k - 1] = 1;
-    const std::vector<uint32_t> act = ku_active_tiles(G[0], pn);
+    std::vector<uint32_t> zr;
+    const std::vector<uint32_t> act = ku_active_tiles(G[0], pn, &zr);
     const std::vector<uint8_t> all(pn.size(), 1);
     const size_t full = ku_active_tiles(G[0], all).size();
     if (!act.empty() && act.size() < full * 9 / 10) {
@@ -193,7 +194,8 @@ Engine::Engine(Model& model, int precision, int device, bool coarse_coop) : M(mo
       // an empty row list (no present node on the row y = ny) launches no last-row kernel
       const std::vector<uint32_t> rows = ku_active_row_tiles(G[0], pn);
       if (!rows.empty()) kuRows.upload(rows.data(), rows.size());
-      kut = KuTiles{kuTiles.p, int(act.size()), rows.empty() ? kuTiles.p : kuRows.p, int(rows.size())};
+      kuZr.upload(zr.data(), zr.size());
+      kut = KuTiles{kuTiles.p, int(act.size()), rows.empty() ? kuTiles.p : kuRows.p, int(rows.size()), kuZr.p};
     }
     const std::vector<uint32_t> fact = filter_active_tiles(G[0], pn);
     if (!fact.empty() && fact.size() < filter_active_tiles(G[0], all).size() * 9 / 10) {

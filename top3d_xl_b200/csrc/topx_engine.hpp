@@ -215,6 +215,7 @@ class Engine {
   int nflag = 0;
   DevBuf<uint32_t> kuTiles;  // level-1 K*u tiles that own a node of the domain
   DevBuf<uint32_t> kuRows;   // and the last-row kernel's tiles that hold one of the row y = ny
+  DevBuf<uint32_t> kuZr;     // per listed tile, its planes that hold a present node
   KuTiles kut;               // their list (null: the whole grid)
   DevBuf<uint32_t> filterTiles;  // the same for the filter's K*u (its own z-chunks)
   KuTiles fut;

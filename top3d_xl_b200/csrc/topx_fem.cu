@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
                                                   T* __restrict__ pout, T* __restrict__ out, const T* __restrict__ E,
                                                   const uint8_t* __restrict__ fixbits, const T* __restrict__ cfix,
                                                   PcgScalars* sc, RedScratch rs, const uint32_t* __restrict__ active,
-                                                  double* __restrict__ yacc) {
+                                                  double* __restrict__ yacc, const uint32_t* __restrict__ zr) {
   if (MODE != KU_PLAIN && sc->done) return;
   extern __shared__ __align__(16) unsigned char ku_dyn_smem[];
   KuSmem<T, MODE>& sm = *reinterpret_cast<KuSmem<T, MODE>*>(ku_dyn_smem);
@@ -237,8 +237,13 @@ __global__ void __launch_bounds__(KNT, 3) k_ku_l1(Grid g, int zc, const T* __res
   const int64_t S = g.stride;
   int tyi, txi, tzi;
   ku_tile(active, tyi, txi, tzi);
-  const int y0 = tyi * KY, x0 = txi * KX, zc0 = tzi * zc;
-  const int zend = min(zc0 + zc, nnz);
+  const int y0 = tyi * KY, x0 = txi * KX;
+  int zc0 = tzi * zc, zend = min(zc0 + zc, nnz);
+  if (active && zr) {  // only the planes of the chunk that hold a present node
+    const uint32_t r = zr[blockIdx.x];
+    zc0 = int(r & 0xffffu);
+    zend = int(r >> 16);
+  }
   const int ty = threadIdx.x, tx = threadIdx.y;
   const int tid = ty + KY * tx;
   const bool first = (MODE != KU_PLAIN) && sc->first;
@@ -569,20 +574,30 @@ static KuGeometry ku_geometry(Grid g) {
   return k;
 }
 
-std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present) {
+std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present, std::vector<uint32_t>* zranges) {
   const KuGeometry k = ku_geometry(g);
   const int nny = g.nny(), nnx = g.nnx(), nnz = g.nnz();
-  if (k.grd.x > 1024 || k.grd.y > 1024 || k.grd.z > 4095) return {};
+  if (k.grd.x > 1024 || k.grd.y > 1024 || k.grd.z > 4095 || nnz > 65535) return {};
   std::vector<uint32_t> list;
+  if (zranges) zranges->clear();
   for (unsigned tz = 0; tz < k.grd.z; ++tz)
     for (unsigned tx = 0; tx < k.grd.y; ++tx)
       for (unsigned ty = 0; ty < k.grd.x; ++ty) {
-        bool any = false;
-        for (int z = int(tz) * k.zc; z < std::min(nnz, int(tz + 1) * k.zc) && !any; ++z)
+        int lo = -1, hi = -1;
+        for (int z = int(tz) * k.zc; z < std::min(nnz, int(tz + 1) * k.zc); ++z) {
+          bool any = false;
           for (int x = int(tx) * KX; x < std::min(nnx, int(tx + 1) * KX) && !any; ++x)
             for (int y = int(ty) * KY; y < std::min(k.rows, int(ty + 1) * KY) && !any; ++y)
               any = present[size_t(y + int64_t(nny) * (x + int64_t(nnx) * z))] != 0;
-        if (any) list.push_back(ty | (tx << 10) | (tz << 20));
+          if (any) {
+            if (lo < 0) lo = z;
+            hi = z + 1;
+          }
+        }
+        if (lo >= 0) {
+          list.push_back(ty | (tx << 10) | (tz << 20));
+          if (zranges) zranges->push_back(uint32_t(lo) | (uint32_t(hi) << 16));
+        }
       }
   return list;
 }
@@ -616,11 +631,11 @@ void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T*
   if (grd.x == 0) {
   } else if (mode == KU_PLAIN)
     (k_ku_l1<T, KU_PLAIN><<<grd, blk, sizeof(KuSmem<T, KU_PLAIN>), st>>>(g, zc, in, z, pout, out, E, fixbits, cfix,
-                                                                       sc, rs, tiles.list, yacc),
+                                                                       sc, rs, tiles.list, yacc, tiles.zr),
      topx::count_launch());
   else
     (k_ku_l1<T, KU_P_UPDATE><<<grd, blk, sizeof(KuSmem<T, KU_P_UPDATE>), st>>>(g, zc, in, z, pout, out, E, fixbits,
-                                                                             cfix, sc, rs, tiles.list, yacc),
+                                                                             cfix, sc, rs, tiles.list, yacc, tiles.zr),
      topx::count_launch());
   if (lastrow && !(tiles.list && tiles.rows && tiles.nrows == 0)) {
     const uint32_t* rows = tiles.list ? tiles.rows : nullptr;

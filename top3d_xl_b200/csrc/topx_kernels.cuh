@@ -53,8 +53,13 @@ struct KuTiles {
   // used when list is given (non-null with nrows = 0: no last-row launch)
   const uint32_t* rows = nullptr;
   int nrows = 0;
+  // per listed tile, the planes [lo, hi) of its z-chunk that hold a present node (lo | hi << 16);
+  // the tile kernel marches only those (null: the whole chunk)
+  const uint32_t* zr = nullptr;
 };
-std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present);
+// zranges (optional): the z-range entry of each listed tile
+std::vector<uint32_t> ku_active_tiles(Grid g, const std::vector<uint8_t>& present,
+                                      std::vector<uint32_t>* zranges = nullptr);
 std::vector<uint32_t> ku_active_row_tiles(Grid g, const std::vector<uint8_t>& present);
 template <typename T>
 void launch_ku(cudaStream_t st, KuMode mode, Grid g, const T* in, const T* z, T* pout, T* out, const T* E,
