@@ -18,11 +18,19 @@ def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
 
-@pytest.fixture(scope="module", params=["cuboid", "irregular"])
+@pytest.fixture(scope="module", params=["cuboid", "irregular", "u_shape"])
 def setup(request):
+    # u_shape: most (x, z) columns are void, so the level-1 passes run over the domain's tiles
+    # and chunks only: K*u tiles with part of their z-chunk present, the last-row kernel's row
+    # tiles (ny = 32), the filter's tiles, the restriction's column mask
     from top3d_xl_b200 import Context
     if request.param == "cuboid":
         vox = np.ones((12, 24, 12), bool)
+    elif request.param == "u_shape":
+        vox = np.zeros((32, 64, 32), bool)
+        vox[:, :4, :] = True
+        vox[:, -4:, :] = True
+        vox[:, :, :4] = True
     else:
         rng = np.random.default_rng(5)
         vox = rng.random((13, 27, 11)) < 0.75
@@ -39,7 +47,7 @@ def setup(request):
     sol.assemble(E)
     ctx.set_moduli(E)
     ctx.assemble()
-    yield dict(m=m, ctx=ctx, sol=sol, E=E, x=x, vox=vox)
+    yield dict(m=m, ctx=ctx, sol=sol, E=E, x=x, vox=vox, kind=request.param)
     ctx.close()
 
 
@@ -59,7 +67,10 @@ def test_diagonals(setup):
 def test_vcycle(setup):
     m, ctx, sol = setup["m"], setup["ctx"], setup["sol"]
     r = np.random.default_rng(3).standard_normal(m.levels[0].numDOFs)
-    assert _rel(ctx.vcycle(r), sol.vcycle(r)) < 1e-11
+    # the U's prongs are cantilevers: its coarsest matrix is ill-conditioned (the V-cycle of a unit
+    # residual reaches 1e4), and the two factorisations' rounding differs by that much more
+    bar = 1e-10 if setup["kind"] == "u_shape" else 1e-11
+    assert _rel(ctx.vcycle(r), sol.vcycle(r)) < bar
 
 
 def test_pcg(setup):
@@ -69,6 +80,12 @@ def test_pcg(setup):
     u, its = ctx.pcg()
     uo, itso, _ = O.pcg(sol.ku, sol.vcycle, m.F[:, 0], m.S.tol, m.S.maxIT)
     f = m.F[:, 0]
+    if setup["kind"] == "u_shape":
+        # 88 iterations of a tol-1e-3 PCG on the ill-conditioned U: the stopping test may fall one
+        # iteration apart, and the solutions then differ by that last step
+        assert abs(its - itso) <= 1
+        assert abs(f @ u - f @ uo) / abs(f @ uo) < 1e-5
+        return
     assert its == itso
     assert _rel(u, uo) < 1e-6
     assert abs(f @ u - f @ uo) / abs(f @ uo) < 1e-8
