@@ -266,12 +266,22 @@ NDPlan nd_plan(int nny, int nnx, int nnz, int64_t stride, const std::vector<uint
               if (j != k - 1) add(f, k - 1, j);
         }
       L.step.push_back(int64_t(P.tasks.size()));
+      // the tiles whose CTA then inverts the next pivot go first: the longest tasks of the launch
+      // start in its first wave instead of lengthening its tail
+      auto next_pivot = [&](const NDFront& d, int i, int j) { return i == k + 1 && j == k + 1 && k + 1 < d.T1; };
+      for (int f : L.fronts) {
+        const NDFront& d = P.fronts[size_t(f)];
+        if (d.T1 > k + 1) {
+          add(f, k + 1, k + 1);
+          P.flops += tile_flops;
+        }
+      }
       for (int f : L.fronts) {
         const NDFront& d = P.fronts[size_t(f)];
         if (d.T1 > k)
           for (int i = 0; i < d.N; ++i)
             for (int j = 0; j <= i; ++j)
-              if (i != k && j != k) {
+              if (i != k && j != k && !next_pivot(d, i, j)) {
                 add(f, i, j);
                 P.flops += tile_flops;
               }
