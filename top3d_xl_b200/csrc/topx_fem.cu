@@ -1234,13 +1234,14 @@ __global__ void k_unit_compliance(Grid g, const double* __restrict__ U, const in
 #pragma unroll
       for (int c = 0; c < 3; ++c) u[3 * a + c] = U[n + c * g.stride];
     }
+    // Ke is symmetric: u^T Ke u = sum_j u_j (Ke_jj u_j + 2 sum_{i<j} Ke_ij u_i), 324 FMA for 600
     double s = 0.0;
 #pragma unroll
     for (int j = 0; j < 24; ++j) {
-      double v = 0.0;
+      double t = 0.0;
 #pragma unroll
-      for (int i = 0; i < 24; ++i) v = fma(u[i], c_Ke64[i * 24 + j], v);
-      s = fma(v, u[j], s);
+      for (int i = 0; i < j; ++i) t = fma(u[i], c_Ke64[i * 24 + j], t);
+      s = fma(u[j], fma(2.0, t, c_Ke64[j * 24 + j] * u[j]), s);
     }
     ce[e] = acc ? ce[e] + w * s : w * s;
   }
