@@ -875,6 +875,50 @@ __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny
   }
 }
 
+// The span-2 restriction in one pass: each coarse node sums its 3 x 3 x 3 fine taps as the three
+// axis passes would (y sums, then x sums of those, then z sums, each in the pass's element type
+// and tap order), so the result is the same bit for bit, with one launch instead of three.
+template <typename TI, typename T>
+__global__ void k_restrict_span2(const TI* __restrict__ in, int64_t istr, int iny, int inx, int inz,
+                                 T* __restrict__ out, int64_t ostr, int ony, int onx, int onz, FastDiv fdy,
+                                 FastDiv fdx) {
+  const uint32_t N = uint32_t(ony) * onx * onz;
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    const uint32_t q = fdy.div(n), oz = fdx.div(q);
+    const int oy = int(n - q * uint32_t(ony)), ox = int(q - oz * uint32_t(onx));
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int iz = 2 * int(oz) + dz;
+      if (iz < 0 || iz >= inz) continue;
+      T t2[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int ix = 2 * ox + dx;
+        if (ix < 0 || ix >= inx) continue;
+        T t1[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int iy = 2 * oy + dy;
+          if (iy < 0 || iy >= iny) continue;
+          const T wy = T(2 - (dy < 0 ? -dy : dy)) / T(2);
+          const int64_t k = iy + int64_t(iny) * (ix + int64_t(inx) * iz);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) t1[c] = fma(wy, T(in[k + c * istr]), t1[c]);
+        }
+        const T wx = T(2 - (dx < 0 ? -dx : dx)) / T(2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t2[c] = fma(wx, t1[c], t2[c]);
+      }
+      const T wz = T(2 - (dz < 0 ? -dz : dz)) / T(2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[c] = fma(wz, t2[c], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[n + c * ostr] = acc[c];
+  }
+}
+
 template <typename TI, typename T>
 void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, T* tmp2, T* out, Grid gc,
                      const uint32_t* cols) {
@@ -888,6 +932,11 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
     (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
     (k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
                                                                              cx, cz, dcy, dcx, nullptr), topx::count_launch());
+  } else if (!cols && gf.nnodes() <= (int64_t(1) << 21)) {
+    // small grids are launch-latency bound: one pass over the 27 taps of every coarse node
+    (k_restrict_span2<TI, T><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, out, gc.stride, cy,
+                                                                       cx, cz, dcy, dcx),
+     topx::count_launch());
   } else {
     (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx, cols), topx::count_launch());
     (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
