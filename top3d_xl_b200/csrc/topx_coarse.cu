@@ -38,7 +38,18 @@ __global__ void __launch_bounds__(GL2_THREADS) k_galerkin_l2(Grid gc, const doub
     }
     sE[jj][c] = v;
   }
-  __syncthreads();
+  // a group of coarse elements whose children are all void (E = 0) sums to zero: write it
+  // without streaming the templates (irregular domains)
+  bool any = false;
+  for (int i = threadIdx.x; i < GL2_ELEMS * 64; i += GL2_THREADS) any = any || sE[i / 64][i % 64] != 0.0;
+  if (!__syncthreads_or(any)) {
+    for (int jj = 0; jj < GL2_ELEMS; ++jj) {
+      const int64_t j = j0 + jj;
+      if (j < nce)
+        for (int k = threadIdx.x; k < 576; k += GL2_THREADS) Ks[j * 576 + k] = 0.0;
+    }
+    return;
+  }
   double acc[GL2_ELEMS][3];
 #pragma unroll
   for (int jj = 0; jj < GL2_ELEMS; ++jj) acc[jj][0] = acc[jj][1] = acc[jj][2] = 0.0;
