@@ -547,7 +547,7 @@ static int ku_z_chunk(int nny, int nnx, int nnz) {
   const int64_t slots = int64_t(g_num_sms) * 3;
   int best = KZC;
   int64_t bestCost = -1;
-  for (int zc = 6; zc <= 24; ++zc) {
+  for (int zc = 1; zc <= 24; ++zc) {
     const int64_t ctas = tiles * ((nnz + zc - 1) / zc);
     const int64_t cost = ((ctas + slots - 1) / slots) * (zc + 2);
     if (bestCost < 0 || cost < bestCost) {
