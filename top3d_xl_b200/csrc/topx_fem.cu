@@ -875,81 +875,45 @@ __global__ void k_restrict_axis(const TI* __restrict__ in, int64_t istr, int iny
   }
 }
 
-// The span-2 restriction in one pass: each coarse node sums its 3 x 3 x 3 fine taps as the three
-// axis passes would (y sums, then x sums of those, then z sums, each in the pass's element type
-// and tap order), so the result is the same bit for bit, with one launch instead of three.
-template <typename TI, typename T>
-__global__ void k_restrict_span2(const TI* __restrict__ in, int64_t istr, int iny, int inx, int inz,
-                                 T* __restrict__ out, int64_t ostr, int ony, int onx, int onz, FastDiv fdy,
-                                 FastDiv fdx) {
+// The restriction in one pass, for small grids (launch-latency bound): L threads per coarse node,
+// one per (x, z) column of its (2S-1)^3 fine taps.  Thread (dx, dz) forms the column's y sum as the
+// first axis pass does (a column without a present node is zero, unread), thread dz of the node
+// the x sum of its columns as the second pass does, and thread 0 the z sum as the third; each sum
+// keeps the pass's element type and tap order, so the result equals the three passes bit for bit.
+template <int S>
+struct RestrictCoop {
+  static constexpr int W = 2 * S - 1;           // taps per axis
+  static constexpr int L = S == 4 ? 64 : 16;    // threads per coarse node (>= W * W)
+  static constexpr int NODES = 256 / L;         // coarse nodes per block
+};
+template <int S, typename TI, typename T>
+__global__ void __launch_bounds__(256) k_restrict_coop(const TI* __restrict__ in, int64_t istr, int iny, int inx,
+                                                      int inz, T* __restrict__ out, int64_t ostr, int ony, int onx,
+                                                      int onz, FastDiv fdy, FastDiv fdx,
+                                                      const uint32_t* __restrict__ cols) {
+  using RC = RestrictCoop<S>;
+  constexpr int W = RC::W, L = RC::L, NODES = RC::NODES;
+  static_assert(W * W <= L, "a thread per tap column");
+  __shared__ T sy[NODES][W * W][3];  // y sums of the node's (dx, dz) columns
+  __shared__ T sx[NODES][W][3];      // x sums per dz
+  const int sub = threadIdx.x / L, lane = threadIdx.x % L;
   const uint32_t N = uint32_t(ony) * onx * onz;
-  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
-    const uint32_t q = fdy.div(n), oz = fdx.div(q);
-    const int oy = int(n - q * uint32_t(ony)), ox = int(q - oz * uint32_t(onx));
-    T acc[3] = {T(0), T(0), T(0)};
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int iz = 2 * int(oz) + dz;
-      if (iz < 0 || iz >= inz) continue;
-      T t2[3] = {T(0), T(0), T(0)};
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int ix = 2 * ox + dx;
-        if (ix < 0 || ix >= inx) continue;
-        T t1[3] = {T(0), T(0), T(0)};
-#pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const int iy = 2 * oy + dy;
-          if (iy < 0 || iy >= iny) continue;
-          const T wy = T(2 - (dy < 0 ? -dy : dy)) / T(2);
-          const int64_t k = iy + int64_t(iny) * (ix + int64_t(inx) * iz);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) t1[c] = fma(wy, T(in[k + c * istr]), t1[c]);
-        }
-        const T wx = T(2 - (dx < 0 ? -dx : dx)) / T(2);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) t2[c] = fma(wx, t1[c], t2[c]);
-      }
-      const T wz = T(2 - (dz < 0 ? -dz : dz)) / T(2);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) acc[c] = fma(wz, t2[c], acc[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) out[n + c * ostr] = acc[c];
-  }
-}
-
-// The span-4 restriction in one pass, for small grids: 64 threads per coarse node, one per (x, z)
-// column of its 7 x 7 x 7 fine taps.  Thread (dx, dz) forms the column's y sum as the first pass
-// does (a column without a present node is zero, unread), thread dz of the node the x sum of its 7
-// columns as the second pass does, and thread 0 the z sum as the third; each sum keeps the pass's
-// element type and tap order, so the result equals the three passes bit for bit.
-constexpr int RS4_NODES = 4;  // coarse nodes per 256-thread block
-template <typename TI, typename T>
-__global__ void __launch_bounds__(64 * RS4_NODES) k_restrict_span4(const TI* __restrict__ in, int64_t istr, int iny,
-                                                                   int inx, int inz, T* __restrict__ out, int64_t ostr,
-                                                                   int ony, int onx, int onz, FastDiv fdy, FastDiv fdx,
-                                                                   const uint32_t* __restrict__ cols) {
-  __shared__ T sy[RS4_NODES][49][3];  // y sums of the node's (dx, dz) columns
-  __shared__ T sx[RS4_NODES][7][3];   // x sums per dz
-  const int sub = threadIdx.x >> 6, lane = threadIdx.x & 63;
-  const uint32_t N = uint32_t(ony) * onx * onz;
-  for (uint32_t base = blockIdx.x * uint32_t(RS4_NODES); base < N; base += gridDim.x * uint32_t(RS4_NODES)) {
+  for (uint32_t base = blockIdx.x * uint32_t(NODES); base < N; base += gridDim.x * uint32_t(NODES)) {
     const uint32_t n = base + uint32_t(sub);
     const bool valid = n < N;
     const uint32_t q = valid ? fdy.div(n) : 0u, oz = valid ? fdx.div(q) : 0u;
     const int oy = int(n - q * uint32_t(ony)), ox = int(q - oz * uint32_t(onx));
-    if (valid && lane < 49) {
-      const int ix = 4 * ox + lane % 7 - 3, iz = 4 * int(oz) + lane / 7 - 3;
+    if (valid && lane < W * W) {
+      const int ix = S * ox + lane % W - (S - 1), iz = S * int(oz) + lane / W - (S - 1);
       T t[3] = {T(0), T(0), T(0)};
       if (ix >= 0 && ix < inx && iz >= 0 && iz < inz) {
         const uint32_t col = uint32_t(ix) + uint32_t(inx) * uint32_t(iz);
         if (!cols || ((__ldg(cols + (col >> 5)) >> (col & 31)) & 1u) != 0u) {
 #pragma unroll
-          for (int dy = -3; dy <= 3; ++dy) {
-            const int iy = 4 * oy + dy;
+          for (int dy = -(S - 1); dy <= S - 1; ++dy) {
+            const int iy = S * oy + dy;
             if (iy < 0 || iy >= iny) continue;
-            const T w = T(4 - (dy < 0 ? -dy : dy)) / T(4);
+            const T w = T(S - (dy < 0 ? -dy : dy)) / T(S);
             const int64_t k = iy + int64_t(iny) * (ix + int64_t(inx) * iz);
 #pragma unroll
             for (int c = 0; c < 3; ++c) t[c] = fma(w, T(in[k + c * istr]), t[c]);
@@ -960,15 +924,15 @@ __global__ void __launch_bounds__(64 * RS4_NODES) k_restrict_span4(const TI* __r
       for (int c = 0; c < 3; ++c) sy[sub][lane][c] = t[c];
     }
     __syncthreads();
-    if (valid && lane < 7) {
+    if (valid && lane < W) {
       T t[3] = {T(0), T(0), T(0)};
 #pragma unroll
-      for (int dx = -3; dx <= 3; ++dx) {
-        const int ix = 4 * ox + dx;
+      for (int dx = -(S - 1); dx <= S - 1; ++dx) {
+        const int ix = S * ox + dx;
         if (ix < 0 || ix >= inx) continue;
-        const T w = T(4 - (dx < 0 ? -dx : dx)) / T(4);
+        const T w = T(S - (dx < 0 ? -dx : dx)) / T(S);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) t[c] = fma(w, sy[sub][lane * 7 + dx + 3][c], t[c]);
+        for (int c = 0; c < 3; ++c) t[c] = fma(w, sy[sub][lane * W + dx + (S - 1)][c], t[c]);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) sx[sub][lane][c] = t[c];
@@ -977,12 +941,12 @@ __global__ void __launch_bounds__(64 * RS4_NODES) k_restrict_span4(const TI* __r
     if (valid && lane == 0) {
       T acc[3] = {T(0), T(0), T(0)};
 #pragma unroll
-      for (int dz = -3; dz <= 3; ++dz) {
-        const int iz = 4 * int(oz) + dz;
+      for (int dz = -(S - 1); dz <= S - 1; ++dz) {
+        const int iz = S * int(oz) + dz;
         if (iz < 0 || iz >= inz) continue;
-        const T w = T(4 - (dz < 0 ? -dz : dz)) / T(4);
+        const T w = T(S - (dz < 0 ? -dz : dz)) / T(S);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[c] = fma(w, sx[sub][dz + 3][c], acc[c]);
+        for (int c = 0; c < 3; ++c) acc[c] = fma(w, sx[sub][dz + (S - 1)][c], acc[c]);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) out[n + c * ostr] = acc[c];
@@ -999,21 +963,21 @@ void launch_restrict(cudaStream_t st, int span, const TI* in, Grid gf, T* tmp1, 
   const int64_t s1 = int64_t(cy) * fx * fz, s2 = int64_t(cy) * cx * fz;
   if (gf.nnodes() >= (int64_t(1) << 32)) throw std::runtime_error("grid too large for 32-bit node indices");
   const FastDiv dcy{uint32_t(cy)}, dfx{uint32_t(fx)}, dcx{uint32_t(cx)};
-  if (span == 4 && gf.nnodes() <= (int64_t(1) << 21)) {
-    // small grids are launch-latency bound: one launch, 64 threads per coarse node
-    (k_restrict_span4<TI, T><<<grid1d(gc.nnodes() * 64, 64 * RS4_NODES), 64 * RS4_NODES, 0, st>>>(
-         in, gf.stride, fy, fx, fz, out, gc.stride, cy, cx, cz, dcy, dcx, cols),
-     topx::count_launch());
+  if (gf.nnodes() <= (int64_t(1) << 21) && (span == 2 || span == 4)) {
+    // small grids are launch-latency bound: one launch, a thread per tap column of a coarse node
+    if (span == 4)
+      (k_restrict_coop<4, TI, T><<<grid1d(gc.nnodes() * RestrictCoop<4>::L, 256), 256, 0, st>>>(
+           in, gf.stride, fy, fx, fz, out, gc.stride, cy, cx, cz, dcy, dcx, cols),
+       topx::count_launch());
+    else
+      (k_restrict_coop<2, TI, T><<<grid1d(gc.nnodes() * RestrictCoop<2>::L, 256), 256, 0, st>>>(
+           in, gf.stride, fy, fx, fz, out, gc.stride, cy, cx, cz, dcy, dcx, cols),
+       topx::count_launch());
   } else if (span == 4) {
     (k_restrict_axis<TI, T, 4, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx, cols), topx::count_launch());
     (k_restrict_axis<T, T, 4, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
     (k_restrict_axis<T, T, 4, 2><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(tmp2, s2, cy, cx, fz, out, gc.stride, cy,
                                                                              cx, cz, dcy, dcx, nullptr), topx::count_launch());
-  } else if (!cols && gf.nnodes() <= (int64_t(1) << 21)) {
-    // small grids are launch-latency bound: one pass over the 27 taps of every coarse node
-    (k_restrict_span2<TI, T><<<grid1d(gc.nnodes(), 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, out, gc.stride, cy,
-                                                                       cx, cz, dcy, dcx),
-     topx::count_launch());
   } else {
     (k_restrict_axis<TI, T, 2, 0><<<grid1d(s1, 256), 256, 0, st>>>(in, gf.stride, fy, fx, fz, tmp1, s1, cy, fx, fz, dcy, dfx, cols), topx::count_launch());
     (k_restrict_axis<T, T, 2, 1><<<grid1d(s2, 256), 256, 0, st>>>(tmp1, s1, cy, fx, fz, tmp2, s2, cy, cx, fz, dcy, dcx, nullptr), topx::count_launch());
